@@ -1,0 +1,242 @@
+/*
+ * naga_b200: B200-native (sm_100a) nonlocal lattice-Boltzmann acoustics step.
+ *
+ * C ABI of libnaga_b200.so. Plain pointers and sizes only; no exceptions
+ * cross this boundary. Every entry point returns an int status (NAGA_OK on
+ * success); naga_last_error() gives a message for the calling thread.
+ *
+ * Each declaration names the NAGA (NAGAGroup/NAGA) interface it replaces,
+ * as path:line within that project. The header-only C++ facade in
+ * include/naga/ maps the reference's template API onto these calls.
+ *
+ * Memory: "host" arguments are ordinary host memory; "device" arguments are
+ * CUDA device pointers on the current device. Scene and batch handles own
+ * their device buffers. Streams are passed as void* (a cudaStream_t; NULL is
+ * the legacy default stream).
+ *
+ * Threading: a handle is not thread-safe; distinct handles may be used from
+ * distinct threads. The library starts no threads of its own.
+ */
+#ifndef NAGA_B200_H
+#define NAGA_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+/* replaces the exceptions of sclx::throw_exception<std::invalid_argument |
+ * std::runtime_error> (e.g. fluids/nonlocal_lattice_boltzmann/detail/
+ * simulation_engine.cuh:128-167, linalg/batched_matrix_inverse.cuh:252-272) */
+enum {
+    NAGA_OK = 0,
+    NAGA_EINVAL = 1,       /* invalid argument / shape mismatch            */
+    NAGA_ENOMEM = 2,       /* allocation failed or over the memory budget  */
+    NAGA_ECUDA = 3,        /* a CUDA runtime call failed                   */
+    NAGA_ENOCONVERGE = 4,  /* refinement did not reach the tolerance       */
+    NAGA_ETIMEOUT = 5,     /* a bounded device wait gave up                */
+    NAGA_ESINGULAR = 6,    /* exactly singular matrix in a factorisation   */
+    NAGA_ENODEVICE = 7     /* no CUDA device / extension not usable        */
+};
+
+/* message for the last failing call on this thread ("" if none) */
+const char* naga_last_error(void);
+/* library version: major * 10000 + minor * 100 + patch */
+int naga_version(void);
+
+/* ------------------------------------------------------ synthetic scenes */
+/* Jittered uniform grid in the unit square/cube with the node classes of
+ * NAGA's uniform_grid_provider (fluids/nonlocal_lattice_boltzmann/
+ * node_providers/uniform_grid_provider.cuh:65-161): interior nodes jittered
+ * by U(-jitter h, +jitter h) per coordinate (splitmix64 stream from `seed`,
+ * `dim` draws per grid node in row-major order), walls unjittered, layer =
+ * squared distance to the nearest boundary node <= (n_layers h)^2,
+ * sigma = sigma_peak ((L - d) / L)^2. Output order: bulk, layer, boundary,
+ * each in Morton order of the grid indices.                                 */
+typedef struct naga_grid_spec {
+    int dim;            /* 2 or 3 */
+    int n_layers;       /* absorbing-layer thickness in grid spacings */
+    int64_t n_side;     /* grid nodes per side, spacing h = 1 / (n_side - 1) */
+    double jitter;      /* jitter as a fraction of h, in [0, 0.5) */
+    double sigma_peak;  /* peak absorption coefficient */
+    uint64_t seed;
+} naga_grid_spec;
+
+int naga_grid_counts(const naga_grid_spec* spec, int64_t* n_bulk,
+                     int64_t* n_layer, int64_t* n_boundary);
+/* host outputs: points [N][dim], normals [n_boundary][dim] (inward),
+ * sigma [n_layer]; any output may be NULL.                                  */
+int naga_grid_generate(const naga_grid_spec* spec, float* points,
+                       float* normals, float* sigma, double* nodal_spacing);
+/* drho_i = amplitude * exp(-|x_i - center|^2 / (2 width^2)), host arrays    */
+int naga_gaussian_pulse(const float* points, int64_t n, int dim,
+                        const double* center, double amplitude, double width,
+                        float* drho);
+
+/* ------------------------------------------------------------ primitives */
+/* Exact k nearest neighbours of each query among src under the
+ * (dist^2, index) order; dist^2 is the FP32 value of
+ * distance_functions.hpp:138-161 (highest dimension added last). Device
+ * arrays: src [n][dim], qry [nq][dim] float; idx, d2 [nq][k] (ascending).
+ * Replaces nd_cubic_segmentation<T,D>(points, approx_size)
+ * (segmentation/nd_cubic_segmentation.cuh:227-303) followed by
+ * batched_nearest_neighbors(k, query_map, segmentation)
+ * (segmentation/nearest_neighbors.cuh:95-108, 444-477).                     */
+int naga_knn(const float* src, int64_t n, const float* qry, int64_t nq,
+             int dim, int k, uint32_t* idx, float* d2, void* stream);
+
+/* Self-kNN of many independent clouds in one launch. pts: device
+ * [total][dim], clouds back to back; offsets: host [n_clouds + 1]. Output
+ * indices are local to each cloud. No reference counterpart as a single
+ * call: the reference runs one segmentation + search per cloud
+ * (examples/batched_knn_search.cu:96-157 runs it per partition size).       */
+int naga_knn_clouds(const float* pts, const int64_t* offsets, int n_clouds,
+                    int dim, int k, uint32_t* idx, float* d2, void* stream);
+
+/* Batched inverse of n x n matrices, each column-major, batch back to back
+ * (device arrays A, A_inv [batch][n][n]; info [batch] or NULL: 0 = ok,
+ * j > 0 = zero pivot at column j). One warp per matrix, LU with partial
+ * pivoting (first maximal |a|) then inversion. Replaces
+ * linalg::batched_matrix_inverse(A, A_inv, copy_A)
+ * (linalg/batched_matrix_inverse.cuh:325-397; cuBLAS getrf/getri at
+ * linalg/detail/batched_matrix_inverse.cuh:46-72). n <= 64.               */
+int naga_batched_inverse_f64(const double* A, double* A_inv, int n,
+                             int64_t batch, int* info, void* stream);
+/* Same result computed from an FP32 LU with FP64-residual iterative
+ * refinement of each column; iterations stop at max_iter or when the
+ * correction is below rel_tol relative to the column. info: as above, or
+ * -1 when a column did not converge.                                        */
+int naga_batched_inverse_f32r(const double* A, double* A_inv, int n,
+                              int64_t batch, int max_iter, double rel_tol,
+                              int* info, void* stream);
+
+/* RBF (radial point interpolation) weights: for every group g with support
+ * indices support[g][k] into src [n][dim], and its `group` query points
+ * qry [ngroups*group][dim], weights[q][k] such that the interpolant at
+ * query q is sum_s weights[q][s] * value(support[g][s]). Augmented system
+ * [[Phi, P], [P^T, 0]] with P = [1, x] (n_sys = k + dim + 1 <= 64).
+ * shape: 0 = multiquadric (r^2 + (0.1 spacing)^2)^0.5, 1 = cubic r^3.
+ * precision: 0 = FP64 LU, 1 = FP32 LU + FP64-residual refinement.
+ * Replaces radial_point_method<T>::compute_weights
+ * (interpolation/radial_point_method.cuh:118-139; detail :92-472).
+ * Device arrays; weights are FP64.                                          */
+int naga_rbf_weights(const float* src, int64_t n, int dim,
+                     const uint32_t* support, int k, const double* qry,
+                     int64_t ngroups, int group, double spacing, int shape,
+                     int precision, double* weights, void* stream);
+
+/* Nonlocal divergence stencil over the points pts [n][dim] (device):
+ * idx [n][k] (kNN), W [n][k][dim] (FP64) with W(d,s,i) the weight of
+ * support s of node i in dimension d, delta [n] (interaction radius) or
+ * NULL. Replaces divergence_operator<T,D>::create(domain, queries)
+ * (nonlocal_calculus/divergence.cuh:53-166; operators.cuh:77-136;
+ * detail/divergence.inl:135-227).                                           */
+int naga_divergence_build(const float* pts, int64_t n, int dim, int k,
+                          int shape, int precision, uint32_t* idx, double* W,
+                          double* delta, void* stream);
+/* result_i = sum_s sum_d W(d,s,i) * field[idx(s,i)][d] with W stored FP32
+ * [n][k][dim] and field [n][dim] (device). Replaces
+ * divergence_operator::apply with default_point_map
+ * (nonlocal_calculus/divergence.cuh:183-212, 377-488).                      */
+int naga_divergence_apply(const float* W, const uint32_t* idx, int64_t n,
+                          int dim, int k, const float* field, float* result,
+                          void* stream);
+
+/* ---------------------------------------------------------------- scenes */
+/* One acoustic scene: domain, stencils and device-resident state.
+ * Replaces naga::fluids::nonlocal_lbm::simulation_engine<Lattice>
+ * (fluids/nonlocal_lattice_boltzmann/simulation_engine.cuh:40-121):
+ * set_problem_parameters :52-66, init_domain :68-74, step_forward :76,
+ * reset :78, attach_observer(density_observer) :90-96, time() :98.        */
+typedef struct naga_scene naga_scene;
+
+typedef struct naga_scene_desc {
+    int dim;              /* 2 -> D2Q9, 3 -> D3Q27 */
+    int k;                /* divergence and filter stencil size (<= 64)   */
+    int k_boundary;       /* boundary-interpolation support size          */
+    int k_probe;          /* probe-interpolation support size             */
+    int shape;            /* RBF: 0 = multiquadric (NAGA default), 1 = r^3 */
+    int pml_indexing;     /* 0 = as NAGA (layer fields read Q of the node
+                             n_bulk places earlier, pml_absorption.inl:
+                             438-448), 1 = each layer node reads its own Q */
+    int weight_precision; /* 0 = FP64 weight solves, 1 = FP32 + refinement */
+    int n_probes;
+    int64_t n_bulk, n_layer, n_boundary, n_ghost;
+    double nodal_spacing;
+    /* set_problem_parameters(nu, rho0, dt, c) */
+    double viscosity, rho0, time_step, speed_of_sound;
+    /* host arrays, copied at creation */
+    const float* points;   /* [N][dim], order bulk, layer, boundary, ghost */
+    const float* normals;  /* [n_boundary][dim], inward                     */
+    const float* sigma;    /* [n_layer]                                     */
+    const float* probes;   /* [n_probes][dim]                               */
+    int probe_capacity;    /* probe samples kept on the device (ring)       */
+} naga_scene_desc;
+
+/* builds stencils and weights on the device and sets the rest state */
+int naga_scene_create(const naga_scene_desc* desc, naga_scene** out);
+int naga_scene_destroy(naga_scene* scene);
+/* stream the scene's work is issued on (a cudaStream_t) */
+void* naga_scene_stream(naga_scene* scene);
+/* rest state plus a density perturbation (host [N], units of rho0), u = 0;
+ * resets time and the probe ring. drho == NULL gives NAGA's reset().     */
+int naga_scene_set_density(naga_scene* scene, const float* drho);
+/* enqueue nsteps time steps on the scene's stream (asynchronous)         */
+int naga_scene_step(naga_scene* scene, int nsteps);
+int naga_scene_sync(naga_scene* scene);
+/* steps taken since the last set_density                                 */
+int64_t naga_scene_step_count(const naga_scene* scene);
+/* probe samples (rho - rho0, sampled at the start of each step) for steps
+ * [first, first + count), host out [count][n_probes]; the ring keeps the
+ * last probe_capacity steps. Synchronises the scene's stream.            */
+int naga_scene_read_probes(naga_scene* scene, int64_t first, int64_t count,
+                           float* out);
+/* centred populations g = f - w, host [N][Q], and rho - rho0, host [N]   */
+int naga_scene_read_state(naga_scene* scene, float* g, float* drho);
+int naga_scene_write_state(naga_scene* scene, const float* g);
+/* set-up tables as stored for the step: idx [N][k], W [N][k][dim],
+ * filter weights [N][k], boundary idx/weights [n_boundary][k_boundary],
+ * probe idx/weights [n_probes][k_probe]. Any output may be NULL.         */
+int naga_scene_read_tables(naga_scene* scene, uint32_t* idx, float* W,
+                           float* filter_w, uint32_t* bidx, float* bw,
+                           uint32_t* pidx, float* pw);
+/* device bytes held by the scene                                          */
+int64_t naga_scene_device_bytes(const naga_scene* scene);
+/* number of nodes N and populations Q                                     */
+int naga_scene_size(const naga_scene* scene, int64_t* n_nodes, int* q);
+
+/* ---------------------------------------------------------------- batches */
+/* Many independent scenes of one lattice advanced together: one launch per
+ * kernel of the step covers every member scene, and the whole step is a
+ * CUDA graph. No reference counterpart: NAGA steps one engine at a time.  */
+typedef struct naga_batch naga_batch;
+
+int naga_batch_create(int dim, naga_batch** out);
+int naga_batch_destroy(naga_batch* batch);
+/* membership changes take effect at the next naga_batch_step             */
+int naga_batch_add(naga_batch* batch, naga_scene* scene);
+int naga_batch_remove(naga_batch* batch, naga_scene* scene);
+int naga_batch_size(const naga_batch* batch);
+void* naga_batch_stream(naga_batch* batch);
+/* enqueue nsteps steps of every member scene (asynchronous)              */
+int naga_batch_step(naga_batch* batch, int nsteps);
+int naga_batch_sync(naga_batch* batch);
+
+/* ---------------------------------------------------------------- timing */
+/* Per-kernel CUDA-event timing of the step kernels (off by default).
+ * When on, every step kernel launch is bracketed by events on the stream
+ * it runs on; naga_profile_read returns, per kernel id, the launch count
+ * and the summed milliseconds. Enabling it disables graph replay.         */
+int naga_profile_enable(int on);
+int naga_profile_reset(void);
+/* names[i] (static strings), launches[i], ms[i] for i < *count (in/out)  */
+int naga_profile_read(int* count, const char** names, int64_t* launches,
+                      double* ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NAGA_B200_H */

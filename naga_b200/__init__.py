@@ -1,0 +1,417 @@
+"""naga_b200: B200-native nonlocal lattice-Boltzmann acoustics step.
+
+Python binding of the C ABI in include/naga_b200.h (libnaga_b200.so, built
+in-tree by naga_b200/_build.py). The names follow NAGA's C++ API
+(NAGAGroup/NAGA, fluids/nonlocal_lattice_boltzmann/simulation_engine.cuh):
+a `Scene` is one simulation_engine with its domain and density observers; a
+`Batch` steps many scenes per launch. There is no CPU fallback: every call
+goes to the CUDA library, and importing this module without the built
+library raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+__all__ = [
+    "NagaError", "lib", "build", "GridSpec", "SceneDesc", "generate_grid", "gaussian_pulse",
+    "Scene", "Batch", "knn", "knn_clouds", "batched_inverse_f64", "batched_inverse_f32r",
+    "rbf_weights", "divergence_build", "profile", "Q_OF", "lattice_weights",
+]
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libnaga_b200.so")
+
+NAGA_OK, NAGA_EINVAL, NAGA_ENOMEM, NAGA_ECUDA = 0, 1, 2, 3
+NAGA_ENOCONVERGE, NAGA_ETIMEOUT, NAGA_ESINGULAR, NAGA_ENODEVICE = 4, 5, 6, 7
+Q_OF = {2: 9, 3: 27}
+
+
+class NagaError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"naga error {code}: {msg}")
+        self.code = code
+
+
+class GridSpec(C.Structure):
+    _fields_ = [("dim", C.c_int), ("n_layers", C.c_int), ("n_side", C.c_int64),
+                ("jitter", C.c_double), ("sigma_peak", C.c_double), ("seed", C.c_uint64)]
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [
+        ("dim", C.c_int), ("k", C.c_int), ("k_boundary", C.c_int), ("k_probe", C.c_int),
+        ("shape", C.c_int), ("pml_indexing", C.c_int), ("weight_precision", C.c_int),
+        ("n_probes", C.c_int),
+        ("n_bulk", C.c_int64), ("n_layer", C.c_int64), ("n_boundary", C.c_int64),
+        ("n_ghost", C.c_int64),
+        ("nodal_spacing", C.c_double), ("viscosity", C.c_double), ("rho0", C.c_double),
+        ("time_step", C.c_double), ("speed_of_sound", C.c_double),
+        ("points", C.c_void_p), ("normals", C.c_void_p), ("sigma", C.c_void_p),
+        ("probes", C.c_void_p), ("probe_capacity", C.c_int),
+    ]
+
+
+_lib = None
+_SIGS = {
+    "naga_last_error": ([], C.c_char_p),
+    "naga_version": ([], C.c_int),
+    "naga_grid_counts": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "naga_grid_generate": ([C.c_void_p] * 5, C.c_int),
+    "naga_gaussian_pulse": ([C.c_void_p, C.c_int64, C.c_int, C.c_void_p, C.c_double, C.c_double,
+                             C.c_void_p], C.c_int),
+    "naga_knn": ([C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_void_p,
+                  C.c_void_p, C.c_void_p], C.c_int),
+    "naga_knn_clouds": ([C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                         C.c_void_p], C.c_int),
+    "naga_batched_inverse_f64": ([C.c_void_p, C.c_void_p, C.c_int, C.c_int64, C.c_void_p, C.c_void_p],
+                                 C.c_int),
+    "naga_batched_inverse_f32r": ([C.c_void_p, C.c_void_p, C.c_int, C.c_int64, C.c_int, C.c_double,
+                                   C.c_void_p, C.c_void_p], C.c_int),
+    "naga_rbf_weights": ([C.c_void_p, C.c_int64, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int64,
+                          C.c_int, C.c_double, C.c_int, C.c_int, C.c_void_p, C.c_void_p], C.c_int),
+    "naga_divergence_build": ([C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                               C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "naga_divergence_apply": ([C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_void_p,
+                               C.c_void_p, C.c_void_p], C.c_int),
+    "naga_scene_create": ([C.c_void_p, C.c_void_p], C.c_int),
+    "naga_scene_destroy": ([C.c_void_p], C.c_int),
+    "naga_scene_stream": ([C.c_void_p], C.c_void_p),
+    "naga_scene_set_density": ([C.c_void_p, C.c_void_p], C.c_int),
+    "naga_scene_step": ([C.c_void_p, C.c_int], C.c_int),
+    "naga_scene_sync": ([C.c_void_p], C.c_int),
+    "naga_scene_step_count": ([C.c_void_p], C.c_int64),
+    "naga_scene_read_probes": ([C.c_void_p, C.c_int64, C.c_int64, C.c_void_p], C.c_int),
+    "naga_scene_read_state": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "naga_scene_write_state": ([C.c_void_p, C.c_void_p], C.c_int),
+    "naga_scene_read_tables": ([C.c_void_p] * 8, C.c_int),
+    "naga_scene_device_bytes": ([C.c_void_p], C.c_int64),
+    "naga_scene_size": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "naga_batch_create": ([C.c_int, C.c_void_p], C.c_int),
+    "naga_batch_destroy": ([C.c_void_p], C.c_int),
+    "naga_batch_add": ([C.c_void_p, C.c_void_p], C.c_int),
+    "naga_batch_remove": ([C.c_void_p, C.c_void_p], C.c_int),
+    "naga_batch_size": ([C.c_void_p], C.c_int),
+    "naga_batch_stream": ([C.c_void_p], C.c_void_p),
+    "naga_batch_step": ([C.c_void_p, C.c_int], C.c_int),
+    "naga_batch_sync": ([C.c_void_p], C.c_int),
+    "naga_profile_enable": ([C.c_int], C.c_int),
+    "naga_profile_reset": ([], C.c_int),
+    "naga_profile_read": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+}
+
+
+def build(verbose: bool = False) -> str:
+    from . import _build
+
+    return _build.build(verbose=verbose)
+
+
+def lib():
+    """The loaded libnaga_b200.so; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run naga_b200._build.build() (nvcc, sm_100a)")
+        L = C.CDLL(LIB_PATH)
+        for name, (args, res) in _SIGS.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def _check(rc: int) -> None:
+    if rc != NAGA_OK:
+        raise NagaError(rc, lib().naga_last_error().decode())
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def lattice_weights(dim: int) -> np.ndarray:
+    if dim == 2:
+        return np.array([4 / 9, 1 / 36, 1 / 9, 1 / 36, 1 / 9, 1 / 36, 1 / 9, 1 / 36, 1 / 9])
+    return np.array([8 / 27] + [2 / 27] * 6 + [1 / 54] * 12 + [1 / 216] * 8)
+
+
+# ------------------------------------------------------------ synthetic input
+def generate_grid(dim: int, n_side: int, n_layers: int, seed: int, jitter: float = 0.25,
+                  sigma_peak: float = 0.1) -> dict:
+    """Jittered unit-grid scene (see naga_grid_generate in include/naga_b200.h)."""
+    sp = GridSpec(dim, n_layers, n_side, jitter, sigma_peak, seed)
+    nb, nl, nbd = C.c_int64(), C.c_int64(), C.c_int64()
+    _check(lib().naga_grid_counts(C.byref(sp), C.byref(nb), C.byref(nl), C.byref(nbd)))
+    n = nb.value + nl.value + nbd.value
+    pts = np.zeros((n, dim), np.float32)
+    nrm = np.zeros((nbd.value, dim), np.float32)
+    sig = np.zeros(nl.value, np.float32)
+    h = C.c_double()
+    _check(lib().naga_grid_generate(C.byref(sp), _p(pts), _p(nrm), _p(sig), C.byref(h)))
+    return dict(dim=dim, points=pts, n_bulk=nb.value, n_layer=nl.value, n_boundary=nbd.value,
+                normals=nrm, sigma=sig, h=h.value)
+
+
+def gaussian_pulse(points: np.ndarray, center, amplitude: float, width: float) -> np.ndarray:
+    pts = np.ascontiguousarray(points, np.float32)
+    c = np.ascontiguousarray(center, np.float64)
+    out = np.zeros(pts.shape[0], np.float32)
+    _check(lib().naga_gaussian_pulse(_p(pts), pts.shape[0], pts.shape[1], _p(c), amplitude, width,
+                                     _p(out)))
+    return out
+
+
+# ---------------------------------------------------------------- scenes
+class Scene:
+    """One acoustic scene: NAGA's simulation_engine<Lattice> after
+    set_problem_parameters + init_domain, with density observers (probes)."""
+
+    def __init__(self, grid: dict, *, k: int, k_boundary: int | None = None,
+                 k_probe: int | None = None, shape: int = 1, pml_indexing: int = 0,
+                 weight_precision: int = 0, viscosity: float = 1e-5, rho0: float = 1.0,
+                 time_step: float | None = None, speed_of_sound: float = 1.0, probes=None,
+                 probe_capacity: int = 4096, n_ghost: int = 0):
+        dim = grid["dim"]
+        self.dim, self.Q = dim, Q_OF[dim]
+        self._keep = [np.ascontiguousarray(grid["points"], np.float32),
+                      np.ascontiguousarray(grid["normals"], np.float32),
+                      np.ascontiguousarray(grid["sigma"], np.float32),
+                      np.ascontiguousarray(probes if probes is not None else np.zeros((0, dim)),
+                                           np.float32)]
+        self.N = self._keep[0].shape[0]
+        self.n_probes = self._keep[3].shape[0]
+        d = SceneDesc()
+        d.dim, d.k = dim, k
+        d.k_boundary = k_boundary or k
+        d.k_probe = k_probe or k
+        d.shape, d.pml_indexing, d.weight_precision = shape, pml_indexing, weight_precision
+        d.n_probes = self.n_probes
+        d.n_bulk, d.n_layer, d.n_boundary = grid["n_bulk"], grid["n_layer"], grid["n_boundary"]
+        d.n_ghost = n_ghost
+        d.nodal_spacing = grid["h"]
+        d.viscosity, d.rho0, d.speed_of_sound = viscosity, rho0, speed_of_sound
+        d.time_step = time_step if time_step is not None else 0.5 * grid["h"] / speed_of_sound
+        d.points, d.normals, d.sigma, d.probes = (_p(a) for a in self._keep)
+        d.probe_capacity = probe_capacity
+        self.desc = d
+        self.h = C.c_void_p()
+        _check(lib().naga_scene_create(C.byref(d), C.byref(self.h)))
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            lib().naga_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_density(self, drho=None):
+        if drho is None:
+            _check(lib().naga_scene_set_density(self.h, None))
+        else:
+            drho = np.ascontiguousarray(drho, np.float32)
+            assert drho.shape == (self.N,)
+            _check(lib().naga_scene_set_density(self.h, _p(drho)))
+
+    def step(self, n: int = 1):
+        _check(lib().naga_scene_step(self.h, n))
+
+    def sync(self):
+        _check(lib().naga_scene_sync(self.h))
+
+    @property
+    def step_count(self) -> int:
+        return lib().naga_scene_step_count(self.h)
+
+    @property
+    def stream(self) -> int:
+        return lib().naga_scene_stream(self.h) or 0
+
+    def probes(self, first: int = 0, count: int | None = None) -> np.ndarray:
+        if count is None:
+            count = self.step_count - first
+        out = np.zeros((count, self.n_probes), np.float32)
+        _check(lib().naga_scene_read_probes(self.h, first, count, _p(out)))
+        return out
+
+    def state(self):
+        g = np.zeros((self.N, self.Q), np.float32)
+        r = np.zeros(self.N, np.float32)
+        _check(lib().naga_scene_read_state(self.h, _p(g), _p(r)))
+        return g, r
+
+    def write_state(self, g):
+        g = np.ascontiguousarray(g, np.float32)
+        _check(lib().naga_scene_write_state(self.h, _p(g)))
+
+    def tables(self) -> dict:
+        d = self.desc
+        k, kb, kp, dim = d.k, d.k_boundary, d.k_probe, self.dim
+        out = dict(idx=np.zeros((self.N, k), np.uint32), W=np.zeros((self.N, k, dim), np.float32),
+                   fw=np.zeros((self.N, k), np.float32),
+                   bidx=np.zeros((d.n_boundary, kb), np.uint32),
+                   bw=np.zeros((d.n_boundary, kb), np.float32),
+                   pidx=np.zeros((self.n_probes, kp), np.uint32),
+                   pw=np.zeros((self.n_probes, kp), np.float32))
+        _check(lib().naga_scene_read_tables(self.h, *(_p(out[n]) for n in
+                                                      ("idx", "W", "fw", "bidx", "bw", "pidx", "pw"))))
+        return out
+
+    @property
+    def device_bytes(self) -> int:
+        return lib().naga_scene_device_bytes(self.h)
+
+
+class Batch:
+    """Many scenes of one lattice, stepped together (one launch per kernel)."""
+
+    def __init__(self, dim: int):
+        self.h = C.c_void_p()
+        self.scenes: list[Scene] = []
+        _check(lib().naga_batch_create(dim, C.byref(self.h)))
+
+    def add(self, s: Scene):
+        _check(lib().naga_batch_add(self.h, s.h))
+        self.scenes.append(s)
+
+    def remove(self, s: Scene):
+        _check(lib().naga_batch_remove(self.h, s.h))
+        self.scenes.remove(s)
+
+    def step(self, n: int = 1):
+        _check(lib().naga_batch_step(self.h, n))
+
+    def sync(self):
+        _check(lib().naga_batch_sync(self.h))
+
+    @property
+    def stream(self) -> int:
+        return lib().naga_batch_stream(self.h) or 0
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            lib().naga_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------- primitives
+# Device buffers are torch CUDA tensors (plumbing only); results are torch
+# tensors on the same device.
+def _torch():
+    import torch
+
+    return torch
+
+
+def _dptr(t):
+    return C.c_void_p(t.data_ptr())
+
+
+def _stream_ptr():
+    torch = _torch()
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def knn(src, qry, k: int):
+    """Exact kNN (device tensors [n][dim] float32) -> (idx int32 [nq][k], d2)."""
+    torch = _torch()
+    src = src.contiguous().float()
+    qry = qry.contiguous().float()
+    idx = torch.empty((qry.shape[0], k), dtype=torch.int32, device=src.device)
+    d2 = torch.empty((qry.shape[0], k), dtype=torch.float32, device=src.device)
+    _check(lib().naga_knn(_dptr(src), src.shape[0], _dptr(qry), qry.shape[0], src.shape[1], k,
+                          _dptr(idx), _dptr(d2), _stream_ptr()))
+    return idx, d2
+
+
+def knn_clouds(pts, offsets, k: int):
+    torch = _torch()
+    pts = pts.contiguous().float()
+    off = np.ascontiguousarray(offsets, np.int64)
+    idx = torch.empty((pts.shape[0], k), dtype=torch.int32, device=pts.device)
+    d2 = torch.empty((pts.shape[0], k), dtype=torch.float32, device=pts.device)
+    _check(lib().naga_knn_clouds(_dptr(pts), _p(off), len(off) - 1, pts.shape[1], k, _dptr(idx),
+                                 _dptr(d2), _stream_ptr()))
+    return idx, d2
+
+
+def batched_inverse_f64(A):
+    """A: device float64 [batch][n][n] with element (i, j) at A[b, j, i]."""
+    torch = _torch()
+    A = A.contiguous()
+    out = torch.empty_like(A)
+    info = torch.empty(A.shape[0], dtype=torch.int32, device=A.device)
+    _check(lib().naga_batched_inverse_f64(_dptr(A), _dptr(out), A.shape[1], A.shape[0], _dptr(info),
+                                          _stream_ptr()))
+    return out, info
+
+
+def batched_inverse_f32r(A, max_iter: int = 20, rel_tol: float = 1e-14):
+    torch = _torch()
+    A = A.contiguous()
+    out = torch.empty_like(A)
+    info = torch.empty(A.shape[0], dtype=torch.int32, device=A.device)
+    _check(lib().naga_batched_inverse_f32r(_dptr(A), _dptr(out), A.shape[1], A.shape[0], max_iter,
+                                           rel_tol, _dptr(info), _stream_ptr()))
+    return out, info
+
+
+def rbf_weights(src, support, qry, group: int, spacing: float, shape: int, precision: int = 0):
+    torch = _torch()
+    src = src.contiguous().float()
+    support = support.contiguous().to(torch.int32)
+    qry = qry.contiguous().double()
+    ng, k = support.shape
+    w = torch.empty((ng * group, k), dtype=torch.float64, device=src.device)
+    _check(lib().naga_rbf_weights(_dptr(src), src.shape[0], src.shape[1], _dptr(support), k,
+                                  _dptr(qry), ng, group, spacing, shape, precision, _dptr(w),
+                                  _stream_ptr()))
+    return w
+
+
+def divergence_build(pts, k: int, shape: int, precision: int = 0):
+    torch = _torch()
+    pts = pts.contiguous().float()
+    n, dim = pts.shape
+    idx = torch.empty((n, k), dtype=torch.int32, device=pts.device)
+    W = torch.empty((n, k, dim), dtype=torch.float64, device=pts.device)
+    delta = torch.empty(n, dtype=torch.float64, device=pts.device)
+    _check(lib().naga_divergence_build(_dptr(pts), n, dim, k, shape, precision, _dptr(idx), _dptr(W),
+                                       _dptr(delta), _stream_ptr()))
+    return idx, W, delta
+
+
+class profile:
+    """Per-kernel CUDA-event timing of the step kernels (context manager)."""
+
+    def __enter__(self):
+        _check(lib().naga_profile_enable(1))
+        _check(lib().naga_profile_reset())
+        return self
+
+    def __exit__(self, *exc):
+        self.result = read_profile()
+        lib().naga_profile_enable(0)
+        return False
+
+
+def read_profile() -> dict:
+    n = C.c_int(64)
+    names = (C.c_char_p * 64)()
+    launches = np.zeros(64, np.int64)
+    ms = np.zeros(64, np.float64)
+    _check(lib().naga_profile_read(C.byref(n), names, _p(launches), _p(ms)))
+    return {names[i].decode(): (int(launches[i]), float(ms[i])) for i in range(n.value)}

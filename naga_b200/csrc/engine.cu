@@ -1,0 +1,785 @@
+// Scenes and batches: device memory, the set-up pipeline (kNN, stencil and
+// RPIM weights on the GPU), work tables, CUDA-graph replay of the step, and
+// the C ABI around them.
+//
+// Reference: fluids/nonlocal_lattice_boltzmann/simulation_engine.cuh:40-121
+// (public engine) and detail/simulation_engine.cuh:94-339 (parameters and
+// init_domain), simulation_observers/density_observer.cuh:62-113 (probes).
+#include "common.cuh"
+#include "scene_dev.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <vector>
+
+namespace naga {
+
+int sm_count() {
+    static int cached[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) dev = 0;
+    if (!cached[dev]) {
+        int v = 0;
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+        cached[dev] = v > 0 ? v : 148;
+    }
+    return cached[dev];
+}
+
+// ------------------------------------------------------------- profiling
+namespace {
+struct ProfState {
+    bool on = false;
+    std::mutex mu;
+    struct Rec {
+        int id;
+        cudaEvent_t a, b;
+    };
+    std::vector<Rec> pending;
+    std::vector<int64_t> launches;
+    std::vector<double> ms;
+    cudaEvent_t cur_a = nullptr;
+} g_prof;
+
+void prof_drain() {
+    for (auto& r : g_prof.pending) {
+        cudaEventSynchronize(r.b);
+        float t = 0;
+        cudaEventElapsedTime(&t, r.a, r.b);
+        if ((size_t)r.id >= g_prof.ms.size()) {
+            g_prof.ms.resize(r.id + 1, 0.0);
+            g_prof.launches.resize(r.id + 1, 0);
+        }
+        g_prof.ms[r.id] += t;
+        g_prof.launches[r.id] += 1;
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    g_prof.pending.clear();
+}
+}  // namespace
+
+bool prof_on() { return g_prof.on; }
+void prof_begin(int, cudaStream_t st) {
+    cudaEventCreate(&g_prof.cur_a);
+    cudaEventRecord(g_prof.cur_a, st);
+}
+void prof_end(int id, cudaStream_t st) {
+    cudaEvent_t b;
+    cudaEventCreate(&b);
+    cudaEventRecord(b, st);
+    std::lock_guard<std::mutex> lk(g_prof.mu);
+    g_prof.pending.push_back({id, g_prof.cur_a, b});
+    if (g_prof.pending.size() > 4096) prof_drain();
+}
+
+}  // namespace naga
+
+using namespace naga;
+
+// ================================================================ objects
+struct naga_batch;
+
+struct naga_scene {
+    int dim = 0, Q = 0, QP = 0;
+    naga_scene_desc desc{};
+    int64_t N = 0, nb = 0, nl = 0, nbd = 0, ng = 0, nbl = 0, nd = 0;
+    cudaStream_t stream = nullptr;
+    SceneDev dev{};
+    std::vector<void*> allocs;
+    int64_t bytes = 0;
+    std::vector<WorkItem> items_all, items_fluid, items_edge;  // scene slot 0
+    naga_batch* owner = nullptr;                               // user batch, if any
+    naga_batch* solo = nullptr;                                // private batch for naga_scene_step
+    int64_t steps = 0;                                         // host mirror of the device counter
+    std::vector<float> probe_xyz;
+
+    template <class T>
+    int alloc(T** p, int64_t count) {
+        size_t b = sizeof(T) * (size_t)std::max<int64_t>(count, 1);
+        cudaError_t e = cudaMalloc((void**)p, b);
+        if (e != cudaSuccess) {
+            *p = nullptr;
+            cudaGetLastError();
+            return set_error(e == cudaErrorMemoryAllocation ? NAGA_ENOMEM : NAGA_ECUDA,
+                             std::string("naga_scene_create: cudaMalloc: ") + cudaGetErrorString(e));
+        }
+        allocs.push_back((void*)*p);
+        bytes += (int64_t)b;
+        return NAGA_OK;
+    }
+};
+
+struct naga_batch {
+    int dim = 0;
+    bool is_solo = false;
+    std::vector<naga_scene*> members;
+    bool dirty = true;
+    cudaStream_t stream = nullptr;
+    SceneDev* d_scenes = nullptr;
+    WorkItem *d_all = nullptr, *d_fluid = nullptr, *d_edge = nullptr;
+    int n_all = 0, n_fluid = 0, n_edge = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+
+    void free_tables() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+        if (d_scenes) cudaFree(d_scenes);
+        if (d_all) cudaFree(d_all);
+        if (d_fluid) cudaFree(d_fluid);
+        if (d_edge) cudaFree(d_edge);
+        d_scenes = nullptr;
+        d_all = d_fluid = d_edge = nullptr;
+    }
+};
+
+namespace {
+
+cudaStream_t active_stream(naga_scene* s) { return s->owner ? s->owner->stream : s->stream; }
+
+int check_device() {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return set_error(NAGA_ENODEVICE, "no CUDA device available");
+    }
+    return NAGA_OK;
+}
+
+void make_items(int64_t begin, int64_t end, std::vector<WorkItem>& out) {
+    out.clear();
+    uint32_t local = 0;
+    for (int64_t b = begin; b < end; b += 128)
+        out.push_back({0u, (uint32_t)b, (uint32_t)std::min<int64_t>(end, b + 128), local++});
+}
+
+float lattice_cs_f() { return 0.57735026918962576450914878050196f; }
+
+// set_problem_parameters (detail/simulation_engine.cuh:94-124) in FP32, and
+// the relaxation rates of the collision models
+void set_parameters(naga_scene* s) {
+    const naga_scene_desc& d = s->desc;
+    SceneDev& D = s->dev;
+    const float c = (float)d.speed_of_sound;
+    const float ratio = lattice_cs_f() / c;
+    const float dt_lat = (float)d.time_step / ratio;
+    const float nu_lat = (float)d.viscosity / ratio;
+    D.dt_lat = dt_lat;
+    D.inv_dt = 1.f / dt_lat;
+    D.rho0 = (float)d.rho0;
+    if (s->dim == 3) {
+        D.om_ab = 1.f / (3.f * nu_lat + .5f) / dt_lat;
+        const float fixed[6] = {1.5f, 1.83f, 1.4f, 1.61f, 1.98f, 1.74f};
+        for (int t = 0; t < 6; ++t) {
+            float unit_nu = (1.f / fixed[t] - .5f) / 3.f;
+            D.om_fix[t] = 1.f / (3.f * unit_nu + .5f) / dt_lat;
+        }
+    } else {
+        D.om_ab = 1.f / (3.f * nu_lat + .5f * dt_lat);
+        for (int t = 0; t < 6; ++t) D.om_fix[t] = 0.f;
+    }
+    D.a_half = dt_lat * 0.5f;
+    D.a_full = dt_lat * 1.f;
+    D.b1 = (float)(1. / 6.);
+    D.b2 = (float)(2. / 6.);
+    D.half_dt = dt_lat / 2.f;
+}
+
+int scene_setup(naga_scene* s) {
+    const naga_scene_desc& d = s->desc;
+    const int D = s->dim, QP = s->QP;
+    const int64_t N = s->N;
+    cudaStream_t st = s->stream;
+    SceneDev& V = s->dev;
+    V.N = N;
+    V.nb = s->nb;
+    V.nl = s->nl;
+    V.nbd = s->nbd;
+    V.ng = s->ng;
+    V.nbl = s->nbl;
+    V.k = d.k;
+    V.kb = d.k_boundary;
+    V.kp = d.k_probe;
+    V.np = d.n_probes;
+    V.pml_shift = d.pml_indexing == 0 ? (int)s->nb : 0;
+    V.probe_cap = std::max(1, d.probe_capacity);
+    set_parameters(s);
+
+    float* pts = nullptr;
+    int rc;
+    if ((rc = s->alloc(&pts, N * D))) return rc;
+    NAGA_CUDA_TRY(cudaMemcpyAsync(pts, d.points, sizeof(float) * N * D, cudaMemcpyHostToDevice, st));
+    NAGA_CUDA_TRY(cudaStreamSynchronize(st));
+    float* nrm = nullptr;
+    float* sig = nullptr;
+    if ((rc = s->alloc(&nrm, s->nbd * D))) return rc;
+    if ((rc = s->alloc(&sig, s->nl))) return rc;
+    if (s->nbd) NAGA_CUDA_TRY(cudaMemcpyAsync(nrm, d.normals, sizeof(float) * s->nbd * D, cudaMemcpyHostToDevice, st));
+    if (s->nl) NAGA_CUDA_TRY(cudaMemcpyAsync(sig, d.sigma, sizeof(float) * s->nl, cudaMemcpyHostToDevice, st));
+    V.normals = nrm;
+    V.sigma = sig;
+
+    // state buffers
+    float* bufs[8];
+    for (int b = 0; b < 8; ++b) {
+        if ((rc = s->alloc(&bufs[b], N * QP))) return rc;
+        NAGA_CUDA_TRY(cudaMemsetAsync(bufs[b], 0, sizeof(float) * N * QP, st));
+    }
+    V.G = bufs[0];
+    V.G1 = bufs[1];
+    V.G2 = bufs[2];
+    V.ACC = bufs[3];
+    V.S1 = bufs[4];
+    V.S1P = bufs[5];
+    V.Q1a = bufs[6];
+    V.Q1b = bufs[7];
+    float4* M = nullptr;
+    if ((rc = s->alloc(&M, N))) return rc;
+    NAGA_CUDA_TRY(cudaMemsetAsync(M, 0, sizeof(float4) * N, st));
+    V.M = M;
+
+    // divergence stencil + filter weights over the domain [0, nd)
+    const int k = d.k;
+    StencilOut out{};
+    out.ld = N;
+    out.filter_sigma = d.nodal_spacing / 2.5;
+    uint32_t* knn_idx = nullptr;
+    if ((rc = s->alloc(&knn_idx, s->nd * k))) return rc;
+    if (D == 3) {
+        float4* W = nullptr;
+        if ((rc = s->alloc(&W, (int64_t)k * N))) return rc;
+        NAGA_CUDA_TRY(cudaMemsetAsync(W, 0, sizeof(float4) * k * N, st));
+        out.Wf = reinterpret_cast<float*>(W);
+        V.stW = W;
+        V.stI = nullptr;
+    } else {
+        float2* W = nullptr;
+        uint32_t* I = nullptr;
+        if ((rc = s->alloc(&W, (int64_t)k * N))) return rc;
+        if ((rc = s->alloc(&I, (int64_t)k * N))) return rc;
+        NAGA_CUDA_TRY(cudaMemsetAsync(W, 0, sizeof(float2) * k * N, st));
+        NAGA_CUDA_TRY(cudaMemsetAsync(I, 0, sizeof(uint32_t) * k * N, st));
+        out.Wf = reinterpret_cast<float*>(W);
+        out.If = I;
+        V.stW = W;
+        V.stI = I;
+    }
+    float2* F = nullptr;
+    if ((rc = s->alloc(&F, (int64_t)k * N))) return rc;
+    NAGA_CUDA_TRY(cudaMemsetAsync(F, 0, sizeof(float2) * k * N, st));
+    out.Ff = F;
+    V.stF = F;
+    rc = divergence_build_device(pts, s->nd, D, k, d.shape, d.weight_precision, knn_idx, out, st);
+    if (rc) return rc;
+
+    // boundary interpolation: kNN among bulk + layer, RPIM at the boundary
+    // node with the nodal spacing (detail/simulation_engine.cuh:223-258)
+    std::vector<uint8_t> is_src(N, 0);
+    auto rpim = [&](const float* qry_host, int64_t nq, int64_t nsrc, int kk, uint32_t** idx_out, float** w_out) -> int {
+        uint32_t* didx = nullptr;
+        float* dd2 = nullptr;
+        float* dq = nullptr;
+        double* dqd = nullptr;
+        double* dw = nullptr;
+        NAGA_CUDA_TRY(cudaMallocAsync(&didx, sizeof(uint32_t) * nq * kk, st));
+        NAGA_CUDA_TRY(cudaMallocAsync(&dd2, sizeof(float) * nq * kk, st));
+        NAGA_CUDA_TRY(cudaMallocAsync(&dq, sizeof(float) * nq * D, st));
+        NAGA_CUDA_TRY(cudaMallocAsync(&dqd, sizeof(double) * nq * D, st));
+        NAGA_CUDA_TRY(cudaMallocAsync(&dw, sizeof(double) * nq * kk, st));
+        std::vector<double> qd(nq * D);
+        for (int64_t t = 0; t < nq * D; ++t) qd[t] = qry_host[t];
+        NAGA_CUDA_TRY(cudaMemcpyAsync(dq, qry_host, sizeof(float) * nq * D, cudaMemcpyHostToDevice, st));
+        NAGA_CUDA_TRY(cudaMemcpyAsync(dqd, qd.data(), sizeof(double) * nq * D, cudaMemcpyHostToDevice, st));
+        int r = knn_device(pts, nsrc, dq, nq, D, kk, didx, dd2, st);
+        if (!r) r = rbf_weights_device(pts, nsrc, D, didx, kk, dqd, nq, 1, d.nodal_spacing, d.shape,
+                                       d.weight_precision, dw, st);
+        std::vector<uint32_t> hi(nq * kk);
+        std::vector<double> hw(nq * kk);
+        if (!r) {
+            cudaError_t e1 = cudaMemcpyAsync(hi.data(), didx, sizeof(uint32_t) * nq * kk, cudaMemcpyDeviceToHost, st);
+            cudaError_t e2 = cudaMemcpyAsync(hw.data(), dw, sizeof(double) * nq * kk, cudaMemcpyDeviceToHost, st);
+            cudaError_t e3 = cudaStreamSynchronize(st);
+            if (e1 || e2 || e3) r = set_error(NAGA_ECUDA, "naga_scene_create: copy of interpolation tables failed");
+        }
+        cudaFreeAsync(didx, st);
+        cudaFreeAsync(dd2, st);
+        cudaFreeAsync(dq, st);
+        cudaFreeAsync(dqd, st);
+        cudaFreeAsync(dw, st);
+        if (r) return r;
+        // transpose to [k][nq] for coalesced per-node reads
+        std::vector<uint32_t> ti(nq * kk);
+        std::vector<float> tw(nq * kk);
+        for (int64_t q = 0; q < nq; ++q)
+            for (int t = 0; t < kk; ++t) {
+                ti[(int64_t)t * nq + q] = hi[q * kk + t];
+                tw[(int64_t)t * nq + q] = (float)hw[q * kk + t];
+            }
+        if ((r = s->alloc(idx_out, nq * kk))) return r;
+        if ((r = s->alloc(w_out, nq * kk))) return r;
+        NAGA_CUDA_TRY(cudaMemcpyAsync(*idx_out, ti.data(), sizeof(uint32_t) * nq * kk, cudaMemcpyHostToDevice, st));
+        NAGA_CUDA_TRY(cudaMemcpyAsync(*w_out, tw.data(), sizeof(float) * nq * kk, cudaMemcpyHostToDevice, st));
+        NAGA_CUDA_TRY(cudaStreamSynchronize(st));
+        if (idx_out && nsrc == s->nbl)
+            for (auto j : hi) is_src[j] = 1;
+        return NAGA_OK;
+    };
+    uint32_t* bidx = nullptr;
+    float* bw = nullptr;
+    if (s->nbd > 0) {
+        if ((rc = rpim(d.points + s->nbl * D, s->nbd, s->nbl, d.k_boundary, &bidx, &bw))) return rc;
+    }
+    V.bidx = bidx;
+    V.bw = bw;
+    uint32_t* pidx = nullptr;
+    float* pw = nullptr;
+    if (d.n_probes > 0) {
+        // probes: kNN among all points (density_observer.cuh:62-97); they do
+        // not mark interpolation sources
+        std::vector<uint8_t> keep = is_src;
+        if ((rc = rpim(d.probes, d.n_probes, N, d.k_probe, &pidx, &pw))) return rc;
+        is_src = keep;
+    }
+    V.pidx = pidx;
+    V.pw = pw;
+    uint8_t* dsrc = nullptr;
+    if ((rc = s->alloc(&dsrc, N))) return rc;
+    NAGA_CUDA_TRY(cudaMemcpyAsync(dsrc, is_src.data(), N, cudaMemcpyHostToDevice, st));
+    NAGA_CUDA_TRY(cudaStreamSynchronize(st));
+    V.is_src = dsrc;
+
+    float* ring = nullptr;
+    if ((rc = s->alloc(&ring, (int64_t)V.probe_cap * std::max(1, d.n_probes)))) return rc;
+    NAGA_CUDA_TRY(cudaMemsetAsync(ring, 0, sizeof(float) * V.probe_cap * std::max(1, d.n_probes), st));
+    V.probe_ring = ring;
+
+    make_items(0, N, s->items_all);
+    make_items(0, s->nbl, s->items_fluid);
+    make_items(s->nbl, N, s->items_edge);
+    V.n_all_items = (int)s->items_all.size();
+    double* partials = nullptr;
+    if ((rc = s->alloc(&partials, (int64_t)V.n_all_items * 2 * s->Q))) return rc;
+    NAGA_CUDA_TRY(cudaMemsetAsync(partials, 0, sizeof(double) * V.n_all_items * 2 * s->Q, st));
+    V.partials = partials;
+    float* means = nullptr;
+    if ((rc = s->alloc(&means, 2 * s->Q))) return rc;
+    NAGA_CUDA_TRY(cudaMemsetAsync(means, 0, sizeof(float) * 2 * s->Q, st));
+    V.means = means;
+    unsigned long long* step = nullptr;
+    if ((rc = s->alloc(&step, 1))) return rc;
+    NAGA_CUDA_TRY(cudaMemsetAsync(step, 0, sizeof(unsigned long long), st));
+    V.step = step;
+    NAGA_CUDA_TRY(cudaStreamSynchronize(st));
+    return NAGA_OK;
+}
+
+int batch_rebuild(naga_batch* b) {
+    b->free_tables();
+    std::vector<SceneDev> sd;
+    std::vector<WorkItem> all, fluid, edge;
+    for (size_t t = 0; t < b->members.size(); ++t) {
+        naga_scene* s = b->members[t];
+        sd.push_back(s->dev);
+        for (auto it : s->items_all) {
+            it.scene = (uint32_t)t;
+            all.push_back(it);
+        }
+        for (auto it : s->items_fluid) {
+            it.scene = (uint32_t)t;
+            fluid.push_back(it);
+        }
+        for (auto it : s->items_edge) {
+            it.scene = (uint32_t)t;
+            edge.push_back(it);
+        }
+    }
+    b->n_all = (int)all.size();
+    b->n_fluid = (int)fluid.size();
+    b->n_edge = (int)edge.size();
+    auto up = [&](auto** dst, const auto& v) -> int {
+        using T = typename std::remove_reference<decltype(v)>::type::value_type;
+        size_t bytes = sizeof(T) * std::max<size_t>(v.size(), 1);
+        NAGA_CUDA_TRY(cudaMalloc((void**)dst, bytes));
+        if (!v.empty())
+            NAGA_CUDA_TRY(cudaMemcpyAsync(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, b->stream));
+        NAGA_CUDA_TRY(cudaStreamSynchronize(b->stream));
+        return NAGA_OK;
+    };
+    int rc;
+    if ((rc = up(&b->d_scenes, sd))) return rc;
+    if ((rc = up(&b->d_all, all))) return rc;
+    if ((rc = up(&b->d_fluid, fluid))) return rc;
+    if ((rc = up(&b->d_edge, edge))) return rc;
+    b->dirty = false;
+    return NAGA_OK;
+}
+
+StepLaunch launch_of(naga_batch* b) {
+    StepLaunch P;
+    P.scenes = b->d_scenes;
+    P.nscenes = (int)b->members.size();
+    P.all = b->d_all;
+    P.n_all = b->n_all;
+    P.fluid = b->d_fluid;
+    P.n_fluid = b->n_fluid;
+    P.edge = b->d_edge;
+    P.n_edge = b->n_edge;
+    return P;
+}
+
+int batch_step(naga_batch* b, int nsteps) {
+    if (nsteps < 0) return set_error(NAGA_EINVAL, "step: negative step count");
+    if (b->members.empty() || nsteps == 0) return NAGA_OK;
+    int rc;
+    if (b->dirty && (rc = batch_rebuild(b))) return rc;
+    StepLaunch P = launch_of(b);
+    if (prof_on()) {
+        for (int n = 0; n < nsteps; ++n)
+            if ((rc = enqueue_step(b->dim, P, b->stream))) return rc;
+    } else {
+        if (!b->exec) {
+            NAGA_CUDA_TRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+            rc = enqueue_step(b->dim, P, b->stream);
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+            if (rc) {
+                if (g) cudaGraphDestroy(g);
+                return rc;
+            }
+            if (e != cudaSuccess) return set_error(NAGA_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+            b->graph = g;
+            NAGA_CUDA_TRY(cudaGraphInstantiate(&b->exec, g, 0));
+        }
+        for (int n = 0; n < nsteps; ++n) NAGA_CUDA_TRY(cudaGraphLaunch(b->exec, b->stream));
+    }
+    for (auto* s : b->members) s->steps += nsteps;
+    return NAGA_OK;
+}
+
+}  // namespace
+
+// ================================================================== C ABI
+extern "C" int naga_scene_create(const naga_scene_desc* d, naga_scene** out) {
+    if (!d || !out) return set_error(NAGA_EINVAL, "naga_scene_create: null argument");
+    *out = nullptr;
+    if (d->dim != 2 && d->dim != 3) return set_error(NAGA_EINVAL, "naga_scene_create: dim must be 2 or 3");
+    if (d->n_bulk < 0 || d->n_layer < 0 || d->n_boundary < 0 || d->n_ghost < 0)
+        return set_error(NAGA_EINVAL, "naga_scene_create: negative node count");
+    const int64_t N = d->n_bulk + d->n_layer + d->n_boundary + d->n_ghost;
+    const int nsys_k = d->k + d->dim + 1, nsys_b = d->k_boundary + d->dim + 1, nsys_p = d->k_probe + d->dim + 1;
+    if (d->k < d->dim + 2 || nsys_k > 64 || d->k_boundary < d->dim + 1 || nsys_b > 64 || d->k_probe < d->dim + 1 ||
+        nsys_p > 64)
+        return set_error(NAGA_EINVAL, "naga_scene_create: stencil sizes must satisfy dim + 2 <= k <= 64 - dim - 1");
+    if (N - d->n_ghost < d->k || d->n_bulk + d->n_layer < d->k_boundary || N < d->k_probe)
+        return set_error(NAGA_EINVAL, "naga_scene_create: fewer nodes than the stencil size");
+    if (N > (int64_t)0x7fffffff) return set_error(NAGA_EINVAL, "naga_scene_create: more than 2^31 - 1 nodes");
+    if (!d->points || (d->n_boundary > 0 && !d->normals) || (d->n_layer > 0 && !d->sigma) ||
+        (d->n_probes > 0 && !d->probes) || d->n_probes < 0)
+        return set_error(NAGA_EINVAL, "naga_scene_create: missing input array");
+    if (!(d->nodal_spacing > 0) || !(d->time_step > 0) || !(d->speed_of_sound > 0) || !(d->rho0 > 0) ||
+        !(d->viscosity >= 0))
+        return set_error(NAGA_EINVAL, "naga_scene_create: physical parameters must be positive");
+    if (d->shape != 0 && d->shape != 1) return set_error(NAGA_EINVAL, "naga_scene_create: unknown RBF shape");
+    if (d->pml_indexing != 0 && d->pml_indexing != 1)
+        return set_error(NAGA_EINVAL, "naga_scene_create: pml_indexing must be 0 or 1");
+    if (d->weight_precision != 0 && d->weight_precision != 1)
+        return set_error(NAGA_EINVAL, "naga_scene_create: weight_precision must be 0 or 1");
+    int rc;
+    if ((rc = check_device())) return rc;
+    auto s = std::make_unique<naga_scene>();
+    s->dim = d->dim;
+    s->Q = d->dim == 2 ? D2Q9::Q : D3Q27::Q;
+    s->QP = d->dim == 2 ? D2Q9::QP : D3Q27::QP;
+    s->desc = *d;
+    s->N = N;
+    s->nb = d->n_bulk;
+    s->nl = d->n_layer;
+    s->nbd = d->n_boundary;
+    s->ng = d->n_ghost;
+    s->nbl = s->nb + s->nl;
+    s->nd = N - s->ng;
+    s->desc.points = nullptr;
+    s->desc.normals = nullptr;
+    s->desc.sigma = nullptr;
+    s->desc.probes = nullptr;
+    if (d->n_probes > 0) s->probe_xyz.assign(d->probes, d->probes + (size_t)d->n_probes * d->dim);
+    NAGA_CUDA_TRY(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    naga_scene_desc full = *d;
+    s->desc = full;
+    rc = scene_setup(s.get());
+    s->desc.points = s->desc.normals = s->desc.sigma = s->desc.probes = nullptr;
+    if (rc) {
+        naga_scene_destroy(s.release());
+        return rc;
+    }
+    *out = s.release();
+    return NAGA_OK;
+}
+
+extern "C" int naga_scene_destroy(naga_scene* s) {
+    if (!s) return NAGA_OK;
+    if (s->owner) naga_batch_remove(s->owner, s);
+    if (s->solo) naga_batch_destroy(s->solo);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    for (void* p : s->allocs) cudaFree(p);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return NAGA_OK;
+}
+
+extern "C" void* naga_scene_stream(naga_scene* s) { return s ? (void*)active_stream(s) : nullptr; }
+
+extern "C" int naga_scene_set_density(naga_scene* s, const float* drho) {
+    if (!s) return set_error(NAGA_EINVAL, "naga_scene_set_density: null scene");
+    cudaStream_t st = active_stream(s);
+    NAGA_CUDA_TRY(cudaStreamSynchronize(st));
+    const int Q = s->Q, QP = s->QP;
+    std::vector<float> g((size_t)s->N * QP, 0.f);
+    if (drho) {
+        auto w = [&](int a) { return s->dim == 2 ? LatticeTables<D2Q9>::w(a) : LatticeTables<D3Q27>::w(a); };
+        for (int64_t i = 0; i < s->N; ++i)
+            for (int a = 0; a < Q; ++a) g[(size_t)i * QP + a] = w(a) * drho[i];
+    }
+    SceneDev& V = s->dev;
+    NAGA_CUDA_TRY(cudaMemcpyAsync(V.G, g.data(), sizeof(float) * g.size(), cudaMemcpyHostToDevice, st));
+    NAGA_CUDA_TRY(cudaMemsetAsync(V.M, 0, sizeof(float4) * s->N, st));
+    NAGA_CUDA_TRY(cudaMemsetAsync(V.Q1a, 0, sizeof(float) * s->N * QP, st));
+    NAGA_CUDA_TRY(cudaMemsetAsync(V.Q1b, 0, sizeof(float) * s->N * QP, st));
+    NAGA_CUDA_TRY(cudaMemsetAsync(V.step, 0, sizeof(unsigned long long), st));
+    NAGA_CUDA_TRY(cudaMemsetAsync(V.probe_ring, 0, sizeof(float) * V.probe_cap * std::max(1, V.np), st));
+    NAGA_CUDA_TRY(cudaStreamSynchronize(st));
+    s->steps = 0;
+    return NAGA_OK;
+}
+
+extern "C" int naga_scene_step(naga_scene* s, int nsteps) {
+    if (!s) return set_error(NAGA_EINVAL, "naga_scene_step: null scene");
+    if (s->owner) return set_error(NAGA_EINVAL, "naga_scene_step: scene belongs to a batch; step the batch");
+    if (!s->solo) {
+        s->solo = new naga_batch();
+        s->solo->dim = s->dim;
+        s->solo->is_solo = true;
+        s->solo->stream = s->stream;
+        s->solo->members.push_back(s);
+    }
+    return batch_step(s->solo, nsteps);
+}
+
+extern "C" int naga_scene_sync(naga_scene* s) {
+    if (!s) return set_error(NAGA_EINVAL, "naga_scene_sync: null scene");
+    NAGA_CUDA_TRY(cudaStreamSynchronize(active_stream(s)));
+    return NAGA_OK;
+}
+
+extern "C" int64_t naga_scene_step_count(const naga_scene* s) { return s ? s->steps : -1; }
+
+extern "C" int naga_scene_read_probes(naga_scene* s, int64_t first, int64_t count, float* out) {
+    if (!s || (!out && count > 0)) return set_error(NAGA_EINVAL, "naga_scene_read_probes: null argument");
+    const int np = s->dev.np, cap = s->dev.probe_cap;
+    if (first < 0 || count < 0 || first + count > s->steps || first < s->steps - cap)
+        return set_error(NAGA_EINVAL, "naga_scene_read_probes: requested steps are not in the probe ring");
+    if (np == 0 || count == 0) return NAGA_OK;
+    NAGA_CUDA_TRY(cudaStreamSynchronize(active_stream(s)));
+    std::vector<float> ring((size_t)cap * np);
+    NAGA_CUDA_TRY(cudaMemcpyAsync(ring.data(), s->dev.probe_ring, sizeof(float) * ring.size(), cudaMemcpyDeviceToHost, active_stream(s)));
+    NAGA_CUDA_TRY(cudaStreamSynchronize(active_stream(s)));
+    for (int64_t t = 0; t < count; ++t)
+        std::memcpy(out + t * np, ring.data() + ((first + t) % cap) * np, sizeof(float) * np);
+    return NAGA_OK;
+}
+
+extern "C" int naga_scene_read_state(naga_scene* s, float* g, float* drho) {
+    if (!s) return set_error(NAGA_EINVAL, "naga_scene_read_state: null scene");
+    NAGA_CUDA_TRY(cudaStreamSynchronize(active_stream(s)));
+    const int Q = s->Q, QP = s->QP;
+    std::vector<float> buf((size_t)s->N * QP);
+    NAGA_CUDA_TRY(cudaMemcpy(buf.data(), s->dev.G, sizeof(float) * buf.size(), cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < s->N; ++i) {
+        double r = 0;
+        for (int a = 0; a < Q; ++a) {
+            float v = buf[(size_t)i * QP + a];
+            if (g) g[i * Q + a] = v;
+            r += v;
+        }
+        if (drho) drho[i] = (float)(r * s->desc.rho0);
+    }
+    return NAGA_OK;
+}
+
+extern "C" int naga_scene_write_state(naga_scene* s, const float* g) {
+    if (!s || !g) return set_error(NAGA_EINVAL, "naga_scene_write_state: null argument");
+    NAGA_CUDA_TRY(cudaStreamSynchronize(active_stream(s)));
+    const int Q = s->Q, QP = s->QP;
+    std::vector<float> buf((size_t)s->N * QP, 0.f);
+    for (int64_t i = 0; i < s->N; ++i)
+        for (int a = 0; a < Q; ++a) buf[(size_t)i * QP + a] = g[i * Q + a];
+    cudaStream_t st = active_stream(s);
+    NAGA_CUDA_TRY(cudaMemcpyAsync(s->dev.G, buf.data(), sizeof(float) * buf.size(), cudaMemcpyHostToDevice, st));
+    NAGA_CUDA_TRY(cudaStreamSynchronize(st));
+    return NAGA_OK;
+}
+
+extern "C" int naga_scene_read_tables(naga_scene* s, uint32_t* idx, float* W, float* fw, uint32_t* bidx, float* bw,
+                                      uint32_t* pidx, float* pw) {
+    if (!s) return set_error(NAGA_EINVAL, "naga_scene_read_tables: null scene");
+    NAGA_CUDA_TRY(cudaStreamSynchronize(active_stream(s)));
+    const int k = s->desc.k, D = s->dim;
+    const int64_t N = s->N;
+    if (idx || W) {
+        std::vector<float> wv((size_t)k * N * (D == 3 ? 4 : 2));
+        std::vector<uint32_t> iv;
+        NAGA_CUDA_TRY(cudaMemcpy(wv.data(), s->dev.stW, sizeof(float) * wv.size(), cudaMemcpyDeviceToHost));
+        if (D == 2) {
+            iv.resize((size_t)k * N);
+            NAGA_CUDA_TRY(cudaMemcpy(iv.data(), s->dev.stI, sizeof(uint32_t) * iv.size(), cudaMemcpyDeviceToHost));
+        }
+        for (int64_t i = 0; i < N; ++i)
+            for (int t = 0; t < k; ++t) {
+                const size_t e = (size_t)t * N + i;
+                if (D == 3) {
+                    if (W)
+                        for (int d = 0; d < 3; ++d) W[(i * k + t) * 3 + d] = wv[e * 4 + d];
+                    if (idx) std::memcpy(&idx[i * k + t], &wv[e * 4 + 3], 4);
+                } else {
+                    if (W)
+                        for (int d = 0; d < 2; ++d) W[(i * k + t) * 2 + d] = wv[e * 2 + d];
+                    if (idx) idx[i * k + t] = iv[e];
+                }
+            }
+    }
+    if (fw) {
+        std::vector<float2> fv((size_t)k * N);
+        NAGA_CUDA_TRY(cudaMemcpy(fv.data(), s->dev.stF, sizeof(float2) * fv.size(), cudaMemcpyDeviceToHost));
+        for (int64_t i = 0; i < N; ++i)
+            for (int t = 0; t < k; ++t) fw[i * k + t] = fv[(size_t)t * N + i].x;
+    }
+    auto tr = [&](const void* dsrc_i, const float* dsrc_w, int64_t nq, int kk, uint32_t* oi, float* ow) -> int {
+        if (nq == 0) return NAGA_OK;
+        std::vector<uint32_t> ti((size_t)nq * kk);
+        std::vector<float> tw((size_t)nq * kk);
+        NAGA_CUDA_TRY(cudaMemcpy(ti.data(), dsrc_i, sizeof(uint32_t) * ti.size(), cudaMemcpyDeviceToHost));
+        NAGA_CUDA_TRY(cudaMemcpy(tw.data(), dsrc_w, sizeof(float) * tw.size(), cudaMemcpyDeviceToHost));
+        for (int64_t q = 0; q < nq; ++q)
+            for (int t = 0; t < kk; ++t) {
+                if (oi) oi[q * kk + t] = ti[(size_t)t * nq + q];
+                if (ow) ow[q * kk + t] = tw[(size_t)t * nq + q];
+            }
+        return NAGA_OK;
+    };
+    int rc;
+    if ((bidx || bw) && (rc = tr(s->dev.bidx, s->dev.bw, s->nbd, s->desc.k_boundary, bidx, bw))) return rc;
+    if ((pidx || pw) && (rc = tr(s->dev.pidx, s->dev.pw, s->dev.np, s->desc.k_probe, pidx, pw))) return rc;
+    return NAGA_OK;
+}
+
+extern "C" int64_t naga_scene_device_bytes(const naga_scene* s) { return s ? s->bytes : 0; }
+
+extern "C" int naga_scene_size(const naga_scene* s, int64_t* n, int* q) {
+    if (!s) return set_error(NAGA_EINVAL, "naga_scene_size: null scene");
+    if (n) *n = s->N;
+    if (q) *q = s->Q;
+    return NAGA_OK;
+}
+
+// --------------------------------------------------------------- batches
+extern "C" int naga_batch_create(int dim, naga_batch** out) {
+    if (!out || (dim != 2 && dim != 3)) return set_error(NAGA_EINVAL, "naga_batch_create: bad argument");
+    int rc;
+    if ((rc = check_device())) return rc;
+    auto b = new naga_batch();
+    b->dim = dim;
+    cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete b;
+        return set_error(NAGA_ECUDA, std::string("naga_batch_create: ") + cudaGetErrorString(e));
+    }
+    *out = b;
+    return NAGA_OK;
+}
+
+extern "C" int naga_batch_destroy(naga_batch* b) {
+    if (!b) return NAGA_OK;
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (!b->is_solo)
+        for (auto* s : b->members) s->owner = nullptr;
+    b->free_tables();
+    if (b->stream && !b->is_solo) cudaStreamDestroy(b->stream);
+    delete b;
+    return NAGA_OK;
+}
+
+extern "C" int naga_batch_add(naga_batch* b, naga_scene* s) {
+    if (!b || !s) return set_error(NAGA_EINVAL, "naga_batch_add: null argument");
+    if (b->is_solo) return set_error(NAGA_EINVAL, "naga_batch_add: not a user batch");
+    if (s->dim != b->dim) return set_error(NAGA_EINVAL, "naga_batch_add: lattice of the scene differs from the batch");
+    if (s->owner) return set_error(NAGA_EINVAL, "naga_batch_add: scene already belongs to a batch");
+    NAGA_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    NAGA_CUDA_TRY(cudaStreamSynchronize(b->stream));
+    s->owner = b;
+    b->members.push_back(s);
+    b->dirty = true;
+    return NAGA_OK;
+}
+
+extern "C" int naga_batch_remove(naga_batch* b, naga_scene* s) {
+    if (!b || !s) return set_error(NAGA_EINVAL, "naga_batch_remove: null argument");
+    auto it = std::find(b->members.begin(), b->members.end(), s);
+    if (it == b->members.end()) return set_error(NAGA_EINVAL, "naga_batch_remove: scene is not a member");
+    NAGA_CUDA_TRY(cudaStreamSynchronize(b->stream));
+    b->members.erase(it);
+    s->owner = nullptr;
+    b->dirty = true;
+    return NAGA_OK;
+}
+
+extern "C" int naga_batch_size(const naga_batch* b) { return b ? (int)b->members.size() : 0; }
+extern "C" void* naga_batch_stream(naga_batch* b) { return b ? (void*)b->stream : nullptr; }
+
+extern "C" int naga_batch_step(naga_batch* b, int nsteps) {
+    if (!b) return set_error(NAGA_EINVAL, "naga_batch_step: null batch");
+    return batch_step(b, nsteps);
+}
+
+extern "C" int naga_batch_sync(naga_batch* b) {
+    if (!b) return set_error(NAGA_EINVAL, "naga_batch_sync: null batch");
+    NAGA_CUDA_TRY(cudaStreamSynchronize(b->stream));
+    return NAGA_OK;
+}
+
+// --------------------------------------------------------------- profiling
+extern "C" int naga_profile_enable(int on) {
+    std::lock_guard<std::mutex> lk(g_prof.mu);
+    prof_drain();
+    g_prof.on = on != 0;
+    return NAGA_OK;
+}
+
+extern "C" int naga_profile_reset(void) {
+    std::lock_guard<std::mutex> lk(g_prof.mu);
+    prof_drain();
+    g_prof.ms.assign(g_prof.ms.size(), 0.0);
+    g_prof.launches.assign(g_prof.launches.size(), 0);
+    return NAGA_OK;
+}
+
+extern "C" int naga_profile_read(int* count, const char** names, int64_t* launches, double* ms) {
+    if (!count) return set_error(NAGA_EINVAL, "naga_profile_read: null count");
+    std::lock_guard<std::mutex> lk(g_prof.mu);
+    prof_drain();
+    const int n = std::min(*count, kernel_count());
+    for (int i = 0; i < n; ++i) {
+        if (names) names[i] = kernel_name(i);
+        if (launches) launches[i] = i < (int)g_prof.launches.size() ? g_prof.launches[i] : 0;
+        if (ms) ms[i] = i < (int)g_prof.ms.size() ? g_prof.ms[i] : 0.0;
+    }
+    *count = kernel_count();
+    return NAGA_OK;
+}

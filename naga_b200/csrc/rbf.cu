@@ -1,0 +1,562 @@
+// Radial-point-interpolation weights and the nonlocal divergence stencil,
+// built on the GPU in FP64 (or FP32 LU + FP64-residual refinement).
+//
+// NAGA builds the augmented moment matrix G0 = [[Phi, P], [P^T, 0]] per
+// support set, inverts it with cuBLAS and contracts the inverse with G_x
+// (interpolation/detail/radial_point_method.cuh:349-453). Here one warp
+// owns one support set: it assembles G0 in shared memory, factors it with
+// partial pivoting and solves for the right-hand sides directly (the
+// contraction W = G0^-T G_x equals G0^-1 G_x because G0 is symmetric).
+//
+// Coordinates are shifted to the group's centre and divided by the spacing
+// parameter before assembly. Both shape functions are radial, so this
+// leaves the interpolation weights unchanged in exact arithmetic (the RBF
+// block scales by a constant and span{1, x} is shift- and scale-invariant)
+// while it removes most of the ill-conditioning of the absolute-coordinate
+// system.
+#include "warp_lu.cuh"
+#include "scene_dev.hpp"
+
+#include <algorithm>
+#include <vector>
+
+namespace naga {
+
+namespace {
+
+// multiquadric (r^2 + (0.1 h)^2)^0.5 in units of h (radial_point_method.cuh:
+// 44-66 with q = 0.5, alpha_c = 0.1), or the cubic polyharmonic spline r^3
+__device__ __forceinline__ double shape_fn(double r2, int shape) {
+    if (shape == 0) return sqrt(r2 + 0.01);
+    double r = sqrt(r2);
+    return r * r * r;
+}
+
+template <int D>
+__device__ void build_G0(const double* xs, int k, int shape, double* G) {
+    const int n = k + D + 1;
+    for (int e = lane_id(); e < n * n; e += 32) {
+        const int i = e % n, j = e / n;
+        double v;
+        if (i >= k && j >= k)
+            v = 0.0;
+        else if (i >= k)
+            v = (i == k) ? 1.0 : xs[j * D + (i - k - 1)];
+        else if (j >= k)
+            v = (j == k) ? 1.0 : xs[i * D + (j - k - 1)];
+        else {
+            double r2 = 0;
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                double t = xs[i * D + d] - xs[j * D + d];
+                r2 += t * t;
+            }
+            v = shape_fn(r2, shape);
+        }
+        G[e] = v;
+    }
+    __syncwarp();
+}
+
+// G_x row r for the scaled query point x
+template <int D>
+__device__ __forceinline__ double gx_row(const double* xs, int k, int shape, const double* x, int r) {
+    if (r < k) {
+        double r2 = 0;
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            double t = xs[r * D + d] - x[d];
+            r2 += t * t;
+        }
+        return shape_fn(r2, shape);
+    }
+    if (r == k) return 1.0;
+    return x[r - k - 1];
+}
+
+// y = A x for x distributed over the warp (rows r = lane, lane + 32)
+__device__ void warp_matvec(const double* A, int n, double x0, double x1, double& y0, double& y1) {
+    const int lane = lane_id();
+    y0 = 0;
+    y1 = 0;
+    for (int j = 0; j < n; ++j) {
+        double xj = warp_get(x0, x1, j);
+        if (lane < n) y0 += A[lane + n * j] * xj;
+        if (lane + 32 < n) y1 += A[lane + 32 + n * j] * xj;
+    }
+}
+
+// Solves G0 x = b for the distributed right-hand side (x0, x1) in place:
+// precision 0: FP64 LU (factors in G); precision 1: FP32 LU in Gf with
+// FP64-residual refinement against G (unfactored). Returns false when the
+// refinement did not converge.
+__device__ bool solve_rhs(const double* G, const float* Gf, const int* piv, int n, int precision, double& x0,
+                          double& x1) {
+    if (precision == 0) {
+        warp_lu_solve_reg(G, n, piv, x0, x1);
+        return true;
+    }
+    const double b0 = x0, b1 = x1;
+    float f0 = (float)b0, f1 = (float)b1;
+    warp_lu_solve_reg(Gf, n, piv, f0, f1);
+    x0 = f0;
+    x1 = f1;
+    for (int it = 0; it < 30; ++it) {
+        double y0, y1;
+        warp_matvec(G, n, x0, x1, y0, y1);
+        float r0 = (float)(b0 - y0), r1 = (float)(b1 - y1);
+        warp_lu_solve_reg(Gf, n, piv, r0, r1);
+        x0 += r0;
+        x1 += r1;
+        double dm = fmax(fabs((double)r0), fabs((double)r1));
+        double xm = fmax(fabs(x0), fabs(x1));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            dm = fmax(dm, __shfl_xor_sync(kFull, dm, o));
+            xm = fmax(xm, __shfl_xor_sync(kFull, xm, o));
+        }
+        if (dm <= 1e-15 * xm) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ size_t rbf_smem_per_warp(int n, int k, int D, int precision) {
+    size_t s = (size_t)8 * n * n + (size_t)8 * k * D + 16 * ((n + 3) / 4);
+    if (precision) s += (size_t)4 * n * n + 16;
+    return (s + 15) / 16 * 16;
+}
+size_t rbf_smem_per_warp_h(int n, int k, int D, int precision) {
+    size_t s = (size_t)8 * n * n + (size_t)8 * k * D + 16 * ((n + 3) / 4);
+    if (precision) s += (size_t)4 * n * n + 16;
+    return (s + 15) / 16 * 16;
+}
+
+struct WarpSmem {
+    double* G;
+    double* xs;
+    int* piv;
+    float* Gf;
+};
+__device__ WarpSmem carve(unsigned char* base, int n, int k, int D, int precision) {
+    WarpSmem w;
+    w.G = reinterpret_cast<double*>(base);
+    w.xs = w.G + n * n;
+    w.piv = reinterpret_cast<int*>(w.xs + k * D);
+    w.Gf = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(w.piv) + 16 * ((n + 3) / 4));
+    return w;
+}
+
+// Factor G (and its FP32 copy when refining); returns the LU info.
+__device__ int factor(WarpSmem& s, int n, int precision) {
+    if (precision == 0) return warp_lu(s.G, n, s.piv);
+    for (int e = lane_id(); e < n * n; e += 32) s.Gf[e] = (float)s.G[e];
+    __syncwarp();
+    return warp_lu(s.Gf, n, s.piv);
+}
+
+template <int D>
+__global__ void rbf_weights_kernel(const float* __restrict__ src, int64_t nsrc, const uint32_t* __restrict__ support,
+                                   int k, const double* __restrict__ qry, int64_t ngroups, int group, double spacing,
+                                   int shape, int precision, double* __restrict__ weights, int* __restrict__ status,
+                                   int wpb) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int w = threadIdx.x >> 5, lane = lane_id();
+    const int n = k + D + 1;
+    WarpSmem s = carve(smem + rbf_smem_per_warp(n, k, D, precision) * w, n, k, D, precision);
+    for (int64_t g = (int64_t)blockIdx.x * wpb + w; g < ngroups; g += (int64_t)gridDim.x * wpb) {
+        double o[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) o[d] = qry[(g * group) * D + d];
+        for (int t = lane; t < k; t += 32) {
+            uint32_t j = support[g * k + t];
+            if ((int64_t)j >= nsrc) {
+                atomicOr(status, 1);
+                j = 0;
+            }
+#pragma unroll
+            for (int d = 0; d < D; ++d) s.xs[t * D + d] = ((double)src[(int64_t)j * D + d] - o[d]) / spacing;
+        }
+        __syncwarp();
+        build_G0<D>(s.xs, k, shape, s.G);
+        int info = factor(s, n, precision);
+        if (info) atomicOr(status, 2);
+        for (int q = 0; q < group; ++q) {
+            double x[D];
+#pragma unroll
+            for (int d = 0; d < D; ++d) x[d] = (qry[(g * group + q) * D + d] - o[d]) / spacing;
+            double x0 = lane < n ? gx_row<D>(s.xs, k, shape, x, lane) : 0.0;
+            double x1 = lane + 32 < n ? gx_row<D>(s.xs, k, shape, x, lane + 32) : 0.0;
+            if (!solve_rhs(s.G, s.Gf, s.piv, n, precision, x0, x1)) atomicOr(status, 4);
+            double* out = weights + (g * group + q) * k;
+            if (lane < k) out[lane] = x0;
+            if (lane + 32 < k) out[lane + 32] = x1;
+        }
+        __syncwarp();
+    }
+}
+
+// ------------------------------------------------- divergence stencil build
+// 4-point Gauss-Legendre nodes/weights with the six-digit values NAGA uses
+// (nonlocal_calculus/detail/quadrature_points.cuh:49-61).
+__constant__ double c_gl_w[4] = {0.652145, 0.652145, 0.347855, 0.347855};
+__constant__ double c_gl_x[4] = {0.339981, -0.339981, 0.861136, -0.861136};
+
+// unit quadrature offset q (quadrature_points.cuh:74-157): radius
+// (x_gl + 1) / 2; theta = t pi / 2; phi = p pi / 4 + pi / 8.
+template <int D>
+__device__ __forceinline__ void unit_quad(int q, double* u) {
+    const double r = (c_gl_x[q & 3] + 1.0) / 2.0;
+    const int t = (q >> 2) & 3;
+    double st, ct;
+    sincospi(0.5 * t, &st, &ct);
+    if (D == 2) {
+        u[0] = r * ct;
+        u[1] = r * st;
+    } else {
+        const int p = q >> 4;
+        double sp, cp;
+        sincospi((2.0 * p + 1.0) / 8.0, &sp, &cp);
+        u[0] = r * sp * ct;
+        u[1] = r * sp * st;
+        u[2] = r * cp;
+    }
+}
+
+// antisymmetric w4 B-spline kernel (nonlocal_calculus/detail/divergence.inl:
+// 55-133) and the quadrature weight of divergence.inl:171-197
+template <int D>
+__device__ __forceinline__ void kernel_and_weight(double delta, const double* xy, int q, double* a, double& wq) {
+    const double pi = 3.141592653589793;
+    double r2 = 0;
+#pragma unroll
+    for (int d = 0; d < D; ++d) r2 += xy[d] * xy[d];
+    const double r = sqrt(r2);
+    double m;
+    if (2.0 * r / delta < 1)
+        m = (D == 2 ? 240.0 / 7.0 : 48.0) * r * (2.0 * delta - 3.0 * r);
+    else if (2.0 * r / delta < 2)
+        m = (D == 2 ? 240.0 / 7.0 : 48.0) * (delta - r) * (delta - r);
+    else
+        m = 0;
+    wq = c_gl_w[q & 3] * delta / 2.0 * (2.0 * pi / 4.0);
+    if (D == 2) {
+        const double den = pi * delta * delta * delta * delta * delta;
+        a[0] = m * (xy[0] / r) / den;
+        a[1] = m * (xy[1] / r) / den;
+        wq *= r;
+    } else {
+        const double rxy = sqrt(xy[0] * xy[0] + xy[1] * xy[1]);
+        const double den = pi * delta * delta * delta * delta * delta * delta;
+        const double sp = rxy / r, cp = xy[2] / r;
+        const double ct = rxy != 0 ? xy[0] / rxy : 0, st = rxy != 0 ? xy[1] / rxy : 0;
+        a[0] = m * sp * ct / den;
+        a[1] = m * sp * st / den;
+        a[2] = m * cp / den;
+        wq *= pi / 4.0;
+        wq *= r * rxy;
+    }
+}
+
+// nearest-neighbour distance |x_i - x_{idx[i][1]}| in FP64
+template <int D>
+__global__ void nn_kernel(const float* __restrict__ pts, const uint32_t* __restrict__ idx, int k, int64_t n,
+                          double* __restrict__ nn) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t j = idx[i * k + 1];
+        double s = 0;
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            double t = (double)pts[i * D + d] - (double)pts[(int64_t)j * D + d];
+            s += t * t;
+        }
+        nn[i] = sqrt(s);
+    }
+}
+
+// mean nearest-neighbour distance per batch of `batch` consecutive nodes
+__global__ void batch_mean_kernel(const double* __restrict__ nn, int64_t n, int64_t batch, double* __restrict__ out) {
+    __shared__ double red[32];
+    const int64_t b = blockIdx.x;
+    const int64_t s = b * batch, e = min(n, s + batch);
+    double acc = 0;
+    for (int64_t i = s + threadIdx.x; i < e; i += blockDim.x) acc += nn[i];
+    acc = warp_sum(acc);
+    if (lane_id() == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+        v = warp_sum(v);
+        if (threadIdx.x == 0) out[b] = v / (double)(e - s);
+    }
+}
+
+}  // namespace
+
+namespace {
+
+template <int D>
+__global__ void divergence_build_kernel(const float* __restrict__ pts, int64_t n, const uint32_t* __restrict__ idx,
+                                        int k, const double* __restrict__ spacing, int64_t spacing_batch,
+                                        int shape, int precision, StencilOut out, int* __restrict__ status,
+                                        int wpb) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int w = threadIdx.x >> 5, lane = lane_id();
+    const int nsys = k + D + 1;
+    const int nq = D == 2 ? 16 : 64;
+    WarpSmem s = carve(smem + rbf_smem_per_warp(nsys, k, D, precision) * w, nsys, k, D, precision);
+    for (int64_t i = (int64_t)blockIdx.x * wpb + w; i < n; i += (int64_t)gridDim.x * wpb) {
+        double xi[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) xi[d] = (double)pts[i * D + d];
+        const double sp = spacing[i / spacing_batch];
+        uint32_t jl[2] = {0, 0};
+        double r2own[2] = {0, 0};
+        for (int t = lane, r = 0; t < k; t += 32, ++r) {
+            const uint32_t j = idx[i * k + t];
+            jl[r] = j;
+            double rr = 0;
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                const double xj = (double)pts[(int64_t)j * D + d];
+                s.xs[t * D + d] = (xj - xi[d]) / sp;
+                rr += (xj - xi[d]) * (xj - xi[d]);
+            }
+            r2own[r] = rr;
+        }
+        // interaction radius delta_i = 0.05 |x_i - x_nn| (operators.cuh:84-117)
+        const double delta = 0.05 * sqrt(__shfl_sync(kFull, r2own[0], 1));
+        __syncwarp();
+        build_G0<D>(s.xs, k, shape, s.G);
+        // right-hand sides b_d = sum_q alpha_d(q) w_q G_x(q), rows lane / lane+32
+        double b0[D], b1[D], cself[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) b0[d] = b1[d] = cself[d] = 0;
+        for (int q = 0; q < nq; ++q) {
+            double u[D], xy[D], a[D], xq[D], wq;
+            unit_quad<D>(q, u);
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                xy[d] = delta * u[d];
+                xq[d] = xy[d] / sp;
+            }
+            kernel_and_weight<D>(delta, xy, q, a, wq);
+            const double g0 = lane < nsys ? gx_row<D>(s.xs, k, shape, xq, lane) : 0.0;
+            const double g1 = lane + 32 < nsys ? gx_row<D>(s.xs, k, shape, xq, lane + 32) : 0.0;
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                const double aw = a[d] * wq;
+                b0[d] += aw * g0;
+                b1[d] += aw * g1;
+                cself[d] += aw;
+            }
+        }
+        const int info = factor(s, nsys, precision);
+        if (info) atomicOr(status, 2);
+        double W0[D], W1[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            double x0 = b0[d], x1 = b1[d];
+            if (!solve_rhs(s.G, s.Gf, s.piv, nsys, precision, x0, x1)) atomicOr(status, 4);
+            W0[d] = x0 + (lane == 0 ? cself[d] : 0.0);
+            W1[d] = x1;
+        }
+        // selective-filter weights: normalised Gaussian of the distance
+        // (detail/simulation_engine.cuh:1233-1323), computed once
+        double fw0 = 0, fw1 = 0;
+        if (out.Ff) {
+            const double inv2s2 = 0.5 / (out.filter_sigma * out.filter_sigma);
+            fw0 = lane < k ? exp(-r2own[0] * inv2s2) : 0.0;
+            fw1 = lane + 32 < k ? exp(-r2own[1] * inv2s2) : 0.0;
+            const double tot = warp_sum(fw0 + fw1);
+            fw0 /= tot;
+            fw1 /= tot;
+        }
+        for (int r = 0; r < 2; ++r) {
+            const int t = lane + 32 * r;
+            if (t >= k) break;
+            const double* Wt = r == 0 ? W0 : W1;
+            if (out.W64)
+#pragma unroll
+                for (int d = 0; d < D; ++d) out.W64[(i * k + t) * D + d] = Wt[d];
+            if (out.Wf) {
+                if (D == 3) {
+                    float4 v = make_float4((float)Wt[0], (float)Wt[1], (float)Wt[D - 1], __uint_as_float(jl[r]));
+                    reinterpret_cast<float4*>(out.Wf)[t * out.ld + i] = v;
+                } else {
+                    reinterpret_cast<float2*>(out.Wf)[t * out.ld + i] = make_float2((float)Wt[0], (float)Wt[1]);
+                    out.If[t * out.ld + i] = jl[r];
+                }
+            }
+            if (out.Ff) out.Ff[t * out.ld + i] = make_float2((float)(r == 0 ? fw0 : fw1), __uint_as_float(jl[r]));
+        }
+        if (out.delta && lane == 0) out.delta[i] = delta;
+        __syncwarp();
+    }
+}
+
+int warps_per_block_for(size_t per_warp) {
+    int dev = 0, v = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    size_t lim = v > 0 ? (size_t)v : 48 * 1024;
+    return (int)std::min<size_t>(8, lim / per_warp);
+}
+
+}  // namespace
+
+// RBF weights on the device; status bits: 1 bad index, 2 singular, 4 no convergence
+int rbf_weights_device(const float* src, int64_t nsrc, int dim, const uint32_t* support, int k, const double* qry,
+                       int64_t ngroups, int group, double spacing, int shape, int precision, double* weights,
+                       cudaStream_t st) {
+    const int n = k + dim + 1;
+    if (dim != 2 && dim != 3) return set_error(NAGA_EINVAL, "naga_rbf_weights: dim must be 2 or 3");
+    if (k < dim + 1 || n > 64) return set_error(NAGA_EINVAL, "naga_rbf_weights: need dim + 1 <= k <= 60");
+    if (group < 1 || ngroups < 0) return set_error(NAGA_EINVAL, "naga_rbf_weights: bad group size");
+    if (!(spacing > 0)) return set_error(NAGA_EINVAL, "naga_rbf_weights: spacing must be > 0");
+    if (shape != 0 && shape != 1) return set_error(NAGA_EINVAL, "naga_rbf_weights: unknown shape");
+    if (precision != 0 && precision != 1) return set_error(NAGA_EINVAL, "naga_rbf_weights: unknown precision");
+    if (ngroups == 0) return NAGA_OK;
+    const size_t per_warp = rbf_smem_per_warp_h(n, k, dim, precision);
+    const int wpb = warps_per_block_for(per_warp);
+    if (wpb < 1) return set_error(NAGA_EINVAL, "naga_rbf_weights: system too large");
+    int* d_status = nullptr;
+    NAGA_CUDA_TRY(cudaMallocAsync(&d_status, sizeof(int), st));
+    NAGA_CUDA_TRY(cudaMemsetAsync(d_status, 0, sizeof(int), st));
+    const int blocks = (int)std::min<int64_t>((ngroups + wpb - 1) / wpb, (int64_t)sm_count() * 32);
+    const size_t smem = per_warp * wpb;
+    if (dim == 2) {
+        NAGA_CUDA_TRY(cudaFuncSetAttribute(rbf_weights_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        rbf_weights_kernel<2><<<blocks, 32 * wpb, smem, st>>>(src, nsrc, support, k, qry, ngroups, group, spacing,
+                                                              shape, precision, weights, d_status, wpb);
+    } else {
+        NAGA_CUDA_TRY(cudaFuncSetAttribute(rbf_weights_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        rbf_weights_kernel<3><<<blocks, 32 * wpb, smem, st>>>(src, nsrc, support, k, qry, ngroups, group, spacing,
+                                                              shape, precision, weights, d_status, wpb);
+    }
+    NAGA_CUDA_TRY(cudaGetLastError());
+    int h_status = 0;
+    NAGA_CUDA_TRY(cudaMemcpyAsync(&h_status, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    NAGA_CUDA_TRY(cudaFreeAsync(d_status, st));
+    NAGA_CUDA_TRY(cudaStreamSynchronize(st));
+    if (h_status & 1) return set_error(NAGA_EINVAL, "naga_rbf_weights: support index out of range");
+    if (h_status & 2) return set_error(NAGA_ESINGULAR, "naga_rbf_weights: singular moment matrix");
+    if (h_status & 4) return set_error(NAGA_ENOCONVERGE, "naga_rbf_weights: refinement did not converge");
+    return NAGA_OK;
+}
+
+// kNN + interaction radii + MQ spacing + stencil weights for pts[0, n)
+int divergence_build_device(const float* pts, int64_t n, int dim, int k, int shape, int precision, uint32_t* idx,
+                            StencilOut out, cudaStream_t st) {
+    const int nsys = k + dim + 1;
+    if (dim != 2 && dim != 3) return set_error(NAGA_EINVAL, "divergence build: dim must be 2 or 3");
+    if (k < dim + 2 || nsys > 64) return set_error(NAGA_EINVAL, "divergence build: need dim + 2 <= k <= 60");
+    if (n < k) return set_error(NAGA_EINVAL, "divergence build: fewer points than k");
+    float* d2 = nullptr;
+    double* nn = nullptr;
+    double* sp = nullptr;
+    int* d_status = nullptr;
+    const int64_t batch = 16384;
+    const int64_t nb = (n + batch - 1) / batch;
+    NAGA_CUDA_TRY(cudaMallocAsync(&d2, sizeof(float) * n * k, st));
+    int rc = knn_device(pts, n, pts, n, dim, k, idx, d2, st);
+    if (rc) {
+        cudaFreeAsync(d2, st);
+        return rc;
+    }
+    NAGA_CUDA_TRY(cudaMallocAsync(&nn, sizeof(double) * n, st));
+    NAGA_CUDA_TRY(cudaMallocAsync(&sp, sizeof(double) * nb, st));
+    NAGA_CUDA_TRY(cudaMallocAsync(&d_status, sizeof(int), st));
+    NAGA_CUDA_TRY(cudaMemsetAsync(d_status, 0, sizeof(int), st));
+    {
+        const int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)sm_count() * 8);
+        if (dim == 2)
+            nn_kernel<2><<<blocks, 256, 0, st>>>(pts, idx, k, n, nn);
+        else
+            nn_kernel<3><<<blocks, 256, 0, st>>>(pts, idx, k, n, nn);
+        batch_mean_kernel<<<(unsigned)nb, 256, 0, st>>>(nn, n, batch, sp);
+        NAGA_CUDA_TRY(cudaGetLastError());
+    }
+    const size_t per_warp = rbf_smem_per_warp_h(nsys, k, dim, precision);
+    const int wpb = warps_per_block_for(per_warp);
+    const size_t smem = per_warp * wpb;
+    const int blocks = (int)std::min<int64_t>((n + wpb - 1) / wpb, (int64_t)sm_count() * 32);
+    if (dim == 2) {
+        NAGA_CUDA_TRY(cudaFuncSetAttribute(divergence_build_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        divergence_build_kernel<2><<<blocks, 32 * wpb, smem, st>>>(pts, n, idx, k, sp, batch, shape, precision, out,
+                                                                   d_status, wpb);
+    } else {
+        NAGA_CUDA_TRY(cudaFuncSetAttribute(divergence_build_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        divergence_build_kernel<3><<<blocks, 32 * wpb, smem, st>>>(pts, n, idx, k, sp, batch, shape, precision, out,
+                                                                   d_status, wpb);
+    }
+    NAGA_CUDA_TRY(cudaGetLastError());
+    int h_status = 0;
+    NAGA_CUDA_TRY(cudaMemcpyAsync(&h_status, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    NAGA_CUDA_TRY(cudaStreamSynchronize(st));
+    cudaFreeAsync(d2, st);
+    cudaFreeAsync(nn, st);
+    cudaFreeAsync(sp, st);
+    cudaFreeAsync(d_status, st);
+    if (h_status & 2) return set_error(NAGA_ESINGULAR, "divergence build: singular moment matrix");
+    if (h_status & 4) return set_error(NAGA_ENOCONVERGE, "divergence build: refinement did not converge");
+    return NAGA_OK;
+}
+
+}  // namespace naga
+
+using namespace naga;
+
+extern "C" int naga_rbf_weights(const float* src, int64_t n, int dim, const uint32_t* support, int k,
+                                const double* qry, int64_t ngroups, int group, double spacing, int shape,
+                                int precision, double* weights, void* stream) {
+    if (ngroups > 0 && (!src || !support || !qry || !weights))
+        return set_error(NAGA_EINVAL, "naga_rbf_weights: null pointer");
+    return rbf_weights_device(src, n, dim, support, k, qry, ngroups, group, spacing, shape, precision, weights,
+                              (cudaStream_t)stream);
+}
+
+extern "C" int naga_divergence_build(const float* pts, int64_t n, int dim, int k, int shape, int precision,
+                                     uint32_t* idx, double* W, double* delta, void* stream) {
+    if (!pts || !idx) return set_error(NAGA_EINVAL, "naga_divergence_build: null pointer");
+    StencilOut out{};
+    out.W64 = W;
+    out.delta = delta;
+    return divergence_build_device(pts, n, dim, k, shape, precision, idx, out, (cudaStream_t)stream);
+}
+
+namespace naga {
+namespace {
+template <int D>
+__global__ void divergence_apply_kernel(const float* __restrict__ W, const uint32_t* __restrict__ idx, int64_t n,
+                                        int k, const float* __restrict__ field, float* __restrict__ out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        float acc = 0.f;
+        for (int s = 0; s < k; ++s) {
+            const uint32_t j = idx[i * k + s];
+            float t = 0.f;
+#pragma unroll
+            for (int d = 0; d < D; ++d) t = fmaf(W[(i * k + s) * D + d], field[(int64_t)j * D + d], t);
+            acc += t;
+        }
+        out[i] = acc;
+    }
+}
+}  // namespace
+}  // namespace naga
+
+// Generic gather of a vector field through a stored stencil (the default
+// path of divergence_operator::apply, nonlocal_calculus/divergence.cuh:377-488).
+extern "C" int naga_divergence_apply(const float* W, const uint32_t* idx, int64_t n, int dim, int k,
+                                     const float* field, float* result, void* stream) {
+    if (n < 0 || k < 1 || (dim != 2 && dim != 3)) return set_error(NAGA_EINVAL, "naga_divergence_apply: bad sizes");
+    if (n == 0) return NAGA_OK;
+    if (!W || !idx || !field || !result) return set_error(NAGA_EINVAL, "naga_divergence_apply: null pointer");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)sm_count() * 8);
+    if (dim == 2)
+        divergence_apply_kernel<2><<<blocks, 256, 0, st>>>(W, idx, n, k, field, result);
+    else
+        divergence_apply_kernel<3><<<blocks, 256, 0, st>>>(W, idx, n, k, field, result);
+    NAGA_CUDA_TRY(cudaGetLastError());
+    return NAGA_OK;
+}

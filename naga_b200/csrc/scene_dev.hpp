@@ -1,0 +1,114 @@
+// Device-resident description of one scene, as the step kernels see it.
+//
+// HBM layout of a scene with N nodes (order: bulk [0, nb), layer
+// [nb, nb + nl), boundary [nbl, nbl + nbd), ghost [.., N)):
+//   populations   G, G1, G2, ACC, S1, S1P: node-major rows of QP floats
+//                 (QP = 28 for D3Q27, 12 for D2Q9), centred: g = f - w
+//   Q1a, Q1b      PML trapezoid integrals, rows of QP floats, ping-pong
+//                 by step parity
+//   M             float4 per node: (rho - 1, ux, uy, uz) in lattice units
+//   stencil       [k][N] records: D3Q27 float4 (Wx, Wy, Wz, index bits);
+//                 D2Q9 float2 (Wx, Wy) + uint32 index
+//   filter        [k][N] float2 (normalised Gaussian weight, index bits)
+//   boundary      [kb][nbd] indices + weights; probes [kp][np]
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace naga {
+
+struct SceneDev {
+    int64_t N, nb, nl, nbd, ng, nbl;
+    int k, kb, kp, np;
+    int pml_shift;  // index offset of the layer's Q reads (n_bulk as NAGA, or 0)
+    int probe_cap;
+    int n_all_items;
+    int _pad0;
+    // lattice-unit parameters, FP32 as the reference computes them
+    float dt_lat;     // lattice time step
+    float om_ab;      // viscosity-dependent relaxation rate
+    float om_fix[6];  // D3Q27 fixed higher-order rates (1.5, 1.83, 1.4, 1.61, 1.98, 1.74)
+    float inv_dt;     // 1 / dt_lat
+    float rho0;
+    float a_half, a_full, b1, b2;  // RK4 coefficients dt/2, dt, 1/6, 2/6
+    float half_dt;                 // dt_lat / 2 of the PML trapezoid rule
+    float _pad1;
+    // state
+    float* G;
+    float* G1;
+    float* G2;
+    float* ACC;
+    float* S1;
+    float* S1P;
+    float* Q1a;
+    float* Q1b;
+    float4* M;
+    // tables
+    const void* stW;
+    const uint32_t* stI;
+    const float2* stF;
+    const float* sigma;
+    const float* normals;
+    const uint32_t* bidx;
+    const float* bw;
+    const uint32_t* pidx;
+    const float* pw;
+    const uint8_t* is_src;
+    // outputs / bookkeeping
+    float* probe_ring;
+    double* partials;  // [n_all_items][2 Q]
+    float* means;      // [2 Q]
+    unsigned long long* step;
+};
+
+struct WorkItem {
+    uint32_t scene;
+    uint32_t begin;
+    uint32_t end;
+    uint32_t local;  // index of the item among its scene's items of the same range kind
+};
+
+}  // namespace naga
+
+namespace naga {
+
+// Output targets of the divergence-stencil build; any pointer may be null.
+struct StencilOut {
+    double* W64;          // [n][k][D], FP64
+    double* delta;        // [n]
+    float* Wf;            // scene layout: D == 3 float4 [k][ld] (Wx, Wy, Wz, idx); D == 2 float2 [k][ld]
+    uint32_t* If;         // D == 2: [k][ld]
+    float2* Ff;           // filter (w, idx bits) [k][ld]
+    int64_t ld;           // leading dimension of the scene layout
+    double filter_sigma;  // Gaussian sigma of the selective filter (h / 2.5)
+};
+
+// One step's launch parameters for a batch of scenes.
+struct StepLaunch {
+    const SceneDev* scenes;
+    int nscenes;
+    const WorkItem* all;
+    int n_all;
+    const WorkItem* fluid;
+    int n_fluid;
+    const WorkItem* edge;
+    int n_edge;
+};
+
+int enqueue_step(int dim, const StepLaunch& P, cudaStream_t st);
+const char* kernel_name(int id);
+int kernel_count();
+void prof_begin(int id, cudaStream_t st);
+void prof_end(int id, cudaStream_t st);
+bool prof_on();
+int knn_device(const float* src, int64_t n, const float* qry, int64_t nq, int dim, int k, uint32_t* idx,
+               float* d2, cudaStream_t st);
+int rbf_weights_device(const float* src, int64_t nsrc, int dim, const uint32_t* support, int k, const double* qry,
+                       int64_t ngroups, int group, double spacing, int shape, int precision, double* weights,
+                       cudaStream_t st);
+int divergence_build_device(const float* pts, int64_t n, int dim, int k, int shape, int precision, uint32_t* idx,
+                            StencilOut out, cudaStream_t st);
+int batched_inverse(const double* A, double* Ainv, int n, int64_t batch, int* info, bool refined, int max_iter,
+                    double tol, cudaStream_t st);
+
+}  // namespace naga

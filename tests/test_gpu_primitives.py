@@ -1,0 +1,150 @@
+"""GPU set-up primitives through the C ABI against the CPU oracle:
+bit-exact kNN, batched inverses, RBF weights and the divergence stencil."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _t(a):
+    import torch
+
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def _np(t):
+    import torch
+
+    torch.cuda.synchronize()
+    return t.cpu().numpy()
+
+
+def _cloud(dim, seed):
+    rng = np.random.default_rng(seed)
+    m = 9 if dim == 3 else 30
+    lat = np.stack(np.meshgrid(*[np.arange(m)] * dim, indexing="ij"), -1).reshape(-1, dim) / m
+    pts = np.concatenate([lat, rng.random((3000, dim)), lat[:20]]).astype(np.float32)
+    qry = np.concatenate([pts[::5], rng.random((300, dim)) * 1.4 - 0.2]).astype(np.float32)
+    return pts, qry
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("k", [1, 16, 32, 48, 64])
+def test_knn_bit_exact(naga, oracle, dim, k):
+    pts, qry = _cloud(dim, 10 + dim)
+    idx, d2 = naga.knn(_t(pts), _t(qry), k)
+    oi, od = oracle.knn(pts, qry, k)
+    assert np.array_equal(_np(idx).view(np.uint32), oi)
+    assert np.array_equal(_np(d2), od)
+
+
+def test_knn_golden_validation_grid(naga, golden_dir):
+    g = json.load(open(os.path.join(golden_dir, "knn_validation_3d.json")))
+    n1, h, k = g["grid_size"], np.float32(g["spacing"]), g["k"]
+    i = np.arange(n1 ** 3)
+    grid = np.stack([(i % n1).astype(np.float32) * h, ((i // n1) % n1).astype(np.float32) * h,
+                     (i // n1 // n1).astype(np.float32) * h], 1).astype(np.float32)
+    idx, _ = naga.knn(_t(grid), _t(np.array(g["queries"], np.float32)), k)
+    assert np.array_equal(_np(idx), np.array(g["neighbours"], np.int32))
+
+
+def test_knn_clouds_batched(naga, oracle):
+    rng = np.random.default_rng(5)
+    sizes = [40, 500, 3000, 64, 1200]
+    clouds = [rng.random((n, 3)).astype(np.float32) for n in sizes]
+    off = np.concatenate([[0], np.cumsum(sizes)])
+    idx, d2 = naga.knn_clouds(_t(np.concatenate(clouds)), off, 32)
+    idx, d2 = _np(idx), _np(d2)
+    for c, pts in enumerate(clouds):
+        oi, od = oracle.knn(pts, pts, 32)
+        assert np.array_equal(idx[off[c]:off[c + 1]].view(np.uint32), oi)
+        assert np.array_equal(d2[off[c]:off[c + 1]], od)
+
+
+def test_inverse_golden(naga, golden_dir):
+    g = json.load(open(os.path.join(golden_dir, "inverse_3x3.json")))
+    A = np.repeat(np.array(g["A"]).T[None], 1000, 0)
+    out, info = naga.batched_inverse_f64(_t(A))
+    out = _np(out)
+    assert (_np(info) == 0).all()
+    assert np.abs(out.transpose(0, 2, 1) - np.array(g["A_inv"])[None]).max() <= g["tol"]
+
+
+def _rbf_systems(n_sys, seed=0):
+    """36 x 36 augmented PHS r^3 moment matrices of random k = 32 stencils in
+    a jittered cube, centred and scaled as the library assembles them."""
+    rng = np.random.default_rng(seed)
+    pts = rng.random((20000, 3)).astype(np.float32)
+    from oracle import oracle as O
+
+    centres = rng.integers(0, len(pts), n_sys)
+    idx, _ = O.knn(pts, pts[centres], 32)
+    X = pts.astype(np.float64)[idx] - pts.astype(np.float64)[centres][:, None]
+    X /= np.abs(X).max(axis=(1, 2), keepdims=True)
+    r = np.sqrt(((X[:, :, None] - X[:, None]) ** 2).sum(-1))
+    G = np.zeros((n_sys, 36, 36))
+    G[:, :32, :32] = r ** 3
+    G[:, :32, 32] = G[:, 32, :32] = 1
+    G[:, :32, 33:] = X
+    G[:, 33:, :32] = X.transpose(0, 2, 1)
+    return G  # symmetric: column-major storage equals row-major
+
+
+@pytest.mark.parametrize("n", [3, 19, 36, 64])
+def test_inverse_matches_oracle(naga, oracle, n):
+    rng = np.random.default_rng(n)
+    A = rng.standard_normal((300, n, n)) + 3 * np.eye(n)
+    out, info = naga.batched_inverse_f64(_t(A))
+    ref, rinfo = oracle.batched_inverse(A)
+    assert (_np(info) == 0).all()
+    err = np.abs(_np(out) - ref).max() / np.abs(ref).max()
+    assert err < 1e-12
+
+
+def test_inverse_rbf_systems_f64_and_refined(naga, oracle):
+    A = _rbf_systems(500)
+    ref, _ = oracle.batched_inverse(A)
+    out, info = naga.batched_inverse_f64(_t(A))
+    e64 = np.abs(_np(out) - ref).max(axis=(1, 2)) / np.abs(ref).max(axis=(1, 2))
+    assert (_np(info) == 0).all() and e64.max() < 1e-9
+    outr, infor = naga.batched_inverse_f32r(_t(A), max_iter=30, rel_tol=1e-14)
+    er = np.abs(_np(outr) - ref).max(axis=(1, 2)) / np.abs(ref).max(axis=(1, 2))
+    ok = _np(infor) == 0
+    # converged systems agree with FP64; the rest are flagged, never silent
+    assert er[ok].max() < 1e-9
+    assert set(np.unique(_np(infor))) <= {0, -1}
+
+
+@pytest.mark.parametrize("dim,shape,precision", [(2, 0, 0), (2, 1, 0), (3, 0, 0), (3, 1, 0), (3, 1, 1)])
+def test_rbf_weights_match_oracle(naga, oracle, dim, shape, precision):
+    rng = np.random.default_rng(dim * 10 + shape)
+    m = 14 if dim == 3 else 40
+    h = 1.0 / (m - 1)
+    g = np.stack(np.meshgrid(*[np.arange(m) * h] * dim, indexing="ij"), -1).reshape(-1, dim)
+    pts = (g + rng.uniform(-0.25 * h, 0.25 * h, g.shape)).astype(np.float32)
+    k = 32 if dim == 3 else 16
+    qry = rng.random((400, dim)) * 0.9 + 0.05
+    sup, _ = oracle.knn(pts, qry.astype(np.float32), k)
+    w = _np(naga.rbf_weights(_t(pts), _t(sup.astype(np.int32)), _t(qry), 1, h, shape, precision))
+    ref = oracle.rbf_weights(pts, sup, qry, 1, h, shape)
+    err = np.abs(w - ref).max() / np.abs(ref).max()
+    assert err < 1e-10
+
+
+@pytest.mark.parametrize("dim,shape", [(2, 1), (3, 0), (3, 1)])
+def test_divergence_stencil_matches_oracle(naga, oracle, dim, shape):
+    m = 14 if dim == 3 else 40
+    rng = np.random.default_rng(7)
+    h = 1.0 / (m - 1)
+    g = np.stack(np.meshgrid(*[np.arange(m) * h] * dim, indexing="ij"), -1).reshape(-1, dim)
+    pts = (g + rng.uniform(-0.25 * h, 0.25 * h, g.shape)).astype(np.float32)
+    k = 32 if dim == 3 else 16
+    idx, W, delta = naga.divergence_build(_t(pts), k, shape)
+    oi, oW, od = oracle.divergence_stencil(pts, k, shape)
+    assert np.array_equal(_np(idx).view(np.uint32), oi)
+    err = np.abs(_np(W) - oW).max() / np.abs(oW).max()
+    assert err < 1e-9
+    assert np.abs(_np(delta) - od).max() / od.max() < 1e-14

@@ -1,0 +1,117 @@
+"""The CUDA time step (FP32, centred populations) against the FP64 oracle of
+the same step: set-up tables, single steps, probe traces, batches."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+PROBES2 = np.array([[0.3, 0.5], [0.7, 0.5], [0.5, 0.3], [0.5, 0.7]], np.float32)
+PROBES3 = np.array([[x, y, z] for z in (0.35, 0.65) for y in (0.35, 0.65) for x in (0.35, 0.65)],
+                   np.float32)
+
+
+def pair(naga, oracle, dim, n_side, layers, seed=0, shape=None, pml_indexing=0, width=0.05,
+         n_ghost=0, sigma_peak=0.1):
+    g = naga.generate_grid(dim, n_side, layers, seed, sigma_peak=sigma_peak)
+    if n_ghost:
+        rng = np.random.default_rng(seed)
+        extra = rng.random((n_ghost, dim)).astype(np.float32) * 0.9 + 0.05
+        g["points"] = np.concatenate([g["points"], extra]).astype(np.float32)
+    k = 16 if dim == 2 else 32
+    shape = (1 if dim == 2 else 0) if shape is None else shape
+    probes = PROBES2 if dim == 2 else PROBES3
+    gpu = naga.Scene(g, k=k, shape=shape, pml_indexing=pml_indexing, probes=probes, n_ghost=n_ghost)
+    orc = oracle.Scene(dim, g["points"], g["n_bulk"], g["n_layer"], g["n_boundary"], g["normals"],
+                       g["sigma"], g["h"], k=k, shape=shape, pml_indexing=pml_indexing,
+                       probes=probes, n_ghost=n_ghost)
+    drho = naga.gaussian_pulse(g["points"], [0.5] * dim, 1e-3, width)
+    gpu.set_density(drho)
+    orc.set_density(drho)
+    return gpu, orc, g
+
+
+def rel_err(a, b):
+    return float(np.abs(np.asarray(a, np.float64) - b).max() / np.abs(b).max())
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_setup_tables_match_oracle(naga, oracle, dim):
+    gpu, orc, g = pair(naga, oracle, dim, 30 if dim == 2 else 14, 3)
+    t, o = gpu.tables(), orc.tables()
+    nd = gpu.N
+    assert np.array_equal(t["idx"][:nd], o["idx"][:nd])
+    assert rel_err(t["W"], o["W"]) < 1e-6
+    assert rel_err(t["fw"], o["fw"]) < 1e-6
+    assert np.array_equal(t["bidx"], o["bidx"])
+    assert rel_err(t["bw"], o["bw"]) < 1e-6
+    assert np.array_equal(t["pidx"], o["pidx"])
+    assert rel_err(t["pw"], o["pw"]) < 1e-6
+
+
+@pytest.mark.parametrize("dim,pml_indexing", [(2, 0), (2, 1), (3, 0)])
+def test_single_steps_match_oracle(naga, oracle, dim, pml_indexing):
+    gpu, orc, _ = pair(naga, oracle, dim, 30 if dim == 2 else 14, 3, pml_indexing=pml_indexing,
+                       width=0.1)
+    for n in range(3):
+        gpu.step(1)
+        orc.step(1)
+        gg, _ = gpu.state()
+        go, _ = orc.state()
+        assert rel_err(gg, go) < 1e-5, n
+
+
+@pytest.mark.parametrize("dim,n_side,layers,steps", [(2, 40, 4, 200), (3, 16, 3, 60)])
+def test_probe_trace_matches_oracle(naga, oracle, dim, n_side, layers, steps):
+    gpu, orc, _ = pair(naga, oracle, dim, n_side, layers, width=0.08)
+    gpu.step(steps)
+    po = orc.step(steps)
+    pg = gpu.probes(0, steps)
+    assert rel_err(pg, po) <= 1e-5
+
+
+def test_ghost_nodes_match_oracle(naga, oracle):
+    gpu, orc, _ = pair(naga, oracle, 2, 30, 3, n_ghost=7, width=0.1)
+    gpu.step(5)
+    orc.step(5)
+    assert rel_err(gpu.state()[0], orc.state()[0]) < 1e-5
+
+
+@pytest.mark.slow
+def test_config1_probe_trace_500_steps(naga, oracle):
+    """2-D D2Q9, 20,164 jittered nodes (h = 1/141, seed 0), k = 16, r^3 RBF,
+    10-layer PML, Gaussian pulse (1e-3, width 0.05), dt = 0.5 h / c, 500
+    steps, 4 probes: probe error <= 1e-5 against the FP64 oracle."""
+    gpu, orc, _ = pair(naga, oracle, 2, 142, 10, seed=0, width=0.05)
+    gpu.step(500)
+    po = orc.step(500)
+    assert rel_err(gpu.probes(0, 500), po) <= 1e-5
+
+
+def test_batch_equals_individual_scenes(naga, oracle):
+    gs = [naga.generate_grid(2, n, 3, s) for n, s in ((25, 1), (33, 2), (41, 3))]
+    solo, members = [], []
+    for g in gs:
+        for lst in (solo, members):
+            s = naga.Scene(g, k=16, probes=PROBES2)
+            s.set_density(naga.gaussian_pulse(g["points"], [0.5, 0.5], 1e-3, 0.08))
+            lst.append(s)
+    b = naga.Batch(2)
+    for s in members:
+        b.add(s)
+    b.step(25)
+    for s in solo:
+        s.step(25)
+    for a, m in zip(solo, members):
+        assert np.array_equal(a.probes(0, 25), m.probes(0, 25))
+        assert np.array_equal(a.state()[0], m.state()[0])
+    b.close()
+
+
+def test_step_is_deterministic(naga, oracle):
+    a, _, g = pair(naga, oracle, 3, 14, 3)
+    b = naga.Scene(g, k=32, shape=0, probes=PROBES3)
+    b.set_density(naga.gaussian_pulse(g["points"], [0.5] * 3, 1e-3, 0.05))
+    a.step(10)
+    b.step(10)
+    assert np.array_equal(a.state()[0], b.state()[0])
+    assert np.array_equal(a.probes(), b.probes())
