@@ -105,9 +105,11 @@ int naga_knn_clouds(const float* pts, const int64_t* offsets, int n_clouds,
 int naga_batched_inverse_f64(const double* A, double* A_inv, int n,
                              int64_t batch, int* info, void* stream);
 /* Same result computed from an FP32 LU with FP64-residual iterative
- * refinement of each column; iterations stop at max_iter or when the
- * correction is below rel_tol relative to the column. info: as above, or
- * -1 when a column did not converge.                                        */
+ * refinement of each column; a column stops at max_iter, when its
+ * correction is below rel_tol relative to the column, or when the
+ * correction stops shrinking (the FP64 residual's floor). info: as above,
+ * or -1 when some column ended with a correction above both rel_tol and
+ * 1e-10 of the column.                                                      */
 int naga_batched_inverse_f32r(const double* A, double* A_inv, int n,
                               int64_t batch, int max_iter, double rel_tol,
                               int* info, void* stream);
@@ -126,6 +128,11 @@ int naga_rbf_weights(const float* src, int64_t n, int dim,
                      const uint32_t* support, int k, const double* qry,
                      int64_t ngroups, int group, double spacing, int shape,
                      int precision, double* weights, void* stream);
+
+/* Number of systems of the calling thread's last naga_rbf_weights /
+ * naga_divergence_build / scene set-up with precision 1 whose FP32
+ * refinement did not reach 1e-10 and were re-solved in FP64.                */
+int64_t naga_refinement_fallbacks(void);
 
 /* Nonlocal divergence stencil over the points pts [n][dim] (device):
  * idx [n][k] (kNN), W [n][k][dim] (FP64) with W(d,s,i) the weight of

@@ -72,6 +72,7 @@ _SIGS = {
                                    C.c_void_p, C.c_void_p], C.c_int),
     "naga_rbf_weights": ([C.c_void_p, C.c_int64, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int64,
                           C.c_int, C.c_double, C.c_int, C.c_int, C.c_void_p, C.c_void_p], C.c_int),
+    "naga_refinement_fallbacks": ([], C.c_int64),
     "naga_divergence_build": ([C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
                                C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "naga_divergence_apply": ([C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_void_p,
@@ -380,6 +381,11 @@ def rbf_weights(src, support, qry, group: int, spacing: float, shape: int, preci
                                   _dptr(qry), ng, group, spacing, shape, precision, _dptr(w),
                                   _stream_ptr()))
     return w
+
+
+def refinement_fallbacks() -> int:
+    """Systems of this thread's last refined-precision solve re-done in FP64."""
+    return int(lib().naga_refinement_fallbacks())
 
 
 def divergence_build(pts, k: int, shape: int, precision: int = 0):

@@ -92,7 +92,7 @@ struct naga_scene {
     SceneDev dev{};
     std::vector<void*> allocs;
     int64_t bytes = 0;
-    std::vector<WorkItem> items_all, items_fluid, items_edge;  // scene slot 0
+    std::vector<WorkItem> items_all, items_fluid, items_edge, items_pml;  // scene slot 0
     naga_batch* owner = nullptr;                               // user batch, if any
     naga_batch* solo = nullptr;                                // private batch for naga_scene_step
     int64_t steps = 0;                                         // host mirror of the device counter
@@ -121,8 +121,9 @@ struct naga_batch {
     bool dirty = true;
     cudaStream_t stream = nullptr;
     SceneDev* d_scenes = nullptr;
-    WorkItem *d_all = nullptr, *d_fluid = nullptr, *d_edge = nullptr;
-    int n_all = 0, n_fluid = 0, n_edge = 0;
+    WorkItem *d_all = nullptr, *d_fluid = nullptr, *d_edge = nullptr, *d_pml = nullptr;
+    int n_all = 0, n_fluid = 0, n_edge = 0, n_pml = 0;
+    int k = 0;  // common stencil size of the members (0 if they differ)
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
 
@@ -135,8 +136,9 @@ struct naga_batch {
         if (d_all) cudaFree(d_all);
         if (d_fluid) cudaFree(d_fluid);
         if (d_edge) cudaFree(d_edge);
+        if (d_pml) cudaFree(d_pml);
         d_scenes = nullptr;
-        d_all = d_fluid = d_edge = nullptr;
+        d_all = d_fluid = d_edge = d_pml = nullptr;
     }
 };
 
@@ -160,6 +162,9 @@ void make_items(int64_t begin, int64_t end, std::vector<WorkItem>& out) {
     for (int64_t b = begin; b < end; b += 128)
         out.push_back({0u, (uint32_t)b, (uint32_t)std::min<int64_t>(end, b + 128), local++});
 }
+
+// slot of population a in a node row (paired order, see common.cuh)
+int slot_of(int dim, int a) { return dim == 2 ? D2Q9::pos(a) : D3Q27::pos(a); }
 
 float lattice_cs_f() { return 0.57735026918962576450914878050196f; }
 
@@ -364,14 +369,30 @@ int scene_setup(naga_scene* s) {
     make_items(0, N, s->items_all);
     make_items(0, s->nbl, s->items_fluid);
     make_items(s->nbl, N, s->items_edge);
+    // bulk/layer items with at least one stencil support in the layer
+    s->items_pml.clear();
+    if (s->nl > 0) {
+        std::vector<uint32_t> hidx((size_t)s->nd * k);
+        NAGA_CUDA_TRY(cudaMemcpyAsync(hidx.data(), knn_idx, sizeof(uint32_t) * hidx.size(), cudaMemcpyDeviceToHost, st));
+        NAGA_CUDA_TRY(cudaStreamSynchronize(st));
+        for (const WorkItem& it : s->items_fluid) {
+            bool touch = false;
+            for (uint32_t i = it.begin; i < it.end && !touch; ++i)
+                for (int t = 0; t < k && !touch; ++t) {
+                    const int64_t j = hidx[(size_t)i * k + t];
+                    touch = j >= s->nb && j < s->nb + s->nl;
+                }
+            if (touch) s->items_pml.push_back(it);
+        }
+    }
     V.n_all_items = (int)s->items_all.size();
     double* partials = nullptr;
-    if ((rc = s->alloc(&partials, (int64_t)V.n_all_items * 2 * s->Q))) return rc;
-    NAGA_CUDA_TRY(cudaMemsetAsync(partials, 0, sizeof(double) * V.n_all_items * 2 * s->Q, st));
+    if ((rc = s->alloc(&partials, (int64_t)V.n_all_items * 2 * QP))) return rc;
+    NAGA_CUDA_TRY(cudaMemsetAsync(partials, 0, sizeof(double) * V.n_all_items * 2 * QP, st));
     V.partials = partials;
     float* means = nullptr;
-    if ((rc = s->alloc(&means, 2 * s->Q))) return rc;
-    NAGA_CUDA_TRY(cudaMemsetAsync(means, 0, sizeof(float) * 2 * s->Q, st));
+    if ((rc = s->alloc(&means, 2 * QP))) return rc;
+    NAGA_CUDA_TRY(cudaMemsetAsync(means, 0, sizeof(float) * 2 * QP, st));
     V.means = means;
     unsigned long long* step = nullptr;
     if ((rc = s->alloc(&step, 1))) return rc;
@@ -384,10 +405,16 @@ int scene_setup(naga_scene* s) {
 int batch_rebuild(naga_batch* b) {
     b->free_tables();
     std::vector<SceneDev> sd;
-    std::vector<WorkItem> all, fluid, edge;
+    std::vector<WorkItem> all, fluid, edge, pml;
+    b->k = b->members.empty() ? 0 : b->members[0]->desc.k;
     for (size_t t = 0; t < b->members.size(); ++t) {
         naga_scene* s = b->members[t];
+        if (s->desc.k != b->k) b->k = 0;
         sd.push_back(s->dev);
+        for (auto it : s->items_pml) {
+            it.scene = (uint32_t)t;
+            pml.push_back(it);
+        }
         for (auto it : s->items_all) {
             it.scene = (uint32_t)t;
             all.push_back(it);
@@ -404,6 +431,7 @@ int batch_rebuild(naga_batch* b) {
     b->n_all = (int)all.size();
     b->n_fluid = (int)fluid.size();
     b->n_edge = (int)edge.size();
+    b->n_pml = (int)pml.size();
     auto up = [&](auto** dst, const auto& v) -> int {
         using T = typename std::remove_reference<decltype(v)>::type::value_type;
         size_t bytes = sizeof(T) * std::max<size_t>(v.size(), 1);
@@ -418,6 +446,7 @@ int batch_rebuild(naga_batch* b) {
     if ((rc = up(&b->d_all, all))) return rc;
     if ((rc = up(&b->d_fluid, fluid))) return rc;
     if ((rc = up(&b->d_edge, edge))) return rc;
+    if ((rc = up(&b->d_pml, pml))) return rc;
     b->dirty = false;
     return NAGA_OK;
 }
@@ -432,6 +461,8 @@ StepLaunch launch_of(naga_batch* b) {
     P.n_fluid = b->n_fluid;
     P.edge = b->d_edge;
     P.n_edge = b->n_edge;
+    P.pml = b->d_pml;
+    P.n_pml = b->n_pml;
     return P;
 }
 
@@ -443,11 +474,11 @@ int batch_step(naga_batch* b, int nsteps) {
     StepLaunch P = launch_of(b);
     if (prof_on()) {
         for (int n = 0; n < nsteps; ++n)
-            if ((rc = enqueue_step(b->dim, P, b->stream))) return rc;
+            if ((rc = enqueue_step(b->dim, b->k, P, b->stream))) return rc;
     } else {
         if (!b->exec) {
             NAGA_CUDA_TRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-            rc = enqueue_step(b->dim, P, b->stream);
+            rc = enqueue_step(b->dim, b->k, P, b->stream);
             cudaGraph_t g = nullptr;
             cudaError_t e = cudaStreamEndCapture(b->stream, &g);
             if (rc) {
@@ -546,7 +577,7 @@ extern "C" int naga_scene_set_density(naga_scene* s, const float* drho) {
     if (drho) {
         auto w = [&](int a) { return s->dim == 2 ? LatticeTables<D2Q9>::w(a) : LatticeTables<D3Q27>::w(a); };
         for (int64_t i = 0; i < s->N; ++i)
-            for (int a = 0; a < Q; ++a) g[(size_t)i * QP + a] = w(a) * drho[i];
+            for (int a = 0; a < Q; ++a) g[(size_t)i * QP + slot_of(s->dim, a)] = w(a) * drho[i];
     }
     SceneDev& V = s->dev;
     NAGA_CUDA_TRY(cudaMemcpyAsync(V.G, g.data(), sizeof(float) * g.size(), cudaMemcpyHostToDevice, st));
@@ -605,7 +636,7 @@ extern "C" int naga_scene_read_state(naga_scene* s, float* g, float* drho) {
     for (int64_t i = 0; i < s->N; ++i) {
         double r = 0;
         for (int a = 0; a < Q; ++a) {
-            float v = buf[(size_t)i * QP + a];
+            float v = buf[(size_t)i * QP + slot_of(s->dim, a)];
             if (g) g[i * Q + a] = v;
             r += v;
         }
@@ -620,7 +651,7 @@ extern "C" int naga_scene_write_state(naga_scene* s, const float* g) {
     const int Q = s->Q, QP = s->QP;
     std::vector<float> buf((size_t)s->N * QP, 0.f);
     for (int64_t i = 0; i < s->N; ++i)
-        for (int a = 0; a < Q; ++a) buf[(size_t)i * QP + a] = g[i * Q + a];
+        for (int a = 0; a < Q; ++a) buf[(size_t)i * QP + slot_of(s->dim, a)] = g[i * Q + a];
     cudaStream_t st = active_stream(s);
     NAGA_CUDA_TRY(cudaMemcpyAsync(s->dev.G, buf.data(), sizeof(float) * buf.size(), cudaMemcpyHostToDevice, st));
     NAGA_CUDA_TRY(cudaStreamSynchronize(st));

@@ -66,6 +66,9 @@ __global__ void inverse_f32r_kernel(const double* __restrict__ A, double* __rest
         warp_lu_inverse(LUf, n, piv, R);
         for (int e = lane; e < n * n; e += 32) X[e] = (double)R[e];
         __syncwarp();
+        // per column: last correction, the one before, and whether it is done
+        double dlast[2] = {INFINITY, INFINITY}, dprev[2] = {INFINITY, INFINITY}, xlast[2] = {0, 0};
+        bool cdone[2] = {lane >= n, lane + 32 >= n};
         bool done = false;
         for (int it = 0; it < max_iter && !done && inf == 0; ++it) {
             // residual R = I - A X, column c by lane c
@@ -77,14 +80,14 @@ __global__ void inverse_f32r_kernel(const double* __restrict__ A, double* __rest
                 }
             __syncwarp();
             // correction D = LU^-1 R (in place), X += D
-            bool col_ok = true;
-            for (int c = lane; c < n; c += 32) {
+            for (int c = lane, t = 0; c < n; c += 32, ++t) {
+                if (cdone[t]) continue;
                 for (int j = 0; j < n; ++j) {
                     const int p = piv[j];
                     if (p != j) {
-                        float t = R[j * n + c];
+                        float tmp = R[j * n + c];
                         R[j * n + c] = R[p * n + c];
-                        R[p * n + c] = t;
+                        R[p * n + c] = tmp;
                     }
                 }
                 for (int j = 0; j < n; ++j) {
@@ -103,11 +106,22 @@ __global__ void inverse_f32r_kernel(const double* __restrict__ A, double* __rest
                     dmax = fmax(dmax, fabs((double)R[i * n + c]));
                     xmax = fmax(xmax, fabs(x));
                 }
-                col_ok = col_ok && dmax <= tol * xmax;
+                dprev[t] = dlast[t];
+                dlast[t] = dmax;
+                xlast[t] = xmax;
+                // done when below the tolerance or no longer contracting
+                cdone[t] = dmax <= tol * xmax || dmax > 0.5 * dprev[t];
             }
-            done = __all_sync(kFull, col_ok);
+            done = __all_sync(kFull, cdone[0] && cdone[1]);
             __syncwarp();
         }
+        // converged: last correction within the tolerance, or within 1e-10
+        // of the column when refinement stagnated at the FP64 residual floor
+        bool conv = true;
+        for (int t = 0; t < 2; ++t)
+            if (lane + 32 * t < n)
+                conv = conv && (dlast[t] <= tol * xlast[t] || dlast[t] <= 1e-10 * xlast[t]);
+        done = __all_sync(kFull, conv);
         double* o = Ainv + b * (int64_t)n * n;
         for (int e = lane; e < n * n; e += 32) o[e] = X[(e % n) * n + e / n];
         if (info && lane == 0) info[b] = inf != 0 ? inf : (done ? 0 : -1);

@@ -22,6 +22,9 @@
 
 namespace naga {
 
+// systems whose FP32 refinement failed in the last refined call (per thread)
+static thread_local int64_t g_fallbacks = 0;
+
 namespace {
 
 // multiquadric (r^2 + (0.1 h)^2)^0.5 in units of h (radial_point_method.cuh:
@@ -88,8 +91,11 @@ __device__ void warp_matvec(const double* A, int n, double x0, double x1, double
 
 // Solves G0 x = b for the distributed right-hand side (x0, x1) in place:
 // precision 0: FP64 LU (factors in G); precision 1: FP32 LU in Gf with
-// FP64-residual refinement against G (unfactored). Returns false when the
-// refinement did not converge.
+// FP64-residual refinement against G (unfactored). Refinement stops when
+// the correction falls below 1e-14 of the solution or stops shrinking; it
+// has converged when the last correction is below 1e-10 of the solution
+// (the relative weight error the FP64 path is held to). Returns false when
+// it has not.
 __device__ bool solve_rhs(const double* G, const float* Gf, const int* piv, int n, int precision, double& x0,
                           double& x1) {
     if (precision == 0) {
@@ -101,6 +107,7 @@ __device__ bool solve_rhs(const double* G, const float* Gf, const int* piv, int 
     warp_lu_solve_reg(Gf, n, piv, f0, f1);
     x0 = f0;
     x1 = f1;
+    double prev = INFINITY, dm = INFINITY, xm = 0;
     for (int it = 0; it < 30; ++it) {
         double y0, y1;
         warp_matvec(G, n, x0, x1, y0, y1);
@@ -108,16 +115,17 @@ __device__ bool solve_rhs(const double* G, const float* Gf, const int* piv, int 
         warp_lu_solve_reg(Gf, n, piv, r0, r1);
         x0 += r0;
         x1 += r1;
-        double dm = fmax(fabs((double)r0), fabs((double)r1));
-        double xm = fmax(fabs(x0), fabs(x1));
+        dm = fmax(fabs((double)r0), fabs((double)r1));
+        xm = fmax(fabs(x0), fabs(x1));
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             dm = fmax(dm, __shfl_xor_sync(kFull, dm, o));
             xm = fmax(xm, __shfl_xor_sync(kFull, xm, o));
         }
-        if (dm <= 1e-15 * xm) return true;
+        if (dm <= 1e-14 * xm || dm > 0.5 * prev) break;
+        prev = dm;
     }
-    return false;
+    return dm <= 1e-10 * xm;
 }
 
 __device__ __forceinline__ size_t rbf_smem_per_warp(int n, int k, int D, int precision) {
@@ -178,7 +186,8 @@ __global__ void rbf_weights_kernel(const float* __restrict__ src, int64_t nsrc, 
         }
         __syncwarp();
         build_G0<D>(s.xs, k, shape, s.G);
-        int info = factor(s, n, precision);
+        int prec = precision;
+        int info = factor(s, n, prec);
         if (info) atomicOr(status, 2);
         for (int q = 0; q < group; ++q) {
             double x[D];
@@ -186,7 +195,14 @@ __global__ void rbf_weights_kernel(const float* __restrict__ src, int64_t nsrc, 
             for (int d = 0; d < D; ++d) x[d] = (qry[(g * group + q) * D + d] - o[d]) / spacing;
             double x0 = lane < n ? gx_row<D>(s.xs, k, shape, x, lane) : 0.0;
             double x1 = lane + 32 < n ? gx_row<D>(s.xs, k, shape, x, lane + 32) : 0.0;
-            if (!solve_rhs(s.G, s.Gf, s.piv, n, precision, x0, x1)) atomicOr(status, 4);
+            if (!solve_rhs(s.G, s.Gf, s.piv, n, prec, x0, x1)) {
+                // FP32 refinement failed: factor in FP64 and redo the group
+                prec = 0;
+                if (lane == 0) atomicAdd(status + 1, 1);
+                if (warp_lu(s.G, n, s.piv)) atomicOr(status, 2);
+                q = -1;
+                continue;
+            }
             double* out = weights + (g * group + q) * k;
             if (lane < k) out[lane] = x0;
             if (lane + 32 < k) out[lane + 32] = x1;
@@ -353,12 +369,25 @@ __global__ void divergence_build_kernel(const float* __restrict__ pts, int64_t n
         const int info = factor(s, nsys, precision);
         if (info) atomicOr(status, 2);
         double W0[D], W1[D];
+        bool ok = true;
 #pragma unroll
         for (int d = 0; d < D; ++d) {
             double x0 = b0[d], x1 = b1[d];
-            if (!solve_rhs(s.G, s.Gf, s.piv, nsys, precision, x0, x1)) atomicOr(status, 4);
+            ok = ok && solve_rhs(s.G, s.Gf, s.piv, nsys, precision, x0, x1);
             W0[d] = x0 + (lane == 0 ? cself[d] : 0.0);
             W1[d] = x1;
+        }
+        if (!ok) {
+            // FP32 refinement failed for this system: solve it in FP64
+            if (lane == 0) atomicAdd(status + 1, 1);
+            if (warp_lu(s.G, nsys, s.piv)) atomicOr(status, 2);
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                double x0 = b0[d], x1 = b1[d];
+                warp_lu_solve_reg(s.G, nsys, s.piv, x0, x1);
+                W0[d] = x0 + (lane == 0 ? cself[d] : 0.0);
+                W1[d] = x1;
+            }
         }
         // selective-filter weights: normalised Gaussian of the distance
         // (detail/simulation_engine.cuh:1233-1323), computed once
@@ -420,8 +449,8 @@ int rbf_weights_device(const float* src, int64_t nsrc, int dim, const uint32_t* 
     const int wpb = warps_per_block_for(per_warp);
     if (wpb < 1) return set_error(NAGA_EINVAL, "naga_rbf_weights: system too large");
     int* d_status = nullptr;
-    NAGA_CUDA_TRY(cudaMallocAsync(&d_status, sizeof(int), st));
-    NAGA_CUDA_TRY(cudaMemsetAsync(d_status, 0, sizeof(int), st));
+    NAGA_CUDA_TRY(cudaMallocAsync(&d_status, 2 * sizeof(int), st));
+    NAGA_CUDA_TRY(cudaMemsetAsync(d_status, 0, 2 * sizeof(int), st));
     const int blocks = (int)std::min<int64_t>((ngroups + wpb - 1) / wpb, (int64_t)sm_count() * 32);
     const size_t smem = per_warp * wpb;
     if (dim == 2) {
@@ -434,13 +463,14 @@ int rbf_weights_device(const float* src, int64_t nsrc, int dim, const uint32_t* 
                                                               shape, precision, weights, d_status, wpb);
     }
     NAGA_CUDA_TRY(cudaGetLastError());
-    int h_status = 0;
-    NAGA_CUDA_TRY(cudaMemcpyAsync(&h_status, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    int h_st[2] = {0, 0};
+    NAGA_CUDA_TRY(cudaMemcpyAsync(h_st, d_status, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
     NAGA_CUDA_TRY(cudaFreeAsync(d_status, st));
     NAGA_CUDA_TRY(cudaStreamSynchronize(st));
+    const int h_status = h_st[0];
+    g_fallbacks = h_st[1];
     if (h_status & 1) return set_error(NAGA_EINVAL, "naga_rbf_weights: support index out of range");
     if (h_status & 2) return set_error(NAGA_ESINGULAR, "naga_rbf_weights: singular moment matrix");
-    if (h_status & 4) return set_error(NAGA_ENOCONVERGE, "naga_rbf_weights: refinement did not converge");
     return NAGA_OK;
 }
 
@@ -465,8 +495,8 @@ int divergence_build_device(const float* pts, int64_t n, int dim, int k, int sha
     }
     NAGA_CUDA_TRY(cudaMallocAsync(&nn, sizeof(double) * n, st));
     NAGA_CUDA_TRY(cudaMallocAsync(&sp, sizeof(double) * nb, st));
-    NAGA_CUDA_TRY(cudaMallocAsync(&d_status, sizeof(int), st));
-    NAGA_CUDA_TRY(cudaMemsetAsync(d_status, 0, sizeof(int), st));
+    NAGA_CUDA_TRY(cudaMallocAsync(&d_status, 2 * sizeof(int), st));
+    NAGA_CUDA_TRY(cudaMemsetAsync(d_status, 0, 2 * sizeof(int), st));
     {
         const int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)sm_count() * 8);
         if (dim == 2)
@@ -490,21 +520,24 @@ int divergence_build_device(const float* pts, int64_t n, int dim, int k, int sha
                                                                    d_status, wpb);
     }
     NAGA_CUDA_TRY(cudaGetLastError());
-    int h_status = 0;
-    NAGA_CUDA_TRY(cudaMemcpyAsync(&h_status, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    int h_st[2] = {0, 0};
+    NAGA_CUDA_TRY(cudaMemcpyAsync(h_st, d_status, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
     NAGA_CUDA_TRY(cudaStreamSynchronize(st));
+    const int h_status = h_st[0];
+    g_fallbacks = h_st[1];
     cudaFreeAsync(d2, st);
     cudaFreeAsync(nn, st);
     cudaFreeAsync(sp, st);
     cudaFreeAsync(d_status, st);
     if (h_status & 2) return set_error(NAGA_ESINGULAR, "divergence build: singular moment matrix");
-    if (h_status & 4) return set_error(NAGA_ENOCONVERGE, "divergence build: refinement did not converge");
     return NAGA_OK;
 }
 
 }  // namespace naga
 
 using namespace naga;
+
+extern "C" int64_t naga_refinement_fallbacks(void) { return naga::g_fallbacks; }
 
 extern "C" int naga_rbf_weights(const float* src, int64_t n, int dim, const uint32_t* support, int k,
                                 const double* qry, int64_t ngroups, int group, double spacing, int shape,

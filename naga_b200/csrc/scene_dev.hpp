@@ -56,8 +56,8 @@ struct SceneDev {
     const uint8_t* is_src;
     // outputs / bookkeeping
     float* probe_ring;
-    double* partials;  // [n_all_items][2 Q]
-    float* means;      // [2 Q]
+    double* partials;  // [n_all_items][2 QP], slot order
+    float* means;      // [2 QP], slot order
     unsigned long long* step;
 };
 
@@ -93,9 +93,12 @@ struct StepLaunch {
     int n_fluid;
     const WorkItem* edge;
     int n_edge;
+    const WorkItem* pml;  // bulk/layer items whose stencils reach the layer
+    int n_pml;
 };
 
-int enqueue_step(int dim, const StepLaunch& P, cudaStream_t st);
+// k: the batch's common stencil size (0 if the members differ)
+int enqueue_step(int dim, int k, const StepLaunch& P, cudaStream_t st);
 const char* kernel_name(int id);
 int kernel_count();
 void prof_begin(int id, cudaStream_t st);

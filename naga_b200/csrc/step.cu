@@ -6,13 +6,15 @@
 // a fixed sequence of fused kernels over work items (<= 128 consecutive nodes
 // of one scene), so one launch covers every scene of a batch:
 //
-//   macro_pml     all nodes   rho, u; PML trapezoid integrals Q1, Q2;
+//   macro_pml     all nodes   rho, u; PML trapezoid integrals Q1, Q2 and the
+//                             local absorption term; central-moment collision;
 //                             per-item layer sums of Q1, Q2
 //   pml_means     per scene   layer means of Q1, Q2 (fixed-order sums)
 //   probe         per scene   RPIM probe of rho at the start of the step
-//   pml_collide   bulk+layer  f - sigma(3f~ + 3 sigma Q1 + sigma^2 Q2) + PML
-//                             divergence gathers + central-moment collision
-//   edge_collide  boundary    RPIM boundary interpolation + collision
+//   pml_gather    layer-adjacent bulk+layer nodes: the two PML divergence
+//                             gathers div(-2 c sigma (Q1 - <Q1>)) and
+//                             div(c sigma^2 (Q2 - <Q2>))
+//   edge_collide  boundary    RPIM boundary interpolation (+ collision)
 //   filter        all nodes   selective Gaussian filter; bounce-back
 //   rk(1..4)      bulk+layer  streaming gather + RK4 stage update
 //   edge_interp   boundary    RPIM boundary interpolation of the result
@@ -24,6 +26,11 @@
 // precision. Where the collision formulas subtract the O(1) equilibrium
 // parts of the moments, those parts are cancelled analytically and only the
 // small remainders enter the FP32 arithmetic.
+//
+// Gathers run TPN threads per node (8 for D3Q27, 4 for D2Q9): thread c owns
+// float4 chunk c of the node's row, so one warp-wide load of neighbour rows
+// touches 4 (8) rows instead of 32, and each thread holds two opposite
+// population pairs of its chunk.
 #include "common.cuh"
 #include "scene_dev.hpp"
 
@@ -31,31 +38,43 @@ namespace naga {
 
 namespace {
 
-constexpr int kBlock = 128;
+constexpr int kBlock = 128;    // thread-per-node kernels
+constexpr int kBlockMT = 256;  // multi-thread-per-node kernels
 
 template <class L>
 struct Lat : LatticeTables<L> {
-    using T = LatticeTables<L>;
     static constexpr int D = L::D, Q = L::Q, QP = L::QP;
 };
+
+template <class L>
+struct MT {
+    static constexpr int TPN = L::D == 3 ? 8 : 4;  // threads per node
+    static constexpr int NCH = L::QP / 4;          // float4 chunks per row
+    static constexpr int NPB = kBlockMT / TPN;     // nodes per block pass
+};
+
+// direction of the first population of each slot pair of a row
+// ((0, pad) and (pad, pad) pairs have zero direction)
+__constant__ float c_pdir3[14][3] = {{0, 0, 0},  {1, 0, 0},  {0, 1, 0},   {0, 0, 1},  {1, 1, 0},
+                                     {-1, 1, 0}, {1, 0, 1},  {-1, 0, 1},  {0, 1, 1},  {0, -1, 1},
+                                     {1, 1, 1},  {-1, 1, 1}, {1, -1, 1},  {-1, -1, 1}};
+__constant__ float c_pdir2[6][3] = {{0, 0, 0}, {-1, 1, 0}, {-1, 0, 0}, {-1, -1, 0}, {0, -1, 0}, {0, 0, 0}};
+
+template <class L>
+__device__ __forceinline__ void pair_dirs(int c, float* d0, float* d1) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        d0[d] = L::D == 3 ? c_pdir3[2 * c][d] : c_pdir2[2 * c][d];
+        d1[d] = L::D == 3 ? c_pdir3[2 * c + 1][d] : c_pdir2[2 * c + 1][d];
+    }
+}
 
 // lattice speed of sound as the reference spells it (lattices.cuh:46-49)
 __device__ __forceinline__ float cs_f() { return 0.57735026918962576450914878050196f; }
 
+// full row (QP floats) of node i, slot order
 template <class L>
 __device__ __forceinline__ void load_row(const float* base, int64_t i, float* v) {
-    const float4* p = reinterpret_cast<const float4*>(base + i * L::QP);
-#pragma unroll
-    for (int c = 0; c < L::QP / 4; ++c) {
-        float4 t = __ldg(p + c);
-        v[4 * c + 0] = t.x;
-        v[4 * c + 1] = t.y;
-        v[4 * c + 2] = t.z;
-        v[4 * c + 3] = t.w;
-    }
-}
-template <class L>
-__device__ __forceinline__ void load_row_rw(const float* base, int64_t i, float* v) {
     const float4* p = reinterpret_cast<const float4*>(base + i * L::QP);
 #pragma unroll
     for (int c = 0; c < L::QP / 4; ++c) {
@@ -70,18 +89,20 @@ template <class L>
 __device__ __forceinline__ void store_row(float* base, int64_t i, const float* v) {
     float4* p = reinterpret_cast<float4*>(base + i * L::QP);
 #pragma unroll
-    for (int c = 0; c < L::QP / 4; ++c) {
-        float4 t;
-        t.x = v[4 * c + 0];
-        t.y = (4 * c + 1 < L::Q) ? v[4 * c + 1] : 0.f;
-        t.z = (4 * c + 2 < L::Q) ? v[4 * c + 2] : 0.f;
-        t.w = (4 * c + 3 < L::Q) ? v[4 * c + 3] : 0.f;
-        p[c] = t;
-    }
+    for (int c = 0; c < L::QP / 4; ++c) p[c] = make_float4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
+}
+__device__ __forceinline__ float4 ld4(const float* base, int64_t i, int qp, int c) {
+    return __ldg(reinterpret_cast<const float4*>(base + i * qp) + c);
+}
+__device__ __forceinline__ float4 ld4rw(const float* base, int64_t i, int qp, int c) {
+    return reinterpret_cast<const float4*>(base + i * qp)[c];
+}
+__device__ __forceinline__ void st4(float* base, int64_t i, int qp, int c, float4 v) {
+    reinterpret_cast<float4*>(base + i * qp)[c] = v;
 }
 
-// rho - 1 and u (lattice units) from centred populations; sums in
-// population order as detail/simulation_engine.cuh:53-82
+// rho - 1 and u (lattice units) from centred populations (reference order);
+// sums in population order as detail/simulation_engine.cuh:53-82
 template <class L>
 __device__ __forceinline__ void macros(const float* g, float& drho, float* u) {
     using T = Lat<L>;
@@ -114,17 +135,6 @@ __device__ __forceinline__ float feq_c(int a, float drho, const float* u) {
     }
     const float w = T::w(a);
     return w * drho + w * (1.f + drho) * (uc / cs2 + (uc * uc) / (2.f * cs4) - uu);
-}
-
-// c_a . W for a population a
-template <class L>
-__device__ __forceinline__ float proj(int a, float wx, float wy, float wz) {
-    using T = Lat<L>;
-    float p = 0.f;
-    if (T::cx(a)) p = T::cx(a) > 0 ? wx : -wx;
-    if (T::cy(a)) p = T::cy(a) > 0 ? p + wy : p - wy;
-    if (L::D == 3 && T::cz(a)) p = T::cz(a) > 0 ? p + wz : p - wz;
-    return p;
 }
 
 // stencil record s of node i: weights and support index
@@ -400,82 +410,118 @@ __device__ __forceinline__ void collide(const float* g, float drho, const float*
         const WorkItem it = (items)[w_];                                    \
         __syncthreads();                                                    \
         if (threadIdx.x == 0) S = scenes[it.scene];                         \
-        __syncthreads();                                                    \
-        const int64_t i = (int64_t)it.begin + threadIdx.x;                  \
-        const bool active = i < (int64_t)it.end;
+        __syncthreads();
 
 #define NAGA_END_ITEMS }
 
-// rho, u; Q1 = (f~ + f~_prev) dt/2, Q2 = (Q1 + Q1_prev) dt/2
-// (fluids/.../detail/pml_absorption.inl:531-631); layer sums of Q1, Q2
+// Node-local part of the step, one thread per node (all nodes):
+// rho, u (stored for the probes and the next step); the PML trapezoid
+// integrals Q1 = (f~ + f~_prev) dt / 2, Q2 = (Q1 + Q1_prev) dt / 2 with
+// f~ = feq - w (pml_absorption.inl:531-631); the local absorption term
+// -sigma (3 f~ + 3 sigma Q1 + sigma^2 Q2) on layer nodes; the collision
+// increment K k dt (simulation_engine.cuh:469-531). Writes
+//   bulk/layer: S1 = g + local + collision, and S1P = g + local on nodes the
+//               boundary interpolation reads;
+//   boundary:   S1 = collision (the interpolated part is added later);
+//   ghost:      S1 = g + collision.
 template <class L>
 __global__ void __launch_bounds__(kBlock) k_macro_pml(const WorkItem* __restrict__ items, int nitems,
                                                       const SceneDev* __restrict__ scenes) {
-    constexpr int Q = L::Q;
-    __shared__ double red[kBlock / 32][2 * Q];
+    constexpr int Q = L::Q, QP = L::QP;
+    __shared__ double red[kBlock / 32][2 * QP];
     NAGA_FOR_ITEMS(items, nitems)
+    const int64_t i = (int64_t)it.begin + threadIdx.x;
+    const bool active = i < (int64_t)it.end;
     const int par = (int)(*S.step & 1ull);
     float* Q1cur = par ? S.Q1b : S.Q1a;
     const float* Q1prev = par ? S.Q1a : S.Q1b;
     const bool layer = active && i >= S.nb && i < S.nb + S.nl;
-    float s1[Q], s2[Q];
+    float s1[QP], s2[QP];
+#pragma unroll
+    for (int t = 0; t < QP; ++t) s1[t] = s2[t] = 0.f;
     if (active) {
-        float g[L::QP], q1p[L::QP], q1[L::QP];
-        load_row_rw<L>(S.G, i, g);
+        float row[QP], q1p[QP], q1[QP], out[QP];
+        load_row<L>(S.G, i, row);
+        float g[Q];
+#pragma unroll
+        for (int a = 0; a < Q; ++a) g[a] = row[L::pos(a)];
         float drho, u[3] = {0.f, 0.f, 0.f};
         macros<L>(g, drho, u);
         const float4 mp = S.M[i];
         const float up[3] = {mp.y, mp.z, mp.w};
         S.M[i] = make_float4(drho, u[0], u[1], L::D == 3 ? u[2] : 0.f);
-        load_row_rw<L>(Q1prev, i, q1p);
+        load_row<L>(Q1prev, i, q1p);
+        const float sg = layer ? __ldg(S.sigma + (i - S.nb)) : 0.f;
+        float dcol[Q];
+        collide<L>(g, drho, u, S, dcol);
+#pragma unroll
+        for (int t = 0; t < QP; ++t) q1[t] = out[t] = 0.f;
+        const bool src = i < S.nbl && S.is_src[i];
 #pragma unroll
         for (int a = 0; a < Q; ++a) {
+            const int t = L::pos(a);
             const float ft = feq_c<L>(a, drho, u);
             const float ftp = feq_c<L>(a, mp.x, up);
-            q1[a] = (ft + ftp) * S.dt_lat / 2.f;
-            const float q2 = (q1[a] + q1p[a]) * S.dt_lat / 2.f;
-            s1[a] = layer ? q1[a] : 0.f;
-            s2[a] = layer ? q2 : 0.f;
+            q1[t] = (ft + ftp) * S.dt_lat / 2.f;
+            const float q2 = (q1[t] + q1p[t]) * S.dt_lat / 2.f;
+            if (layer) {
+                s1[t] = q1[t];
+                s2[t] = q2;
+            }
+            const float loc = layer ? g[a] - sg * (3.f * ft + 3.f * sg * q1[t] + sg * sg * q2) : g[a];
+            out[t] = loc;
         }
         store_row<L>(Q1cur, i, q1);
-    } else {
+        if (src) store_row<L>(S.S1P, i, out);
+        const bool boundary = i >= S.nbl && i < S.nbl + S.nbd;
 #pragma unroll
-        for (int a = 0; a < Q; ++a) s1[a] = s2[a] = 0.f;
+        for (int a = 0; a < Q; ++a) {
+            const int t = L::pos(a);
+            out[t] = boundary ? dcol[a] : out[t] + dcol[a];
+        }
+        store_row<L>(S.S1, i, out);
     }
     // per-item layer sums in FP64, fixed order
     const bool touches = (int64_t)it.end > S.nb && (int64_t)it.begin < S.nb + S.nl;
     if (touches) {
         const int wid = threadIdx.x >> 5;
 #pragma unroll
-        for (int a = 0; a < Q; ++a) {
-            double v1 = warp_sum((double)s1[a]);
-            double v2 = warp_sum((double)s2[a]);
+        for (int t = 0; t < QP; ++t) {
+            double v1 = warp_sum((double)s1[t]);
+            double v2 = warp_sum((double)s2[t]);
             if (lane_id() == 0) {
-                red[wid][a] = v1;
-                red[wid][Q + a] = v2;
+                red[wid][t] = v1;
+                red[wid][QP + t] = v2;
             }
         }
     }
     __syncthreads();
-    if (threadIdx.x < 2 * Q) {
+    if (threadIdx.x < 2 * QP) {
         double v = 0.0;
         if (touches)
             for (int wv = 0; wv < kBlock / 32; ++wv) v += red[wv][threadIdx.x];
-        S.partials[(int64_t)it.local * 2 * Q + threadIdx.x] = v;
+        S.partials[(int64_t)it.local * 2 * QP + threadIdx.x] = v;
     }
     NAGA_END_ITEMS
 }
 
 // layer means of Q1 and Q2 per scene (the reductions of
-// pml_absorption.inl:776-836), summed in item order
-template <int Q>
+// pml_absorption.inl:776-836); block (scene, slot), summed in item order
+// strided over the block, then a fixed tree
+template <int QP>
 __global__ void k_pml_means(const SceneDev* __restrict__ scenes) {
+    __shared__ double red[256];
     const SceneDev& S = scenes[blockIdx.x];
-    const int t = threadIdx.x;
-    if (t >= 2 * Q) return;
+    const int t = blockIdx.y;
     double acc = 0.0;
-    for (int it = 0; it < S.n_all_items; ++it) acc += S.partials[(int64_t)it * 2 * Q + t];
-    S.means[t] = S.nl > 0 ? (float)acc / (float)S.nl : 0.f;
+    for (int it = threadIdx.x; it < S.n_all_items; it += blockDim.x) acc += S.partials[(int64_t)it * 2 * QP + t];
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) S.means[t] = S.nl > 0 ? (float)red[0] / (float)S.nl : 0.f;
 }
 
 // probe densities (rho - rho0) from the RPIM probe weights
@@ -496,167 +542,145 @@ __global__ void k_probe(const SceneDev* __restrict__ scenes) {
     }
 }
 
-// bulk + layer: s1 = g - sigma(3 f~ + 3 sigma Q1 + sigma^2 Q2)  (layer only)
-//   + div(-2 c sigma (Q1 - <Q1>)) + div(c sigma^2 (Q2 - <Q2>))
-//   [+ collision]  (pml_absorption.inl:770-855; simulation_engine.cuh:469-531)
-template <class L>
-__global__ void __launch_bounds__(kBlock) k_pml_collide(const WorkItem* __restrict__ items, int nitems,
-                                                        const SceneDev* __restrict__ scenes) {
-    constexpr int Q = L::Q;
-    NAGA_FOR_ITEMS(items, nitems)
-    if (active) {
-        const int par = (int)(*S.step & 1ull);
-        const float* Q1cur = par ? S.Q1b : S.Q1a;
-        const float* Q1prev = par ? S.Q1a : S.Q1b;
-        float acc[L::QP];
-        load_row<L>(S.G, i, acc);
-        float drho, u[3] = {0.f, 0.f, 0.f};
-        macros<L>(acc, drho, u);
-        float dcol[Q];
-        collide<L>(acc, drho, u, S, dcol);
-        const float hdt = S.half_dt;
-        if (i >= S.nb && i < S.nb + S.nl) {
-            const float sg = __ldg(S.sigma + (i - S.nb));
-            float q1[L::QP], q1p[L::QP];
-            load_row<L>(Q1cur, i, q1);
-            load_row<L>(Q1prev, i, q1p);
-#pragma unroll
-            for (int a = 0; a < Q; ++a) {
-                const float ft = feq_c<L>(a, drho, u);
-                const float q2 = (q1[a] + q1p[a]) * S.dt_lat / 2.f;
-                acc[a] -= sg * (3.f * ft + 3.f * sg * q1[a] + sg * sg * q2);
-            }
-        }
-        (void)hdt;
-        if (S.nl > 0) {
-            float m1[Q], m2[Q];
-#pragma unroll
-            for (int a = 0; a < Q; ++a) {
-                m1[a] = S.means[a];
-                m2[a] = S.means[Q + a];
-            }
-            float div[Q];
-#pragma unroll
-            for (int a = 0; a < Q; ++a) div[a] = 0.f;
-            for (int s = 0; s < S.k; ++s) {
-                float wx, wy, wz;
-                uint32_t j;
-                stencil<L>(S, s, i, wx, wy, wz, j);
-                if ((int64_t)j < S.nb || (int64_t)j >= S.nb + S.nl) continue;
-                const float sg = __ldg(S.sigma + ((int64_t)j - S.nb));
-                const int64_t jq = (int64_t)j - S.pml_shift;
-                const float4* r1 = reinterpret_cast<const float4*>(Q1cur + jq * L::QP);
-                const float4* r0 = reinterpret_cast<const float4*>(Q1prev + jq * L::QP);
-#pragma unroll
-                for (int c = 0; c < L::QP / 4; ++c) {
-                    const float4 a4 = __ldg(r1 + c), b4 = __ldg(r0 + c);
-                    const float qa[4] = {a4.x, a4.y, a4.z, a4.w};
-                    const float qb[4] = {b4.x, b4.y, b4.z, b4.w};
-#pragma unroll
-                    for (int e = 0; e < 4; ++e) {
-                        const int a = 4 * c + e;
-                        if (a >= Q) continue;
-                        const float p = proj<L>(a, wx, wy, wz);
-                        if (a == 0) continue;
-                        const float q2 = (qa[e] + qb[e]) * S.dt_lat / 2.f;
-                        const float phi = -2.f * sg * (qa[e] - m1[a]) + sg * sg * (q2 - m2[a]);
-                        div[a] = fmaf(p, phi, div[a]);
-                    }
-                }
-            }
-#pragma unroll
-            for (int a = 0; a < Q; ++a) acc[a] += div[a];
-        }
-        if (S.is_src[i]) store_row<L>(S.S1P, i, acc);
-#pragma unroll
-        for (int a = 0; a < Q; ++a) acc[a] += dcol[a];
-        store_row<L>(S.S1, i, acc);
+// Multi-thread-per-node loop over the nodes of an item: thread c of node
+// slot `ns` handles chunk c of node i.
+#define NAGA_MT_NODES(G)                                                      \
+    const int c = threadIdx.x % G::TPN;                                      \
+    const int ns = threadIdx.x / G::TPN;                                     \
+    for (int64_t base = it.begin; base < (int64_t)it.end; base += G::NPB) {  \
+        const int64_t i = base + ns;                                         \
+        if (i < (int64_t)it.end && c < G::NCH) {
+
+#define NAGA_MT_END \
+    }               \
     }
+
+// PML divergence gathers of pml_absorption.inl:770-855 on bulk/layer nodes
+// whose stencil reaches into the layer: for support j in the layer the field
+// is -2 c sigma_j (Q1 - <Q1>) + c sigma_j^2 (Q2 - <Q2>), read at node
+// j - pml_shift (NAGA's field maps index Q by the layer position,
+// pml_absorption.inl:438-448). Adds to S1 and, on interpolation sources, S1P.
+template <class L, int K>
+__global__ void __launch_bounds__(kBlockMT) k_pml_gather(const WorkItem* __restrict__ items, int nitems,
+                                                         const SceneDev* __restrict__ scenes) {
+    using G = MT<L>;
+    constexpr int QP = L::QP;
+    float d0[3], d1[3];
+    pair_dirs<L>(threadIdx.x % G::TPN < G::NCH ? threadIdx.x % G::TPN : 0, d0, d1);
+    NAGA_FOR_ITEMS(items, nitems)
+    const int par = (int)(*S.step & 1ull);
+    const float* Q1cur = par ? S.Q1b : S.Q1a;
+    const float* Q1prev = par ? S.Q1a : S.Q1b;
+    const int k = K > 0 ? K : S.k;
+    NAGA_MT_NODES(G)
+    const float4 m1 = *reinterpret_cast<const float4*>(S.means + 4 * c);
+    const float4 m2 = *reinterpret_cast<const float4*>(S.means + QP + 4 * c);
+    const float dt = S.dt_lat;
+    float4 dv = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll 4
+    for (int s = 0; s < k; ++s) {
+        float wx, wy, wz;
+        uint32_t j;
+        stencil<L>(S, s, i, wx, wy, wz, j);
+        if ((int64_t)j < S.nb || (int64_t)j >= S.nb + S.nl) continue;
+        const float sg = __ldg(S.sigma + ((int64_t)j - S.nb));
+        const int64_t jq = (int64_t)j - S.pml_shift;
+        const float4 a = ld4(Q1cur, jq, QP, c), b = ld4(Q1prev, jq, QP, c);
+        const float p0 = d0[0] * wx + d0[1] * wy + d0[2] * wz;
+        const float p1 = d1[0] * wx + d1[1] * wy + d1[2] * wz;
+        const float sg2 = sg * sg, m2s = -2.f * sg;
+        const float f0 = m2s * (a.x - m1.x) + sg2 * ((a.x + b.x) * dt / 2.f - m2.x);
+        const float f1 = m2s * (a.y - m1.y) + sg2 * ((a.y + b.y) * dt / 2.f - m2.y);
+        const float f2 = m2s * (a.z - m1.z) + sg2 * ((a.z + b.z) * dt / 2.f - m2.z);
+        const float f3 = m2s * (a.w - m1.w) + sg2 * ((a.w + b.w) * dt / 2.f - m2.w);
+        dv.x = fmaf(p0, f0, dv.x);
+        dv.y = fmaf(-p0, f1, dv.y);
+        dv.z = fmaf(p1, f2, dv.z);
+        dv.w = fmaf(-p1, f3, dv.w);
+    }
+    float4 o = ld4rw(S.S1, i, QP, c);
+    st4(S.S1, i, QP, c, make_float4(o.x + dv.x, o.y + dv.y, o.z + dv.z, o.w + dv.w));
+    if (S.is_src[i]) {
+        float4 q = ld4rw(S.S1P, i, QP, c);
+        st4(S.S1P, i, QP, c, make_float4(q.x + dv.x, q.y + dv.y, q.z + dv.z, q.w + dv.w));
+    }
+    NAGA_MT_END
     NAGA_END_ITEMS
 }
 
-// boundary: s1 = interp(s1 of bulk + layer, before collision) + collision;
-// ghost: s1 = g + collision
+// boundary: s1 = interp(s1 of bulk + layer, before collision) + collision
+// (simulation_engine.cuh:434-467 then :469-531); S1 holds the collision
 template <class L>
-__global__ void __launch_bounds__(kBlock) k_edge_collide(const WorkItem* __restrict__ items, int nitems,
-                                                         const SceneDev* __restrict__ scenes) {
-    constexpr int Q = L::Q;
+__global__ void __launch_bounds__(kBlockMT) k_edge_collide(const WorkItem* __restrict__ items, int nitems,
+                                                           const SceneDev* __restrict__ scenes) {
+    using G = MT<L>;
+    constexpr int QP = L::QP;
     NAGA_FOR_ITEMS(items, nitems)
-    if (active) {
-        float g[L::QP];
-        load_row<L>(S.G, i, g);
-        float drho, u[3] = {0.f, 0.f, 0.f};
-        macros<L>(g, drho, u);
-        float dcol[Q];
-        collide<L>(g, drho, u, S, dcol);
-        float acc[L::QP];
-        const int64_t b = i - S.nbl;
-        if (b < S.nbd) {
-#pragma unroll
-            for (int a = 0; a < Q; ++a) acc[a] = 0.f;
-            for (int s = 0; s < S.kb; ++s) {
-                const uint32_t j = __ldg(S.bidx + (int64_t)s * S.nbd + b);
-                const float w = __ldg(S.bw + (int64_t)s * S.nbd + b);
-                float v[L::QP];
-                load_row<L>(S.S1P, j, v);
-#pragma unroll
-                for (int a = 0; a < Q; ++a) acc[a] = fmaf(w, v[a], acc[a]);
-            }
-        } else {
-#pragma unroll
-            for (int a = 0; a < Q; ++a) acc[a] = g[a];
+    NAGA_MT_NODES(G)
+    const int64_t b = i - S.nbl;
+    if (b < S.nbd) {
+        float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int s = 0; s < S.kb; ++s) {
+            const uint32_t j = __ldg(S.bidx + (int64_t)s * S.nbd + b);
+            const float w = __ldg(S.bw + (int64_t)s * S.nbd + b);
+            const float4 v = ld4(S.S1P, j, QP, c);
+            acc.x = fmaf(w, v.x, acc.x);
+            acc.y = fmaf(w, v.y, acc.y);
+            acc.z = fmaf(w, v.z, acc.z);
+            acc.w = fmaf(w, v.w, acc.w);
         }
-#pragma unroll
-        for (int a = 0; a < Q; ++a) acc[a] += dcol[a];
-        store_row<L>(S.S1, i, acc);
+        const float4 d = ld4rw(S.S1, i, QP, c);
+        st4(S.S1, i, QP, c, make_float4(acc.x + d.x, acc.y + d.y, acc.z + d.z, acc.w + d.w));
     }
+    NAGA_MT_END
     NAGA_END_ITEMS
 }
 
 // bulk + layer: f = s1 + 0.75 sum_s w_s (s1_s - s1) (simulation_engine.cuh:
 // 1233-1323); boundary: bounce-back f_a <- f_bb(a) where c_a . n > 0
-// (:789-944); ghost: copy
-template <class L>
-__global__ void __launch_bounds__(kBlock) k_filter(const WorkItem* __restrict__ items, int nitems,
-                                                   const SceneDev* __restrict__ scenes) {
-    using T = Lat<L>;
-    constexpr int Q = L::Q;
+// (:789-944), a swap within each opposite pair; ghost: copy
+template <class L, int K>
+__global__ void __launch_bounds__(kBlockMT) k_filter(const WorkItem* __restrict__ items, int nitems,
+                                                     const SceneDev* __restrict__ scenes) {
+    using G = MT<L>;
+    constexpr int QP = L::QP;
+    float d0[3], d1[3];
+    pair_dirs<L>(threadIdx.x % G::TPN < G::NCH ? threadIdx.x % G::TPN : 0, d0, d1);
     NAGA_FOR_ITEMS(items, nitems)
-    if (active) {
-        float f[L::QP];
-        load_row<L>(S.S1, i, f);
-        float out[L::QP];
-        if (i < S.nbl) {
-            float sum[Q];
-#pragma unroll
-            for (int a = 0; a < Q; ++a) sum[a] = 0.f;
-            for (int s = 0; s < S.k; ++s) {
-                const float2 r = __ldg(S.stF + (int64_t)s * S.N + i);
-                const uint32_t j = __float_as_uint(r.y);
-                float v[L::QP];
-                load_row<L>(S.S1, j, v);
-#pragma unroll
-                for (int a = 0; a < Q; ++a) sum[a] = fmaf(r.x, v[a] - f[a], sum[a]);
-            }
-#pragma unroll
-            for (int a = 0; a < Q; ++a) out[a] = fmaf(0.75f, sum[a], f[a]);
-        } else if (i - S.nbl < S.nbd) {
-            const int64_t b = i - S.nbl;
-            float n[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-            for (int d = 0; d < L::D; ++d) n[d] = __ldg(S.normals + b * L::D + d);
-#pragma unroll
-            for (int a = 0; a < Q; ++a) {
-                float cn = (float)T::cx(a) * n[0] + (float)T::cy(a) * n[1];
-                if (L::D == 3) cn += (float)T::cz(a) * n[2];
-                out[a] = cn > 0.f ? f[T::bb(a)] : f[a];
-            }
-        } else {
-#pragma unroll
-            for (int a = 0; a < Q; ++a) out[a] = f[a];
+    const int k = K > 0 ? K : S.k;
+    NAGA_MT_NODES(G)
+    const float4 f = ld4rw(S.S1, i, QP, c);
+    float4 out;
+    if (i < S.nbl) {
+        float4 sum = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll 8
+        for (int s = 0; s < k; ++s) {
+            const float2 r = __ldg(S.stF + (int64_t)s * S.N + i);
+            const float4 v = ld4rw(S.S1, __float_as_uint(r.y), QP, c);
+            sum.x = fmaf(r.x, v.x - f.x, sum.x);
+            sum.y = fmaf(r.x, v.y - f.y, sum.y);
+            sum.z = fmaf(r.x, v.z - f.z, sum.z);
+            sum.w = fmaf(r.x, v.w - f.w, sum.w);
         }
-        store_row<L>(S.G, i, out);
+        out = make_float4(fmaf(0.75f, sum.x, f.x), fmaf(0.75f, sum.y, f.y), fmaf(0.75f, sum.z, f.z),
+                          fmaf(0.75f, sum.w, f.w));
+    } else if (i - S.nbl < S.nbd) {
+        const int64_t b = i - S.nbl;
+        float n[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+        for (int d = 0; d < L::D; ++d) n[d] = __ldg(S.normals + b * L::D + d);
+        const float cn0 = d0[0] * n[0] + d0[1] * n[1] + d0[2] * n[2];
+        const float cn1 = d1[0] * n[0] + d1[1] * n[1] + d1[2] * n[2];
+        // element 2m carries direction d_m, element 2m+1 carries -d_m
+        out.x = cn0 > 0.f ? f.y : f.x;
+        out.y = -cn0 > 0.f ? f.x : f.y;
+        out.z = cn1 > 0.f ? f.w : f.z;
+        out.w = -cn1 > 0.f ? f.z : f.w;
+    } else {
+        out = f;
     }
+    st4(S.G, i, QP, c, out);
+    NAGA_MT_END
     NAGA_END_ITEMS
 }
 
@@ -664,86 +688,79 @@ __global__ void __launch_bounds__(kBlock) k_filter(const WorkItem* __restrict__ 
 // rate_a(i) = -sum_s (c_a . W_s) g_a(j_s) (pde_right_hand_side.cuh:82-176,
 // divergence.cuh:377-488). Boundary and ghost nodes keep zero rates, so
 // their stage values equal the step's start values (read from G).
-template <class L, int STAGE>
-__global__ void __launch_bounds__(kBlock) k_rk(const WorkItem* __restrict__ items, int nitems,
-                                               const SceneDev* __restrict__ scenes) {
-    constexpr int Q = L::Q;
+template <class L, int K, int STAGE>
+__global__ void __launch_bounds__(kBlockMT) k_rk(const WorkItem* __restrict__ items, int nitems,
+                                                 const SceneDev* __restrict__ scenes) {
+    using G = MT<L>;
+    constexpr int QP = L::QP;
+    float d0[3], d1[3];
+    pair_dirs<L>(threadIdx.x % G::TPN < G::NCH ? threadIdx.x % G::TPN : 0, d0, d1);
     NAGA_FOR_ITEMS(items, nitems)
-    if (active) {
-        const float* src = (STAGE == 1) ? S.G : (STAGE == 2) ? S.G1 : (STAGE == 3) ? S.G2 : S.G1;
-        float r[Q];
-#pragma unroll
-        for (int a = 0; a < Q; ++a) r[a] = 0.f;
-        for (int s = 0; s < S.k; ++s) {
-            float wx, wy, wz;
-            uint32_t j;
-            stencil<L>(S, s, i, wx, wy, wz, j);
-            const float* row = ((int64_t)j < S.nbl ? src : S.G);
-            float v[L::QP];
-            load_row<L>(row, j, v);
-#pragma unroll
-            for (int a = 1; a < Q; ++a) r[a] = fmaf(proj<L>(a, wx, wy, wz), v[a], r[a]);
-        }
-        float f0[L::QP];
-        load_row<L>(S.G, i, f0);
-        float out[L::QP];
-        if (STAGE == 1) {
-            float acc[L::QP];
-#pragma unroll
-            for (int a = 0; a < Q; ++a) {
-                const float kv = -r[a];
-                out[a] = fmaf(S.a_half, kv, f0[a]);
-                acc[a] = kv * S.b1;
-            }
-            store_row<L>(S.G1, i, out);
-            store_row<L>(S.ACC, i, acc);
+    const int k = K > 0 ? K : S.k;
+    const float* src = (STAGE == 1) ? S.G : (STAGE == 2) ? S.G1 : (STAGE == 3) ? S.G2 : S.G1;
+    NAGA_MT_NODES(G)
+    float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll 8
+    for (int s = 0; s < k; ++s) {
+        float wx, wy, wz;
+        uint32_t j;
+        stencil<L>(S, s, i, wx, wy, wz, j);
+        const float4 v = ld4((int64_t)j < S.nbl ? src : S.G, j, QP, c);
+        const float p0 = d0[0] * wx + d0[1] * wy + d0[2] * wz;
+        const float p1 = d1[0] * wx + d1[1] * wy + d1[2] * wz;
+        r.x = fmaf(p0, v.x, r.x);
+        r.y = fmaf(-p0, v.y, r.y);
+        r.z = fmaf(p1, v.z, r.z);
+        r.w = fmaf(-p1, v.w, r.w);
+    }
+    const float4 kv = make_float4(-r.x, -r.y, -r.z, -r.w);
+    const float4 f0 = ld4(S.G, i, QP, c);
+    if (STAGE == 1) {
+        st4(S.G1, i, QP, c, make_float4(fmaf(S.a_half, kv.x, f0.x), fmaf(S.a_half, kv.y, f0.y),
+                                        fmaf(S.a_half, kv.z, f0.z), fmaf(S.a_half, kv.w, f0.w)));
+        st4(S.ACC, i, QP, c, make_float4(kv.x * S.b1, kv.y * S.b1, kv.z * S.b1, kv.w * S.b1));
+    } else {
+        const float4 acc = ld4rw(S.ACC, i, QP, c);
+        if (STAGE == 4) {
+            const float4 df = make_float4(acc.x + kv.x * S.b1, acc.y + kv.y * S.b1, acc.z + kv.z * S.b1,
+                                          acc.w + kv.w * S.b1);
+            st4(S.G, i, QP, c, make_float4(fmaf(S.a_full, df.x, f0.x), fmaf(S.a_full, df.y, f0.y),
+                                           fmaf(S.a_full, df.z, f0.z), fmaf(S.a_full, df.w, f0.w)));
         } else {
-            float acc[L::QP];
-            load_row_rw<L>(S.ACC, i, acc);
-            if (STAGE == 4) {
-#pragma unroll
-                for (int a = 0; a < Q; ++a) {
-                    const float kv = -r[a];
-                    const float df = acc[a] + kv * S.b1;
-                    out[a] = fmaf(S.a_full, df, f0[a]);
-                }
-                store_row<L>(S.G, i, out);
-            } else {
-#pragma unroll
-                for (int a = 0; a < Q; ++a) {
-                    const float kv = -r[a];
-                    out[a] = fmaf(STAGE == 2 ? S.a_half : S.a_full, kv, f0[a]);
-                    acc[a] = acc[a] + kv * S.b2;
-                }
-                store_row<L>(STAGE == 2 ? S.G2 : S.G1, i, out);
-                store_row<L>(S.ACC, i, acc);
-            }
+            const float a = STAGE == 2 ? S.a_half : S.a_full;
+            st4(STAGE == 2 ? S.G2 : S.G1, i, QP, c,
+                make_float4(fmaf(a, kv.x, f0.x), fmaf(a, kv.y, f0.y), fmaf(a, kv.z, f0.z), fmaf(a, kv.w, f0.w)));
+            st4(S.ACC, i, QP, c, make_float4(acc.x + kv.x * S.b2, acc.y + kv.y * S.b2, acc.z + kv.z * S.b2,
+                                             acc.w + kv.w * S.b2));
         }
     }
+    NAGA_MT_END
     NAGA_END_ITEMS
 }
 
 // boundary: f = interp(f of bulk + layer) (simulation_engine.cuh:1370)
 template <class L>
-__global__ void __launch_bounds__(kBlock) k_edge_interp(const WorkItem* __restrict__ items, int nitems,
-                                                        const SceneDev* __restrict__ scenes) {
-    constexpr int Q = L::Q;
+__global__ void __launch_bounds__(kBlockMT) k_edge_interp(const WorkItem* __restrict__ items, int nitems,
+                                                          const SceneDev* __restrict__ scenes) {
+    using G = MT<L>;
+    constexpr int QP = L::QP;
     NAGA_FOR_ITEMS(items, nitems)
+    NAGA_MT_NODES(G)
     const int64_t b = i - S.nbl;
-    if (active && b < S.nbd) {
-        float acc[L::QP];
-#pragma unroll
-        for (int a = 0; a < L::QP; ++a) acc[a] = 0.f;
+    if (b < S.nbd) {
+        float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
         for (int s = 0; s < S.kb; ++s) {
             const uint32_t j = __ldg(S.bidx + (int64_t)s * S.nbd + b);
             const float w = __ldg(S.bw + (int64_t)s * S.nbd + b);
-            float v[L::QP];
-            load_row<L>(S.G, j, v);
-#pragma unroll
-            for (int a = 0; a < Q; ++a) acc[a] = fmaf(w, v[a], acc[a]);
+            const float4 v = ld4rw(S.G, j, QP, c);
+            acc.x = fmaf(w, v.x, acc.x);
+            acc.y = fmaf(w, v.y, acc.y);
+            acc.z = fmaf(w, v.z, acc.z);
+            acc.w = fmaf(w, v.w, acc.w);
         }
-        store_row<L>(S.G, i, acc);
+        st4(S.G, i, QP, c, acc);
     }
+    NAGA_MT_END
     NAGA_END_ITEMS
 }
 
@@ -772,15 +789,15 @@ enum {
 };
 
 const char* kernel_name(int id) {
-    static const char* names[K_COUNT] = {"macro_pml", "pml_means", "probe", "pml_collide", "edge_collide", "filter",
+    static const char* names[K_COUNT] = {"macro_pml", "pml_means", "probe", "pml_gather", "edge_collide", "filter",
                                          "rk_stage1", "rk_stage2", "rk_stage3", "rk_stage4", "edge_interp",
                                          "step_end"};
     return (id >= 0 && id < K_COUNT) ? names[id] : "?";
 }
 int kernel_count() { return K_COUNT; }
 
-template <class L>
-int enqueue_step_t(const StepLaunch& P, cudaStream_t st) {
+template <class L, int K>
+int enqueue_step_k(const StepLaunch& P, cudaStream_t st) {
     const int cap = sm_count() * 8;
     auto grid = [&](int n) { return n < cap ? n : cap; };
     const bool prof = prof_on();
@@ -791,26 +808,35 @@ int enqueue_step_t(const StepLaunch& P, cudaStream_t st) {
         if (prof) prof_end(id, st);             \
     }
     LAUNCH(K_MACRO, P.n_all, (k_macro_pml<L><<<grid(P.n_all), kBlock, 0, st>>>(P.all, P.n_all, P.scenes)));
-    LAUNCH(K_MEANS, P.nscenes, (k_pml_means<L::Q><<<P.nscenes, 64, 0, st>>>(P.scenes)));
+    LAUNCH(K_MEANS, P.nscenes, (k_pml_means<L::QP><<<dim3(P.nscenes, 2 * L::QP), 256, 0, st>>>(P.scenes)));
     LAUNCH(K_PROBE, P.nscenes, (k_probe<<<P.nscenes, 128, 0, st>>>(P.scenes)));
-    LAUNCH(K_PML, P.n_fluid, (k_pml_collide<L><<<grid(P.n_fluid), kBlock, 0, st>>>(P.fluid, P.n_fluid, P.scenes)));
+    LAUNCH(K_PML, P.n_pml, (k_pml_gather<L, K><<<grid(P.n_pml), kBlockMT, 0, st>>>(P.pml, P.n_pml, P.scenes)));
     LAUNCH(K_EDGE_COLLIDE, P.n_edge,
-           (k_edge_collide<L><<<grid(P.n_edge), kBlock, 0, st>>>(P.edge, P.n_edge, P.scenes)));
-    LAUNCH(K_FILTER, P.n_all, (k_filter<L><<<grid(P.n_all), kBlock, 0, st>>>(P.all, P.n_all, P.scenes)));
-    LAUNCH(K_RK1, P.n_fluid, (k_rk<L, 1><<<grid(P.n_fluid), kBlock, 0, st>>>(P.fluid, P.n_fluid, P.scenes)));
-    LAUNCH(K_RK2, P.n_fluid, (k_rk<L, 2><<<grid(P.n_fluid), kBlock, 0, st>>>(P.fluid, P.n_fluid, P.scenes)));
-    LAUNCH(K_RK3, P.n_fluid, (k_rk<L, 3><<<grid(P.n_fluid), kBlock, 0, st>>>(P.fluid, P.n_fluid, P.scenes)));
-    LAUNCH(K_RK4, P.n_fluid, (k_rk<L, 4><<<grid(P.n_fluid), kBlock, 0, st>>>(P.fluid, P.n_fluid, P.scenes)));
+           (k_edge_collide<L><<<grid(P.n_edge), kBlockMT, 0, st>>>(P.edge, P.n_edge, P.scenes)));
+    LAUNCH(K_FILTER, P.n_all, (k_filter<L, K><<<grid(P.n_all), kBlockMT, 0, st>>>(P.all, P.n_all, P.scenes)));
+    LAUNCH(K_RK1, P.n_fluid, (k_rk<L, K, 1><<<grid(P.n_fluid), kBlockMT, 0, st>>>(P.fluid, P.n_fluid, P.scenes)));
+    LAUNCH(K_RK2, P.n_fluid, (k_rk<L, K, 2><<<grid(P.n_fluid), kBlockMT, 0, st>>>(P.fluid, P.n_fluid, P.scenes)));
+    LAUNCH(K_RK3, P.n_fluid, (k_rk<L, K, 3><<<grid(P.n_fluid), kBlockMT, 0, st>>>(P.fluid, P.n_fluid, P.scenes)));
+    LAUNCH(K_RK4, P.n_fluid, (k_rk<L, K, 4><<<grid(P.n_fluid), kBlockMT, 0, st>>>(P.fluid, P.n_fluid, P.scenes)));
     LAUNCH(K_EDGE_INTERP, P.n_edge,
-           (k_edge_interp<L><<<grid(P.n_edge), kBlock, 0, st>>>(P.edge, P.n_edge, P.scenes)));
+           (k_edge_interp<L><<<grid(P.n_edge), kBlockMT, 0, st>>>(P.edge, P.n_edge, P.scenes)));
     LAUNCH(K_STEP_END, P.nscenes, (k_step_end<<<(P.nscenes + 127) / 128, 128, 0, st>>>(P.scenes, P.nscenes)));
 #undef LAUNCH
     NAGA_CUDA_TRY(cudaGetLastError());
     return NAGA_OK;
 }
 
-int enqueue_step(int dim, const StepLaunch& P, cudaStream_t st) {
-    return dim == 2 ? enqueue_step_t<D2Q9>(P, st) : enqueue_step_t<D3Q27>(P, st);
+// k is uniform over a batch (scenes of one batch share k); the common
+// stencil sizes get a fully unrolled gather
+int enqueue_step(int dim, int k, const StepLaunch& P, cudaStream_t st) {
+    if (dim == 2) {
+        if (k == 16) return enqueue_step_k<D2Q9, 16>(P, st);
+        if (k == 32) return enqueue_step_k<D2Q9, 32>(P, st);
+        return enqueue_step_k<D2Q9, 0>(P, st);
+    }
+    if (k == 32) return enqueue_step_k<D3Q27, 32>(P, st);
+    if (k == 16) return enqueue_step_k<D3Q27, 16>(P, st);
+    return enqueue_step_k<D3Q27, 0>(P, st);
 }
 
 }  // namespace naga

@@ -93,3 +93,14 @@ def test_scene_argument_validation_precedes_device(naga):
     with pytest.raises(naga.NagaError) as e:
         naga.Scene(g, k=16, pml_indexing=5)
     assert e.value.code == naga.NAGA_EINVAL
+
+
+def test_cpp_facade_compiles():
+    import shutil
+    import subprocess
+
+    gxx = shutil.which("g++-13") or shutil.which("g++")
+    src = os.path.join(ROOT, "tests", "cpp", "facade_pulse.cpp")
+    r = subprocess.run([gxx, "-std=c++17", "-fsyntax-only", f"-I{ROOT}/include", "-I/usr/local/cuda/include",
+                        src], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr

@@ -1,0 +1,37 @@
+"""The header-only C++ facade (include/naga/naga.hpp): a NAGA-style driver
+program compiled with g++, linked against libnaga_b200.so and run."""
+import os
+import shutil
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+pytestmark = pytest.mark.gpu
+
+
+def test_facade_program_matches_python_binding(naga):
+    gxx = shutil.which("g++-13") or shutil.which("g++")
+    with tempfile.TemporaryDirectory() as d:
+        exe = os.path.join(d, "facade_pulse")
+        r = subprocess.run([gxx, "-std=c++17", "-O2", f"-I{ROOT}/include", "-I/usr/local/cuda/include",
+                            os.path.join(ROOT, "tests", "cpp", "facade_pulse.cpp"), "-o", exe,
+                            f"-L{os.path.dirname(naga.LIB_PATH)}", "-lnaga_b200",
+                            f"-Wl,-rpath,{os.path.dirname(naga.LIB_PATH)}", "-L/usr/local/cuda/lib64",
+                            "-lcudart"], capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+        out = subprocess.run([exe, "15"], capture_output=True, text=True, timeout=120)
+        assert out.returncode == 0, out.stderr
+    rows = np.array([[float(v) for v in l.split()] for l in out.stdout.strip().splitlines()])
+    g = naga.generate_grid(2, 40, 4, 0)
+    s = naga.Scene(g, k=16, shape=1, probes=np.array([[0.3, 0.5], [0.7, 0.5]], np.float32))
+    P = g["points"].astype(np.float64)
+    drho = (1e-3 * np.exp(-((P - 0.5) ** 2).sum(1) / (2 * 0.08 ** 2))).astype(np.float32)
+    s.set_density(drho)
+    s.step(15)
+    p = s.probes(0, 15)
+    assert np.allclose(rows[:, 1:], p, rtol=0, atol=1e-7 * max(1.0, np.abs(p).max()) + 2e-7)
+    assert np.allclose(rows[:, 0], np.arange(15) * 0.5 * g["h"], rtol=1e-5)
