@@ -83,8 +83,8 @@ def kernel_bytes(dim, N, nb, nl, nbd, k, kb):
     st = 4 * k * (dim + 1)  # weights + index per neighbour
     nbl = nb + nl
     return {
-        "macro_pml": N * (3 * row + 32),
-        "pml_collide": nbl * (2 * row + st) + nl * 2 * row,
+        "macro_pml": N * (4 * row + 32),
+        "pml_gather": nbl * (st + 2 * row) + nl * 2 * row,
         "edge_collide": nbd * (2 * row + 8 * kb),
         "filter": N * 2 * row + nbl * 8 * k,
         "rk_stage1": nbl * (st + 3 * row),
@@ -225,6 +225,9 @@ def run_naga(args, rank, world, local_rank):
 
     import naga_b200 as naga
 
+    global CONFIG3
+    if args.n_side != CONFIG3["n_side"]:
+        CONFIG3 = dict(CONFIG3, n_side=args.n_side)
     torch.cuda.set_device(local_rank)
     dist = None
     if world > 1:
@@ -351,6 +354,9 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batched-scenes", type=int, default=256)
+    ap.add_argument("--n-side", type=int, default=63,
+                    help="grid nodes per side of the 3-D scene (63 = the benchmark workload; "
+                         "smaller values give profiling cases)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = _env_int("RANK", 0)

@@ -231,6 +231,49 @@ void* naga_batch_stream(naga_batch* batch);
 int naga_batch_step(naga_batch* batch, int nsteps);
 int naga_batch_sync(naga_batch* batch);
 
+/* --------------------------------------------------------------- serving */
+/* Continuous-batching request loop: requests (a scene and a step count)
+ * queue FIFO; every naga_server_tick advances all active scenes by
+ * steps_per_tick steps as one batch while queued requests that fit the
+ * device-memory budget and the slot limit are set up on their own streams,
+ * then retires finished requests (their probe traces kept on the host) and
+ * admits the new ones into the batch. No reference counterpart: NAGA steps
+ * one engine at a time (simulation_engine.cuh:76).                        */
+typedef struct naga_server naga_server;
+
+typedef struct naga_server_config {
+    int dim;               /* lattice of every request                       */
+    int steps_per_tick;    /* steps per tick (>= 1)                          */
+    int max_active;        /* scene slots, 0 = limited by memory only        */
+    int _reserved;
+    int64_t memory_budget; /* device bytes the active scenes may hold        */
+} naga_server_config;
+
+typedef struct naga_server_stats {
+    int64_t ticks, steps, node_updates;
+    double busy_ms;         /* device time of the batch steps               */
+    double p50_step_ms, p99_step_ms;
+    int64_t bytes_in_use, peak_bytes;
+    int64_t done, failed;
+    int active, queued;
+} naga_server_stats;
+
+/* estimated device bytes of a scene (resident state plus set-up scratch)  */
+int64_t naga_scene_estimate_bytes(const naga_scene_desc* desc);
+int naga_server_create(const naga_server_config* cfg, naga_server** out);
+int naga_server_destroy(naga_server* server);
+/* copies the host inputs; drho as in naga_scene_set_density; probe
+ * capacity is set from steps                                              */
+int naga_server_submit(naga_server* server, const naga_scene_desc* desc,
+                       const float* drho, int64_t steps, int64_t* id);
+int naga_server_tick(naga_server* server, int* n_active, int* n_queued);
+/* state: 0 queued, 1 active, 2 done, 3 failed (naga_last_error has why)  */
+int naga_server_request_state(naga_server* server, int64_t id, int* state,
+                              int64_t* steps_done);
+/* probe trace of a finished request, host [steps][n_probes]; releases it  */
+int naga_server_result(naga_server* server, int64_t id, float* probes);
+int naga_server_read_stats(naga_server* server, naga_server_stats* out);
+
 /* ---------------------------------------------------------------- timing */
 /* Per-kernel CUDA-event timing of the step kernels (off by default).
  * When on, every step kernel launch is bracketed by events on the stream

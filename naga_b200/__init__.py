@@ -98,6 +98,14 @@ _SIGS = {
     "naga_batch_stream": ([C.c_void_p], C.c_void_p),
     "naga_batch_step": ([C.c_void_p, C.c_int], C.c_int),
     "naga_batch_sync": ([C.c_void_p], C.c_int),
+    "naga_scene_estimate_bytes": ([C.c_void_p], C.c_int64),
+    "naga_server_create": ([C.c_void_p, C.c_void_p], C.c_int),
+    "naga_server_destroy": ([C.c_void_p], C.c_int),
+    "naga_server_submit": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p], C.c_int),
+    "naga_server_tick": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "naga_server_request_state": ([C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p], C.c_int),
+    "naga_server_result": ([C.c_void_p, C.c_int64, C.c_void_p], C.c_int),
+    "naga_server_read_stats": ([C.c_void_p, C.c_void_p], C.c_int),
     "naga_profile_enable": ([C.c_int], C.c_int),
     "naga_profile_reset": ([], C.c_int),
     "naga_profile_read": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
@@ -299,6 +307,96 @@ class Batch:
     def close(self):
         if getattr(self, "h", None) is not None and self.h.value:
             lib().naga_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------- serving
+class ServerConfig(C.Structure):
+    _fields_ = [("dim", C.c_int), ("steps_per_tick", C.c_int), ("max_active", C.c_int),
+                ("_reserved", C.c_int), ("memory_budget", C.c_int64)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("ticks", C.c_int64), ("steps", C.c_int64), ("node_updates", C.c_int64),
+                ("busy_ms", C.c_double), ("p50_step_ms", C.c_double), ("p99_step_ms", C.c_double),
+                ("bytes_in_use", C.c_int64), ("peak_bytes", C.c_int64), ("done", C.c_int64),
+                ("failed", C.c_int64), ("active", C.c_int), ("queued", C.c_int)]
+
+
+def scene_desc(grid: dict, *, k: int, k_boundary=None, k_probe=None, shape=1, pml_indexing=0,
+               weight_precision=0, viscosity=1e-5, rho0=1.0, time_step=None, speed_of_sound=1.0,
+               probes=None, probe_capacity=4096, n_ghost=0):
+    """A naga_scene_desc for `grid`; returns (desc, arrays it points into)."""
+    dim = grid["dim"]
+    keep = [np.ascontiguousarray(grid["points"], np.float32),
+            np.ascontiguousarray(grid["normals"], np.float32),
+            np.ascontiguousarray(grid["sigma"], np.float32),
+            np.ascontiguousarray(probes if probes is not None else np.zeros((0, dim)), np.float32)]
+    d = SceneDesc()
+    d.dim, d.k = dim, k
+    d.k_boundary = k_boundary or k
+    d.k_probe = k_probe or k
+    d.shape, d.pml_indexing, d.weight_precision = shape, pml_indexing, weight_precision
+    d.n_probes = keep[3].shape[0]
+    d.n_bulk, d.n_layer, d.n_boundary = grid["n_bulk"], grid["n_layer"], grid["n_boundary"]
+    d.n_ghost = n_ghost
+    d.nodal_spacing = grid["h"]
+    d.viscosity, d.rho0, d.speed_of_sound = viscosity, rho0, speed_of_sound
+    d.time_step = time_step if time_step is not None else 0.5 * grid["h"] / speed_of_sound
+    d.points, d.normals, d.sigma, d.probes = (_p(a) for a in keep)
+    d.probe_capacity = probe_capacity
+    return d, keep
+
+
+class Server:
+    """Continuous-batching request loop (naga_server_* in include/naga_b200.h)."""
+
+    QUEUED, ACTIVE, DONE, FAILED = 0, 1, 2, 3
+
+    def __init__(self, dim: int, memory_budget: int, steps_per_tick: int = 50, max_active: int = 0):
+        self.h = C.c_void_p()
+        cfg = ServerConfig(dim, steps_per_tick, max_active, 0, memory_budget)
+        _check(lib().naga_server_create(C.byref(cfg), C.byref(self.h)))
+        self.n_probes = {}
+
+    def submit(self, grid: dict, drho, steps: int, **kw) -> int:
+        d, keep = scene_desc(grid, **kw)
+        rid = C.c_int64()
+        drho = None if drho is None else np.ascontiguousarray(drho, np.float32)
+        _check(lib().naga_server_submit(self.h, C.byref(d), _p(drho), steps, C.byref(rid)))
+        self.n_probes[rid.value] = (d.n_probes, steps)
+        return rid.value
+
+    def tick(self):
+        a, q = C.c_int(), C.c_int()
+        _check(lib().naga_server_tick(self.h, C.byref(a), C.byref(q)))
+        return a.value, q.value
+
+    def state(self, rid: int):
+        st, done = C.c_int(), C.c_int64()
+        _check(lib().naga_server_request_state(self.h, rid, C.byref(st), C.byref(done)))
+        return st.value, done.value
+
+    def result(self, rid: int) -> np.ndarray:
+        np_, steps = self.n_probes.pop(rid)
+        out = np.zeros((steps, np_), np.float32)
+        _check(lib().naga_server_result(self.h, rid, _p(out)))
+        return out
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(lib().naga_server_read_stats(self.h, C.byref(st)))
+        return {n: getattr(st, n) for n, _ in ServerStats._fields_}
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            lib().naga_server_destroy(self.h)
             self.h = None
 
     def __del__(self):
