@@ -87,6 +87,24 @@ int naga_gaussian_pulse(const float* points, int64_t n, int dim,
 int naga_knn(const float* src, int64_t n, const float* qry, int64_t nq,
              int dim, int k, uint32_t* idx, float* d2, void* stream);
 
+/* The same search without allocating device memory, for callers that
+ * cannot call cudaMalloc while they run: processes that handed the free
+ * device memory to their own caching allocator at start-up and live on a
+ * fixed budget, and latency-critical paths where cudaMalloc / cudaFree may
+ * synchronise the device and stall other streams. No reference counterpart
+ * (NAGA allocates its segmentation arrays on every call).
+ * Scratch is one fixed device array of ~1.8 MB inside the library, held by
+ * every GPU that loads it until the process exits; hence n <= 65536 source
+ * points (larger n returns NAGA_EINVAL), any number of queries. The first
+ * call on a device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * Every call shares the one array: calls that overlap on the GPU (other
+ * streams, other host threads) race, so serialise them. Each call resets
+ * the counters it needs. Results equal naga_knn's bit for bit.             */
+int naga_knn_noalloc(const float* src, int64_t n, const float* qry,
+                     int64_t nq, int dim, int k, uint32_t* idx, float* d2,
+                     void* stream);
+
 /* Self-kNN of many independent clouds in one launch. pts: device
  * [total][dim], clouds back to back; offsets: host [n_clouds + 1]. Output
  * indices are local to each cloud. No reference counterpart as a single

@@ -64,6 +64,8 @@ _SIGS = {
                              C.c_void_p], C.c_int),
     "naga_knn": ([C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_void_p,
                   C.c_void_p, C.c_void_p], C.c_int),
+    "naga_knn_noalloc": ([C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_void_p,
+                          C.c_void_p, C.c_void_p], C.c_int),
     "naga_knn_clouds": ([C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
                          C.c_void_p], C.c_int),
     "naga_batched_inverse_f64": ([C.c_void_p, C.c_void_p, C.c_int, C.c_int64, C.c_void_p, C.c_void_p],

@@ -25,6 +25,8 @@
 #include <cub/device/device_scan.cuh>
 
 #include <cmath>
+#include <mutex>
+#include <string>
 #include <vector>
 
 namespace naga {
@@ -432,9 +434,180 @@ int knn_device(const float* src, int64_t n, const float* qry, int64_t nq, int di
                     : knn_run<3>(src, off, 1, qry, nq, nullptr, k, idx, d2, st);
 }
 
+// ----------------------------------------------- allocation-free variant
+// Some callers cannot call cudaMalloc once they are running: processes that
+// hand all free device memory to their own caching allocator at start-up
+// and run on a fixed budget, and latency-critical serving paths, where
+// cudaMalloc / cudaFree may synchronise the device and stall every other
+// stream. naga_knn_noalloc serves them: its scratch (cell grid, counting
+// sort, sorted point records) lives in one file-scope device array that every
+// GPU loading this library holds until the process exits. The array's
+// host-side name is only a stand-in; its device address is looked up once
+// per device with cudaGetSymbolAddress.
+namespace {
+
+constexpr int64_t kNoAllocMaxPoints = 65536;  // largest source cloud
+constexpr int64_t kNoAllocMaxCells = 65536;   // cap on the cell grid
+
+struct NoAllocScratch {
+    int bbox[8];
+    int64_t offsets[2];
+    CloudGrid grid;
+    unsigned counts[kNoAllocMaxCells + 1];
+    unsigned start[kNoAllocMaxCells + 1];
+    unsigned fill[kNoAllocMaxCells + 1];
+    float4 sorted[kNoAllocMaxPoints];
+};
+
+static __device__ __align__(256) unsigned char g_knn_scratch[sizeof(NoAllocScratch)];
+
+// device address of g_knn_scratch for the current device, looked up once
+int noalloc_scratch(NoAllocScratch** out) {
+    static std::mutex mu;
+    static void* addr[64] = {nullptr};
+    int dev = 0;
+    NAGA_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return set_error(NAGA_EINVAL, "naga_knn_noalloc: device ordinal above 63");
+    std::lock_guard<std::mutex> lk(mu);
+    if (!addr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_knn_scratch);
+        if (e != cudaSuccess)
+            return set_error(NAGA_ECUDA, std::string("naga_knn_noalloc: cudaGetSymbolAddress: ") +
+                                             cudaGetErrorString(e));
+        addr[dev] = p;
+    }
+    *out = reinterpret_cast<NoAllocScratch*>(addr[dev]);
+    return NAGA_OK;
+}
+
+// resets what must start at zero and the bounding box of a new call
+__global__ void noalloc_init_kernel(NoAllocScratch* s, int64_t n) {
+    const int64_t t0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    for (int64_t t = t0; t <= kNoAllocMaxCells; t += (int64_t)gridDim.x * blockDim.x) {
+        s->counts[t] = 0u;
+        s->fill[t] = 0u;
+    }
+    if (t0 < 3) {
+        s->bbox[t0] = 0x7fffffff;
+        s->bbox[3 + t0] = (int)0x80000000;
+    }
+    if (t0 == 0) {
+        s->offsets[0] = 0;
+        s->offsets[1] = n;
+    }
+}
+
+__global__ void noalloc_set_grid_kernel(NoAllocScratch* s, CloudGrid g) { s->grid = g; }
+
+// exclusive scan of counts[0, m) into start[0, m) by one block
+__global__ void noalloc_scan_kernel(NoAllocScratch* s, int m) {
+    __shared__ unsigned part[1024];
+    const int t = threadIdx.x;
+    const int per = (m + blockDim.x - 1) / blockDim.x;
+    const int b = t * per, e = min(m, b + per);
+    unsigned acc = 0;
+    for (int i = b; i < e; ++i) acc += s->counts[i];
+    part[t] = acc;
+    __syncthreads();
+    for (int o = 1; o < (int)blockDim.x; o <<= 1) {
+        unsigned v = t >= o ? part[t - o] : 0u;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    unsigned run = part[t] - acc;
+    for (int i = b; i < e; ++i) {
+        s->start[i] = run;
+        run += s->counts[i];
+    }
+}
+
+template <int D>
+int knn_noalloc_run(const float* src, int64_t n, const float* qry, int64_t nq, int k, uint32_t* idx, float* d2,
+                    cudaStream_t st) {
+    NoAllocScratch* scr = nullptr;
+    int rc = noalloc_scratch(&scr);
+    if (rc) return rc;
+    noalloc_init_kernel<<<64, 256, 0, st>>>(scr, n);
+    NAGA_CUDA_TRY(cudaGetLastError());
+    if (n > 0) {
+        const int blocks = (int)std::min<int64_t>((n + 255) / 256, 4 * 148 * 8);
+        bbox_kernel<D><<<blocks, 256, 0, st>>>(src, scr->offsets, 1, n, scr->bbox);
+        NAGA_CUDA_TRY(cudaGetLastError());
+    }
+    int hb[6];
+    NAGA_CUDA_TRY(cudaMemcpyAsync(hb, scr->bbox, sizeof(hb), cudaMemcpyDeviceToHost, st));
+    NAGA_CUDA_TRY(cudaStreamSynchronize(st));
+    CloudGrid g{};
+    double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0}, vol = 1;
+    for (int d = 0; d < D; ++d) {
+        lo[d] = n > 0 ? (double)ord2f(hb[d]) : 0.0;
+        hi[d] = n > 0 ? (double)ord2f(hb[3 + d]) : 1.0;
+        if (hi[d] - lo[d] < 1e-6) hi[d] = lo[d] + 1e-6;
+        vol *= hi[d] - lo[d];
+    }
+    double w = std::pow(2.0 * vol / (double)std::max<int64_t>(n, 1), 1.0 / D);
+    int64_t cells = 0;
+    for (;;) {
+        cells = 1;
+        for (int d = 0; d < 3; ++d) {
+            const int64_t dd = d < D ? std::max<int64_t>(1, (int64_t)std::ceil((hi[d] - lo[d]) / w)) : 1;
+            g.dims[d] = (int)std::min<int64_t>(dd, 1 << 20);
+            cells *= g.dims[d];
+        }
+        if (cells <= kNoAllocMaxCells) break;
+        w *= 1.25;  // coarser cells: the search stays exact, only slower
+    }
+    for (int d = 0; d < 3; ++d) g.lo[d] = lo[d];
+    g.w = w;
+    g.cell_base = 0;
+    g.pt_base = 0;
+    g.n = n;
+    noalloc_set_grid_kernel<<<1, 1, 0, st>>>(scr, g);
+    if (n > 0) {
+        const int blocks = (int)std::min<int64_t>((n + 255) / 256, 4 * 148 * 8);
+        count_kernel<D><<<blocks, 256, 0, st>>>(src, scr->offsets, 1, n, &scr->grid, scr->counts);
+        noalloc_scan_kernel<<<1, 1024, 0, st>>>(scr, (int)cells + 1);
+        scatter_kernel<D><<<blocks, 256, 0, st>>>(src, scr->offsets, 1, n, &scr->grid, scr->start, scr->fill,
+                                                  scr->sorted);
+    } else {
+        noalloc_scan_kernel<<<1, 1024, 0, st>>>(scr, (int)cells + 1);
+    }
+    NAGA_CUDA_TRY(cudaGetLastError());
+    if (nq > 0) {
+        const int blocks = (int)std::min<int64_t>((nq + 7) / 8, (int64_t)sm_count() * 16);
+        if (k <= 32)
+            query_kernel<D, 1><<<blocks, 256, 0, st>>>(qry, nq, nullptr, 1, &scr->grid, scr->start, scr->sorted, k,
+                                                       idx, d2);
+        else
+            query_kernel<D, 2><<<blocks, 256, 0, st>>>(qry, nq, nullptr, 1, &scr->grid, scr->start, scr->sorted, k,
+                                                       idx, d2);
+        NAGA_CUDA_TRY(cudaGetLastError());
+    }
+    return NAGA_OK;
+}
+
+}  // namespace
+
 }  // namespace naga
 
 using namespace naga;
+
+extern "C" int naga_knn_noalloc(const float* src, int64_t n, const float* qry, int64_t nq, int dim, int k,
+                                uint32_t* idx, float* d2, void* stream) {
+    if (dim != 2 && dim != 3) return set_error(NAGA_EINVAL, "naga_knn_noalloc: dim must be 2 or 3");
+    if (k < 1 || k > 64) return set_error(NAGA_EINVAL, "naga_knn_noalloc: k must be in [1, 64]");
+    if (n < 0 || nq < 0) return set_error(NAGA_EINVAL, "naga_knn_noalloc: negative size");
+    if (n > kNoAllocMaxPoints)
+        return set_error(NAGA_EINVAL, "naga_knn_noalloc: " + std::to_string(n) +
+                                          " source points exceed the fixed scratch of 65536 points; use naga_knn");
+    if ((n > 0 && !src) || (nq > 0 && (!qry || !idx || !d2)))
+        return set_error(NAGA_EINVAL, "naga_knn_noalloc: null pointer");
+    cudaStream_t st = (cudaStream_t)stream;
+    return dim == 2 ? knn_noalloc_run<2>(src, n, qry, nq, k, idx, d2, st)
+                    : knn_noalloc_run<3>(src, n, qry, nq, k, idx, d2, st);
+}
 
 extern "C" int naga_knn(const float* src, int64_t n, const float* qry, int64_t nq, int dim, int k,
                         uint32_t* idx, float* d2, void* stream) {
