@@ -92,7 +92,7 @@ struct naga_scene {
     SceneDev dev{};
     std::vector<void*> allocs;
     int64_t bytes = 0;
-    std::vector<WorkItem> items_all, items_fluid, items_edge, items_pml;  // scene slot 0
+    std::vector<WorkItem> items_all, items_all_mt, items_fluid, items_edge, items_pml;  // scene slot 0
     naga_batch* owner = nullptr;                               // user batch, if any
     naga_batch* solo = nullptr;                                // private batch for naga_scene_step
     int64_t steps = 0;                                         // host mirror of the device counter
@@ -121,9 +121,9 @@ struct naga_batch {
     bool dirty = true;
     cudaStream_t stream = nullptr;
     SceneDev* d_scenes = nullptr;
-    WorkItem *d_all = nullptr, *d_fluid = nullptr, *d_edge = nullptr, *d_pml = nullptr;
-    int n_all = 0, n_fluid = 0, n_edge = 0, n_pml = 0;
-    int k = 0;  // common stencil size of the members (0 if they differ)
+    WorkItem *d_all = nullptr, *d_all_mt = nullptr, *d_fluid = nullptr, *d_edge = nullptr, *d_pml = nullptr;
+    int n_all = 0, n_all_mt = 0, n_fluid = 0, n_edge = 0, n_pml = 0;
+    int k = 0, kb = 0;  // common stencil sizes of the members (0 if they differ)
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
 
@@ -137,8 +137,9 @@ struct naga_batch {
         if (d_fluid) cudaFree(d_fluid);
         if (d_edge) cudaFree(d_edge);
         if (d_pml) cudaFree(d_pml);
+        if (d_all_mt) cudaFree(d_all_mt);
         d_scenes = nullptr;
-        d_all = d_fluid = d_edge = d_pml = nullptr;
+        d_all = d_all_mt = d_fluid = d_edge = d_pml = nullptr;
     }
 };
 
@@ -156,11 +157,11 @@ int check_device() {
     return NAGA_OK;
 }
 
-void make_items(int64_t begin, int64_t end, std::vector<WorkItem>& out) {
+void make_items(int64_t begin, int64_t end, std::vector<WorkItem>& out, int size = 128) {
     out.clear();
     uint32_t local = 0;
-    for (int64_t b = begin; b < end; b += 128)
-        out.push_back({0u, (uint32_t)b, (uint32_t)std::min<int64_t>(end, b + 128), local++});
+    for (int64_t b = begin; b < end; b += size)
+        out.push_back({0u, (uint32_t)b, (uint32_t)std::min<int64_t>(end, b + size), local++});
 }
 
 // slot of population a in a node row (paired order, see common.cuh)
@@ -254,41 +255,30 @@ int scene_setup(naga_scene* s) {
     // divergence stencil + filter weights over the domain [0, nd)
     const int k = d.k;
     StencilOut out{};
-    out.ld = N;
     out.filter_sigma = d.nodal_spacing / 2.5;
     uint32_t* knn_idx = nullptr;
     if ((rc = s->alloc(&knn_idx, s->nd * k))) return rc;
+    float4* W = nullptr;
+    if ((rc = s->alloc(&W, (int64_t)k * N))) return rc;
+    NAGA_CUDA_TRY(cudaMemsetAsync(W, 0, sizeof(float4) * k * N, st));
+    out.Wf = W;
+    V.stW = W;
+    V.stF = nullptr;
     if (D == 3) {
-        float4* W = nullptr;
-        if ((rc = s->alloc(&W, (int64_t)k * N))) return rc;
-        NAGA_CUDA_TRY(cudaMemsetAsync(W, 0, sizeof(float4) * k * N, st));
-        out.Wf = reinterpret_cast<float*>(W);
-        V.stW = W;
-        V.stI = nullptr;
-    } else {
-        float2* W = nullptr;
-        uint32_t* I = nullptr;
-        if ((rc = s->alloc(&W, (int64_t)k * N))) return rc;
-        if ((rc = s->alloc(&I, (int64_t)k * N))) return rc;
-        NAGA_CUDA_TRY(cudaMemsetAsync(W, 0, sizeof(float2) * k * N, st));
-        NAGA_CUDA_TRY(cudaMemsetAsync(I, 0, sizeof(uint32_t) * k * N, st));
-        out.Wf = reinterpret_cast<float*>(W);
-        out.If = I;
-        V.stW = W;
-        V.stI = I;
+        float2* F = nullptr;
+        if ((rc = s->alloc(&F, (int64_t)k * N))) return rc;
+        NAGA_CUDA_TRY(cudaMemsetAsync(F, 0, sizeof(float2) * k * N, st));
+        out.Ff = F;
+        V.stF = F;
     }
-    float2* F = nullptr;
-    if ((rc = s->alloc(&F, (int64_t)k * N))) return rc;
-    NAGA_CUDA_TRY(cudaMemsetAsync(F, 0, sizeof(float2) * k * N, st));
-    out.Ff = F;
-    V.stF = F;
     rc = divergence_build_device(pts, s->nd, D, k, d.shape, d.weight_precision, knn_idx, out, st);
     if (rc) return rc;
 
     // boundary interpolation: kNN among bulk + layer, RPIM at the boundary
     // node with the nodal spacing (detail/simulation_engine.cuh:223-258)
     std::vector<uint8_t> is_src(N, 0);
-    auto rpim = [&](const float* qry_host, int64_t nq, int64_t nsrc, int kk, uint32_t** idx_out, float** w_out) -> int {
+    auto rpim = [&](const float* qry_host, int64_t nq, int64_t nsrc, int kk, uint32_t** idx_out, float** w_out,
+                    float2** rec_out) -> int {
         uint32_t* didx = nullptr;
         float* dd2 = nullptr;
         float* dq = nullptr;
@@ -320,38 +310,46 @@ int scene_setup(naga_scene* s) {
         cudaFreeAsync(dqd, st);
         cudaFreeAsync(dw, st);
         if (r) return r;
-        // transpose to [k][nq] for coalesced per-node reads
-        std::vector<uint32_t> ti(nq * kk);
-        std::vector<float> tw(nq * kk);
-        for (int64_t q = 0; q < nq; ++q)
-            for (int t = 0; t < kk; ++t) {
-                ti[(int64_t)t * nq + q] = hi[q * kk + t];
-                tw[(int64_t)t * nq + q] = (float)hw[q * kk + t];
+        if (idx_out) {
+            // probes: [k][nq] indices and weights
+            std::vector<uint32_t> ti(nq * kk);
+            std::vector<float> tw(nq * kk);
+            for (int64_t q = 0; q < nq; ++q)
+                for (int t = 0; t < kk; ++t) {
+                    ti[(int64_t)t * nq + q] = hi[q * kk + t];
+                    tw[(int64_t)t * nq + q] = (float)hw[q * kk + t];
+                }
+            if ((r = s->alloc(idx_out, nq * kk))) return r;
+            if ((r = s->alloc(w_out, nq * kk))) return r;
+            NAGA_CUDA_TRY(cudaMemcpyAsync(*idx_out, ti.data(), sizeof(uint32_t) * nq * kk, cudaMemcpyHostToDevice, st));
+            NAGA_CUDA_TRY(cudaMemcpyAsync(*w_out, tw.data(), sizeof(float) * nq * kk, cudaMemcpyHostToDevice, st));
+            NAGA_CUDA_TRY(cudaStreamSynchronize(st));
+        } else {
+            // boundary: node-major (weight, index bits) records
+            std::vector<float2> rec(nq * kk);
+            for (int64_t q = 0; q < nq * kk; ++q) {
+                float2 v;
+                v.x = (float)hw[q];
+                std::memcpy(&v.y, &hi[q], 4);
+                rec[q] = v;
+                is_src[hi[q]] = 1;
             }
-        if ((r = s->alloc(idx_out, nq * kk))) return r;
-        if ((r = s->alloc(w_out, nq * kk))) return r;
-        NAGA_CUDA_TRY(cudaMemcpyAsync(*idx_out, ti.data(), sizeof(uint32_t) * nq * kk, cudaMemcpyHostToDevice, st));
-        NAGA_CUDA_TRY(cudaMemcpyAsync(*w_out, tw.data(), sizeof(float) * nq * kk, cudaMemcpyHostToDevice, st));
-        NAGA_CUDA_TRY(cudaStreamSynchronize(st));
-        if (idx_out && nsrc == s->nbl)
-            for (auto j : hi) is_src[j] = 1;
+            if ((r = s->alloc(rec_out, nq * kk))) return r;
+            NAGA_CUDA_TRY(cudaMemcpyAsync(*rec_out, rec.data(), sizeof(float2) * nq * kk, cudaMemcpyHostToDevice, st));
+            NAGA_CUDA_TRY(cudaStreamSynchronize(st));
+        }
         return NAGA_OK;
     };
-    uint32_t* bidx = nullptr;
-    float* bw = nullptr;
+    float2* btab = nullptr;
     if (s->nbd > 0) {
-        if ((rc = rpim(d.points + s->nbl * D, s->nbd, s->nbl, d.k_boundary, &bidx, &bw))) return rc;
+        if ((rc = rpim(d.points + s->nbl * D, s->nbd, s->nbl, d.k_boundary, nullptr, nullptr, &btab))) return rc;
     }
-    V.bidx = bidx;
-    V.bw = bw;
+    V.btab = btab;
     uint32_t* pidx = nullptr;
     float* pw = nullptr;
     if (d.n_probes > 0) {
-        // probes: kNN among all points (density_observer.cuh:62-97); they do
-        // not mark interpolation sources
-        std::vector<uint8_t> keep = is_src;
-        if ((rc = rpim(d.probes, d.n_probes, N, d.k_probe, &pidx, &pw))) return rc;
-        is_src = keep;
+        // probes: kNN among all points (density_observer.cuh:62-97)
+        if ((rc = rpim(d.probes, d.n_probes, N, d.k_probe, &pidx, &pw, nullptr))) return rc;
     }
     V.pidx = pidx;
     V.pw = pw;
@@ -366,9 +364,11 @@ int scene_setup(naga_scene* s) {
     NAGA_CUDA_TRY(cudaMemsetAsync(ring, 0, sizeof(float) * V.probe_cap * std::max(1, d.n_probes), st));
     V.probe_ring = ring;
 
+    const int npb = nodes_per_pass(D);
     make_items(0, N, s->items_all);
-    make_items(0, s->nbl, s->items_fluid);
-    make_items(s->nbl, N, s->items_edge);
+    make_items(0, N, s->items_all_mt, npb);
+    make_items(0, s->nbl, s->items_fluid, npb);
+    make_items(s->nbl, s->nbl + s->nbd, s->items_edge, npb);
     // bulk/layer items with at least one stencil support in the layer
     s->items_pml.clear();
     if (s->nl > 0) {
@@ -405,11 +405,17 @@ int scene_setup(naga_scene* s) {
 int batch_rebuild(naga_batch* b) {
     b->free_tables();
     std::vector<SceneDev> sd;
-    std::vector<WorkItem> all, fluid, edge, pml;
+    std::vector<WorkItem> all, all_mt, fluid, edge, pml;
     b->k = b->members.empty() ? 0 : b->members[0]->desc.k;
+    b->kb = b->members.empty() ? 0 : b->members[0]->desc.k_boundary;
     for (size_t t = 0; t < b->members.size(); ++t) {
         naga_scene* s = b->members[t];
         if (s->desc.k != b->k) b->k = 0;
+        if (s->desc.k_boundary != b->kb) b->kb = 0;
+        for (auto it : s->items_all_mt) {
+            it.scene = (uint32_t)t;
+            all_mt.push_back(it);
+        }
         sd.push_back(s->dev);
         for (auto it : s->items_pml) {
             it.scene = (uint32_t)t;
@@ -429,6 +435,7 @@ int batch_rebuild(naga_batch* b) {
         }
     }
     b->n_all = (int)all.size();
+    b->n_all_mt = (int)all_mt.size();
     b->n_fluid = (int)fluid.size();
     b->n_edge = (int)edge.size();
     b->n_pml = (int)pml.size();
@@ -444,6 +451,7 @@ int batch_rebuild(naga_batch* b) {
     int rc;
     if ((rc = up(&b->d_scenes, sd))) return rc;
     if ((rc = up(&b->d_all, all))) return rc;
+    if ((rc = up(&b->d_all_mt, all_mt))) return rc;
     if ((rc = up(&b->d_fluid, fluid))) return rc;
     if ((rc = up(&b->d_edge, edge))) return rc;
     if ((rc = up(&b->d_pml, pml))) return rc;
@@ -457,6 +465,8 @@ StepLaunch launch_of(naga_batch* b) {
     P.nscenes = (int)b->members.size();
     P.all = b->d_all;
     P.n_all = b->n_all;
+    P.all_mt = b->d_all_mt;
+    P.n_all_mt = b->n_all_mt;
     P.fluid = b->d_fluid;
     P.n_fluid = b->n_fluid;
     P.edge = b->d_edge;
@@ -474,11 +484,11 @@ int batch_step(naga_batch* b, int nsteps) {
     StepLaunch P = launch_of(b);
     if (prof_on()) {
         for (int n = 0; n < nsteps; ++n)
-            if ((rc = enqueue_step(b->dim, b->k, P, b->stream))) return rc;
+            if ((rc = enqueue_step(b->dim, b->k, b->kb, P, b->stream))) return rc;
     } else {
         if (!b->exec) {
             NAGA_CUDA_TRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-            rc = enqueue_step(b->dim, b->k, P, b->stream);
+            rc = enqueue_step(b->dim, b->k, b->kb, P, b->stream);
             cudaGraph_t g = nullptr;
             cudaError_t e = cudaStreamEndCapture(b->stream, &g);
             if (rc) {
@@ -664,33 +674,32 @@ extern "C" int naga_scene_read_tables(naga_scene* s, uint32_t* idx, float* W, fl
     NAGA_CUDA_TRY(cudaStreamSynchronize(active_stream(s)));
     const int k = s->desc.k, D = s->dim;
     const int64_t N = s->N;
-    if (idx || W) {
-        std::vector<float> wv((size_t)k * N * (D == 3 ? 4 : 2));
-        std::vector<uint32_t> iv;
-        NAGA_CUDA_TRY(cudaMemcpy(wv.data(), s->dev.stW, sizeof(float) * wv.size(), cudaMemcpyDeviceToHost));
-        if (D == 2) {
-            iv.resize((size_t)k * N);
-            NAGA_CUDA_TRY(cudaMemcpy(iv.data(), s->dev.stI, sizeof(uint32_t) * iv.size(), cudaMemcpyDeviceToHost));
-        }
-        for (int64_t i = 0; i < N; ++i)
-            for (int t = 0; t < k; ++t) {
-                const size_t e = (size_t)t * N + i;
-                if (D == 3) {
-                    if (W)
-                        for (int d = 0; d < 3; ++d) W[(i * k + t) * 3 + d] = wv[e * 4 + d];
-                    if (idx) std::memcpy(&idx[i * k + t], &wv[e * 4 + 3], 4);
-                } else {
-                    if (W)
-                        for (int d = 0; d < 2; ++d) W[(i * k + t) * 2 + d] = wv[e * 2 + d];
-                    if (idx) idx[i * k + t] = iv[e];
-                }
+    if (idx || W || (fw && D == 2)) {
+        std::vector<float4> wv((size_t)k * N);
+        NAGA_CUDA_TRY(cudaMemcpy(wv.data(), s->dev.stW, sizeof(float4) * wv.size(), cudaMemcpyDeviceToHost));
+        for (size_t e = 0; e < wv.size(); ++e) {
+            if (W) {
+                W[e * D + 0] = wv[e].x;
+                W[e * D + 1] = wv[e].y;
+                if (D == 3) W[e * D + 2] = wv[e].z;
             }
+            if (idx) std::memcpy(&idx[e], &wv[e].w, 4);
+            if (fw && D == 2) fw[e] = wv[e].z;
+        }
     }
-    if (fw) {
+    if (fw && D == 3) {
         std::vector<float2> fv((size_t)k * N);
         NAGA_CUDA_TRY(cudaMemcpy(fv.data(), s->dev.stF, sizeof(float2) * fv.size(), cudaMemcpyDeviceToHost));
-        for (int64_t i = 0; i < N; ++i)
-            for (int t = 0; t < k; ++t) fw[i * k + t] = fv[(size_t)t * N + i].x;
+        for (size_t e = 0; e < fv.size(); ++e) fw[e] = fv[e].x;
+    }
+    if ((bidx || bw) && s->nbd > 0) {
+        const size_t n = (size_t)s->nbd * s->desc.k_boundary;
+        std::vector<float2> bv(n);
+        NAGA_CUDA_TRY(cudaMemcpy(bv.data(), s->dev.btab, sizeof(float2) * n, cudaMemcpyDeviceToHost));
+        for (size_t e = 0; e < n; ++e) {
+            if (bw) bw[e] = bv[e].x;
+            if (bidx) std::memcpy(&bidx[e], &bv[e].y, 4);
+        }
     }
     auto tr = [&](const void* dsrc_i, const float* dsrc_w, int64_t nq, int kk, uint32_t* oi, float* ow) -> int {
         if (nq == 0) return NAGA_OK;
@@ -706,7 +715,6 @@ extern "C" int naga_scene_read_tables(naga_scene* s, uint32_t* idx, float* W, fl
         return NAGA_OK;
     };
     int rc;
-    if ((bidx || bw) && (rc = tr(s->dev.bidx, s->dev.bw, s->nbd, s->desc.k_boundary, bidx, bw))) return rc;
     if ((pidx || pw) && (rc = tr(s->dev.pidx, s->dev.pw, s->dev.np, s->desc.k_probe, pidx, pw))) return rc;
     return NAGA_OK;
 }

@@ -392,7 +392,7 @@ __global__ void divergence_build_kernel(const float* __restrict__ pts, int64_t n
         // selective-filter weights: normalised Gaussian of the distance
         // (detail/simulation_engine.cuh:1233-1323), computed once
         double fw0 = 0, fw1 = 0;
-        if (out.Ff) {
+        if (out.Ff || (D == 2 && out.Wf)) {
             const double inv2s2 = 0.5 / (out.filter_sigma * out.filter_sigma);
             fw0 = lane < k ? exp(-r2own[0] * inv2s2) : 0.0;
             fw1 = lane + 32 < k ? exp(-r2own[1] * inv2s2) : 0.0;
@@ -408,15 +408,10 @@ __global__ void divergence_build_kernel(const float* __restrict__ pts, int64_t n
 #pragma unroll
                 for (int d = 0; d < D; ++d) out.W64[(i * k + t) * D + d] = Wt[d];
             if (out.Wf) {
-                if (D == 3) {
-                    float4 v = make_float4((float)Wt[0], (float)Wt[1], (float)Wt[D - 1], __uint_as_float(jl[r]));
-                    reinterpret_cast<float4*>(out.Wf)[t * out.ld + i] = v;
-                } else {
-                    reinterpret_cast<float2*>(out.Wf)[t * out.ld + i] = make_float2((float)Wt[0], (float)Wt[1]);
-                    out.If[t * out.ld + i] = jl[r];
-                }
+                const float fz = D == 3 ? (float)Wt[D - 1] : (float)(r == 0 ? fw0 : fw1);
+                out.Wf[i * k + t] = make_float4((float)Wt[0], (float)Wt[1], fz, __uint_as_float(jl[r]));
             }
-            if (out.Ff) out.Ff[t * out.ld + i] = make_float2((float)(r == 0 ? fw0 : fw1), __uint_as_float(jl[r]));
+            if (out.Ff) out.Ff[i * k + t] = make_float2((float)(r == 0 ? fw0 : fw1), __uint_as_float(jl[r]));
         }
         if (out.delta && lane == 0) out.delta[i] = delta;
         __syncwarp();

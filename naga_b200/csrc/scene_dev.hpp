@@ -3,14 +3,17 @@
 // HBM layout of a scene with N nodes (order: bulk [0, nb), layer
 // [nb, nb + nl), boundary [nbl, nbl + nbd), ghost [.., N)):
 //   populations   G, G1, G2, ACC, S1, S1P: node-major rows of QP floats
-//                 (QP = 28 for D3Q27, 12 for D2Q9), centred: g = f - w
+//                 (QP = 28 for D3Q27, 12 for D2Q9), centred: g = f - w,
+//                 populations in paired slot order (common.cuh)
 //   Q1a, Q1b      PML trapezoid integrals, rows of QP floats, ping-pong
 //                 by step parity
 //   M             float4 per node: (rho - 1, ux, uy, uz) in lattice units
-//   stencil       [k][N] records: D3Q27 float4 (Wx, Wy, Wz, index bits);
-//                 D2Q9 float2 (Wx, Wy) + uint32 index
-//   filter        [k][N] float2 (normalised Gaussian weight, index bits)
-//   boundary      [kb][nbd] indices + weights; probes [kp][np]
+//   stencil       node-major [N][k] float4 records: D3Q27 (Wx, Wy, Wz,
+//                 index bits); D2Q9 (Wx, Wy, filter weight, index bits)
+//   filter        D3Q27: node-major [N][k] float2 (weight, index bits)
+//   boundary      node-major [nbd][kb] float2 (weight, index bits);
+//                 probes [kp][np] indices + weights
+// Node-major records put a work item's stencil in one contiguous block.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -44,13 +47,11 @@ struct SceneDev {
     float* Q1b;
     float4* M;
     // tables
-    const void* stW;
-    const uint32_t* stI;
+    const float4* stW;
     const float2* stF;
     const float* sigma;
     const float* normals;
-    const uint32_t* bidx;
-    const float* bw;
+    const float2* btab;
     const uint32_t* pidx;
     const float* pw;
     const uint8_t* is_src;
@@ -76,10 +77,8 @@ namespace naga {
 struct StencilOut {
     double* W64;          // [n][k][D], FP64
     double* delta;        // [n]
-    float* Wf;            // scene layout: D == 3 float4 [k][ld] (Wx, Wy, Wz, idx); D == 2 float2 [k][ld]
-    uint32_t* If;         // D == 2: [k][ld]
-    float2* Ff;           // filter (w, idx bits) [k][ld]
-    int64_t ld;           // leading dimension of the scene layout
+    float4* Wf;           // scene records [n][k]: (Wx, Wy, Wz | filter weight, index bits)
+    float2* Ff;           // D == 3 filter records [n][k] (weight, index bits)
     double filter_sigma;  // Gaussian sigma of the selective filter (h / 2.5)
 };
 
@@ -87,18 +86,22 @@ struct StencilOut {
 struct StepLaunch {
     const SceneDev* scenes;
     int nscenes;
-    const WorkItem* all;
+    const WorkItem* all;  // 128-node items (thread-per-node kernels)
     int n_all;
+    const WorkItem* all_mt;  // pass-sized items of all nodes (multi-thread kernels)
+    int n_all_mt;
     const WorkItem* fluid;
     int n_fluid;
-    const WorkItem* edge;
+    const WorkItem* edge;  // pass-sized items of the boundary nodes
     int n_edge;
     const WorkItem* pml;  // bulk/layer items whose stencils reach the layer
     int n_pml;
 };
 
-// k: the batch's common stencil size (0 if the members differ)
-int enqueue_step(int dim, int k, const StepLaunch& P, cudaStream_t st);
+// k, kb: the batch's common stencil sizes (0 if the members differ)
+int enqueue_step(int dim, int k, int kb, const StepLaunch& P, cudaStream_t st);
+// nodes of one pass of the multi-thread-per-node kernels
+int nodes_per_pass(int dim);
 const char* kernel_name(int id);
 int kernel_count();
 void prof_begin(int id, cudaStream_t st);

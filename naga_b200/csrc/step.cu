@@ -137,25 +137,6 @@ __device__ __forceinline__ float feq_c(int a, float drho, const float* u) {
     return w * drho + w * (1.f + drho) * (uc / cs2 + (uc * uc) / (2.f * cs4) - uu);
 }
 
-// stencil record s of node i: weights and support index
-template <class L>
-__device__ __forceinline__ void stencil(const SceneDev& S, int s, int64_t i, float& wx, float& wy, float& wz,
-                                        uint32_t& j) {
-    if (L::D == 3) {
-        float4 r = __ldg(reinterpret_cast<const float4*>(S.stW) + (int64_t)s * S.N + i);
-        wx = r.x;
-        wy = r.y;
-        wz = r.z;
-        j = __float_as_uint(r.w);
-    } else {
-        float2 r = __ldg(reinterpret_cast<const float2*>(S.stW) + (int64_t)s * S.N + i);
-        wx = r.x;
-        wy = r.y;
-        wz = 0.f;
-        j = __ldg(S.stI + (int64_t)s * S.N + i);
-    }
-}
-
 // ------------------------------------------------------------- collision
 // D3Q27 central-moment collision (detail/d3q27_lattice.cuh:125-378) on
 // centred populations. Central moments K_mnp of f = w + g split into the
@@ -404,12 +385,21 @@ __device__ __forceinline__ void collide(const float* g, float drho, const float*
 }
 
 // ------------------------------------------------------------- kernels
-#define NAGA_FOR_ITEMS(items, nitems)                                       \
-    __shared__ SceneDev S;                                                  \
-    for (int w_ = blockIdx.x; w_ < (nitems); w_ += gridDim.x) {             \
-        const WorkItem it = (items)[w_];                                    \
-        __syncthreads();                                                    \
-        if (threadIdx.x == 0) S = scenes[it.scene];                         \
+// SceneDev of the current item into shared memory (warp 0 copies words)
+__device__ __forceinline__ void load_scene(SceneDev& dst, const SceneDev* src) {
+    if (threadIdx.x < 32) {
+        const int* a = reinterpret_cast<const int*>(src);
+        int* b = reinterpret_cast<int*>(&dst);
+        for (int t = threadIdx.x; t < (int)(sizeof(SceneDev) / 4); t += 32) b[t] = a[t];
+    }
+}
+
+#define NAGA_FOR_ITEMS(items, nitems)                           \
+    __shared__ SceneDev S;                                      \
+    for (int w_ = blockIdx.x; w_ < (nitems); w_ += gridDim.x) { \
+        const WorkItem it = (items)[w_];                        \
+        __syncthreads();                                        \
+        load_scene(S, scenes + it.scene);                       \
         __syncthreads();
 
 #define NAGA_END_ITEMS }
@@ -424,24 +414,37 @@ __device__ __forceinline__ void collide(const float* g, float drho, const float*
 //               boundary interpolation reads;
 //   boundary:   S1 = collision (the interpolated part is added later);
 //   ghost:      S1 = g + collision.
+// The item's rows of G and Q1_prev are staged in shared memory by coalesced
+// loads of the whole block before the (register-heavy) per-node work.
 template <class L>
 __global__ void __launch_bounds__(kBlock) k_macro_pml(const WorkItem* __restrict__ items, int nitems,
                                                       const SceneDev* __restrict__ scenes) {
     constexpr int Q = L::Q, QP = L::QP;
     __shared__ double red[kBlock / 32][2 * QP];
+    __shared__ float4 rowG[kBlock * QP / 4], rowQ[kBlock * QP / 4];
     NAGA_FOR_ITEMS(items, nitems)
-    const int64_t i = (int64_t)it.begin + threadIdx.x;
-    const bool active = i < (int64_t)it.end;
     const int par = (int)(*S.step & 1ull);
     float* Q1cur = par ? S.Q1b : S.Q1a;
     const float* Q1prev = par ? S.Q1a : S.Q1b;
+    const int nn = (int)(it.end - it.begin);
+    {
+        const float4* g4 = reinterpret_cast<const float4*>(S.G + (int64_t)it.begin * QP);
+        const float4* q4 = reinterpret_cast<const float4*>(Q1prev + (int64_t)it.begin * QP);
+        for (int e = threadIdx.x; e < nn * QP / 4; e += blockDim.x) {
+            rowG[e] = g4[e];
+            rowQ[e] = q4[e];
+        }
+    }
+    __syncthreads();
+    const int64_t i = (int64_t)it.begin + threadIdx.x;
+    const bool active = (int)threadIdx.x < nn;
     const bool layer = active && i >= S.nb && i < S.nb + S.nl;
     float s1[QP], s2[QP];
 #pragma unroll
     for (int t = 0; t < QP; ++t) s1[t] = s2[t] = 0.f;
     if (active) {
-        float row[QP], q1p[QP], q1[QP], out[QP];
-        load_row<L>(S.G, i, row);
+        const float* row = reinterpret_cast<const float*>(rowG) + threadIdx.x * QP;
+        const float* q1p = reinterpret_cast<const float*>(rowQ) + threadIdx.x * QP;
         float g[Q];
 #pragma unroll
         for (int a = 0; a < Q; ++a) g[a] = row[L::pos(a)];
@@ -450,10 +453,10 @@ __global__ void __launch_bounds__(kBlock) k_macro_pml(const WorkItem* __restrict
         const float4 mp = S.M[i];
         const float up[3] = {mp.y, mp.z, mp.w};
         S.M[i] = make_float4(drho, u[0], u[1], L::D == 3 ? u[2] : 0.f);
-        load_row<L>(Q1prev, i, q1p);
         const float sg = layer ? __ldg(S.sigma + (i - S.nb)) : 0.f;
         float dcol[Q];
         collide<L>(g, drho, u, S, dcol);
+        float q1[QP], out[QP];
 #pragma unroll
         for (int t = 0; t < QP; ++t) q1[t] = out[t] = 0.f;
         const bool src = i < S.nbl && S.is_src[i];
@@ -468,8 +471,7 @@ __global__ void __launch_bounds__(kBlock) k_macro_pml(const WorkItem* __restrict
                 s1[t] = q1[t];
                 s2[t] = q2;
             }
-            const float loc = layer ? g[a] - sg * (3.f * ft + 3.f * sg * q1[t] + sg * sg * q2) : g[a];
-            out[t] = loc;
+            out[t] = layer ? g[a] - sg * (3.f * ft + 3.f * sg * q1[t] + sg * sg * q2) : g[a];
         }
         store_row<L>(Q1cur, i, q1);
         if (src) store_row<L>(S.S1P, i, out);
@@ -542,18 +544,36 @@ __global__ void k_probe(const SceneDev* __restrict__ scenes) {
     }
 }
 
-// Multi-thread-per-node loop over the nodes of an item: thread c of node
-// slot `ns` handles chunk c of node i.
-#define NAGA_MT_NODES(G)                                                      \
-    const int c = threadIdx.x % G::TPN;                                      \
-    const int ns = threadIdx.x / G::TPN;                                     \
-    for (int64_t base = it.begin; base < (int64_t)it.end; base += G::NPB) {  \
-        const int64_t i = base + ns;                                         \
-        if (i < (int64_t)it.end && c < G::NCH) {
+// Multi-thread-per-node kernels: one work item = one pass of <= NPB
+// consecutive nodes; thread c of node slot ns owns float4 chunk c of node
+// i = begin + ns. The item's node-major stencil records are first copied to
+// shared memory by coalesced loads of the whole block, so the neighbour loop
+// only waits on the (mostly L2-resident) neighbour rows.
+template <class T>
+__device__ __forceinline__ void stage_tile(T* tile, const T* src, int count) {
+    for (int e = threadIdx.x; e < count; e += blockDim.x) tile[e] = __ldg(src + e);
+}
 
-#define NAGA_MT_END \
-    }               \
-    }
+// tile storage: fixed-size static shared memory for the unrolled stencil
+// sizes, dynamic shared memory (NPB x 64 records) for any other size
+template <class T, int N>
+__device__ __forceinline__ T* static_tile() {
+    __shared__ T t[N];
+    return t;
+}
+template <class T>
+__device__ __forceinline__ T* dynamic_tile() {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    return reinterpret_cast<T*>(dyn_smem);
+}
+template <class T, int NPB, int K>
+__device__ __forceinline__ T* tile_storage() {
+    if constexpr (K > 0)
+        return static_tile<T, NPB * K>();
+    else
+        return dynamic_tile<T>();
+}
+
 
 // PML divergence gathers of pml_absorption.inl:770-855 on bulk/layer nodes
 // whose stencil reaches into the layer: for support j in the layer the field
@@ -565,74 +585,84 @@ __global__ void __launch_bounds__(kBlockMT) k_pml_gather(const WorkItem* __restr
                                                          const SceneDev* __restrict__ scenes) {
     using G = MT<L>;
     constexpr int QP = L::QP;
+    float4* tile = tile_storage<float4, G::NPB, K>();
+    const int c = threadIdx.x % G::TPN, ns = threadIdx.x / G::TPN;
     float d0[3], d1[3];
-    pair_dirs<L>(threadIdx.x % G::TPN < G::NCH ? threadIdx.x % G::TPN : 0, d0, d1);
+    pair_dirs<L>(c < G::NCH ? c : 0, d0, d1);
     NAGA_FOR_ITEMS(items, nitems)
-    const int par = (int)(*S.step & 1ull);
-    const float* Q1cur = par ? S.Q1b : S.Q1a;
-    const float* Q1prev = par ? S.Q1a : S.Q1b;
     const int k = K > 0 ? K : S.k;
-    NAGA_MT_NODES(G)
-    const float4 m1 = *reinterpret_cast<const float4*>(S.means + 4 * c);
-    const float4 m2 = *reinterpret_cast<const float4*>(S.means + QP + 4 * c);
-    const float dt = S.dt_lat;
-    float4 dv = make_float4(0.f, 0.f, 0.f, 0.f);
+    const int nn = (int)(it.end - it.begin);
+    stage_tile(tile, S.stW + (int64_t)it.begin * k, nn * k);
+    __syncthreads();
+    const int64_t i = (int64_t)it.begin + ns;
+    if (ns < nn && c < G::NCH) {
+        const int par = (int)(*S.step & 1ull);
+        const float* Q1cur = par ? S.Q1b : S.Q1a;
+        const float* Q1prev = par ? S.Q1a : S.Q1b;
+        const float4 m1 = *reinterpret_cast<const float4*>(S.means + 4 * c);
+        const float4 m2 = *reinterpret_cast<const float4*>(S.means + QP + 4 * c);
+        const float dt = S.dt_lat;
+        float4 dv = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll 4
-    for (int s = 0; s < k; ++s) {
-        float wx, wy, wz;
-        uint32_t j;
-        stencil<L>(S, s, i, wx, wy, wz, j);
-        if ((int64_t)j < S.nb || (int64_t)j >= S.nb + S.nl) continue;
-        const float sg = __ldg(S.sigma + ((int64_t)j - S.nb));
-        const int64_t jq = (int64_t)j - S.pml_shift;
-        const float4 a = ld4(Q1cur, jq, QP, c), b = ld4(Q1prev, jq, QP, c);
-        const float p0 = d0[0] * wx + d0[1] * wy + d0[2] * wz;
-        const float p1 = d1[0] * wx + d1[1] * wy + d1[2] * wz;
-        const float sg2 = sg * sg, m2s = -2.f * sg;
-        const float f0 = m2s * (a.x - m1.x) + sg2 * ((a.x + b.x) * dt / 2.f - m2.x);
-        const float f1 = m2s * (a.y - m1.y) + sg2 * ((a.y + b.y) * dt / 2.f - m2.y);
-        const float f2 = m2s * (a.z - m1.z) + sg2 * ((a.z + b.z) * dt / 2.f - m2.z);
-        const float f3 = m2s * (a.w - m1.w) + sg2 * ((a.w + b.w) * dt / 2.f - m2.w);
-        dv.x = fmaf(p0, f0, dv.x);
-        dv.y = fmaf(-p0, f1, dv.y);
-        dv.z = fmaf(p1, f2, dv.z);
-        dv.w = fmaf(-p1, f3, dv.w);
+        for (int s = 0; s < k; ++s) {
+            const float4 rec = tile[ns * k + s];
+            const uint32_t j = __float_as_uint(rec.w);
+            if ((int64_t)j < S.nb || (int64_t)j >= S.nb + S.nl) continue;
+            const float wz = L::D == 3 ? rec.z : 0.f;
+            const float sg = __ldg(S.sigma + ((int64_t)j - S.nb));
+            const int64_t jq = (int64_t)j - S.pml_shift;
+            const float4 a = ld4(Q1cur, jq, QP, c), b = ld4(Q1prev, jq, QP, c);
+            const float p0 = d0[0] * rec.x + d0[1] * rec.y + d0[2] * wz;
+            const float p1 = d1[0] * rec.x + d1[1] * rec.y + d1[2] * wz;
+            const float sg2 = sg * sg, m2s = -2.f * sg;
+            const float f0 = m2s * (a.x - m1.x) + sg2 * ((a.x + b.x) * dt / 2.f - m2.x);
+            const float f1 = m2s * (a.y - m1.y) + sg2 * ((a.y + b.y) * dt / 2.f - m2.y);
+            const float f2 = m2s * (a.z - m1.z) + sg2 * ((a.z + b.z) * dt / 2.f - m2.z);
+            const float f3 = m2s * (a.w - m1.w) + sg2 * ((a.w + b.w) * dt / 2.f - m2.w);
+            dv.x = fmaf(p0, f0, dv.x);
+            dv.y = fmaf(-p0, f1, dv.y);
+            dv.z = fmaf(p1, f2, dv.z);
+            dv.w = fmaf(-p1, f3, dv.w);
+        }
+        const float4 o = ld4rw(S.S1, i, QP, c);
+        st4(S.S1, i, QP, c, make_float4(o.x + dv.x, o.y + dv.y, o.z + dv.z, o.w + dv.w));
+        if (S.is_src[i]) {
+            const float4 q = ld4rw(S.S1P, i, QP, c);
+            st4(S.S1P, i, QP, c, make_float4(q.x + dv.x, q.y + dv.y, q.z + dv.z, q.w + dv.w));
+        }
     }
-    float4 o = ld4rw(S.S1, i, QP, c);
-    st4(S.S1, i, QP, c, make_float4(o.x + dv.x, o.y + dv.y, o.z + dv.z, o.w + dv.w));
-    if (S.is_src[i]) {
-        float4 q = ld4rw(S.S1P, i, QP, c);
-        st4(S.S1P, i, QP, c, make_float4(q.x + dv.x, q.y + dv.y, q.z + dv.z, q.w + dv.w));
-    }
-    NAGA_MT_END
     NAGA_END_ITEMS
 }
 
 // boundary: s1 = interp(s1 of bulk + layer, before collision) + collision
 // (simulation_engine.cuh:434-467 then :469-531); S1 holds the collision
-template <class L>
+template <class L, int KB>
 __global__ void __launch_bounds__(kBlockMT) k_edge_collide(const WorkItem* __restrict__ items, int nitems,
                                                            const SceneDev* __restrict__ scenes) {
     using G = MT<L>;
     constexpr int QP = L::QP;
+    float2* tile = tile_storage<float2, G::NPB, KB>();
+    const int c = threadIdx.x % G::TPN, ns = threadIdx.x / G::TPN;
     NAGA_FOR_ITEMS(items, nitems)
-    NAGA_MT_NODES(G)
-    const int64_t b = i - S.nbl;
-    if (b < S.nbd) {
+    const int kb = KB > 0 ? KB : S.kb;
+    const int nn = (int)(it.end - it.begin);
+    stage_tile(tile, S.btab + ((int64_t)it.begin - S.nbl) * kb, nn * kb);
+    __syncthreads();
+    const int64_t i = (int64_t)it.begin + ns;
+    if (ns < nn && c < G::NCH) {
         float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-        for (int s = 0; s < S.kb; ++s) {
-            const uint32_t j = __ldg(S.bidx + (int64_t)s * S.nbd + b);
-            const float w = __ldg(S.bw + (int64_t)s * S.nbd + b);
-            const float4 v = ld4(S.S1P, j, QP, c);
-            acc.x = fmaf(w, v.x, acc.x);
-            acc.y = fmaf(w, v.y, acc.y);
-            acc.z = fmaf(w, v.z, acc.z);
-            acc.w = fmaf(w, v.w, acc.w);
+#pragma unroll 8
+        for (int s = 0; s < kb; ++s) {
+            const float2 r = tile[ns * kb + s];
+            const float4 v = ld4(S.S1P, __float_as_uint(r.y), QP, c);
+            acc.x = fmaf(r.x, v.x, acc.x);
+            acc.y = fmaf(r.x, v.y, acc.y);
+            acc.z = fmaf(r.x, v.z, acc.z);
+            acc.w = fmaf(r.x, v.w, acc.w);
         }
         const float4 d = ld4rw(S.S1, i, QP, c);
         st4(S.S1, i, QP, c, make_float4(acc.x + d.x, acc.y + d.y, acc.z + d.z, acc.w + d.w));
     }
-    NAGA_MT_END
     NAGA_END_ITEMS
 }
 
@@ -644,43 +674,58 @@ __global__ void __launch_bounds__(kBlockMT) k_filter(const WorkItem* __restrict_
                                                      const SceneDev* __restrict__ scenes) {
     using G = MT<L>;
     constexpr int QP = L::QP;
+    float2* tile = tile_storage<float2, G::NPB, K>();
+    const int c = threadIdx.x % G::TPN, ns = threadIdx.x / G::TPN;
     float d0[3], d1[3];
-    pair_dirs<L>(threadIdx.x % G::TPN < G::NCH ? threadIdx.x % G::TPN : 0, d0, d1);
+    pair_dirs<L>(c < G::NCH ? c : 0, d0, d1);
     NAGA_FOR_ITEMS(items, nitems)
     const int k = K > 0 ? K : S.k;
-    NAGA_MT_NODES(G)
-    const float4 f = ld4rw(S.S1, i, QP, c);
-    float4 out;
-    if (i < S.nbl) {
-        float4 sum = make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll 8
-        for (int s = 0; s < k; ++s) {
-            const float2 r = __ldg(S.stF + (int64_t)s * S.N + i);
-            const float4 v = ld4rw(S.S1, __float_as_uint(r.y), QP, c);
-            sum.x = fmaf(r.x, v.x - f.x, sum.x);
-            sum.y = fmaf(r.x, v.y - f.y, sum.y);
-            sum.z = fmaf(r.x, v.z - f.z, sum.z);
-            sum.w = fmaf(r.x, v.w - f.w, sum.w);
-        }
-        out = make_float4(fmaf(0.75f, sum.x, f.x), fmaf(0.75f, sum.y, f.y), fmaf(0.75f, sum.z, f.z),
-                          fmaf(0.75f, sum.w, f.w));
-    } else if (i - S.nbl < S.nbd) {
-        const int64_t b = i - S.nbl;
-        float n[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-        for (int d = 0; d < L::D; ++d) n[d] = __ldg(S.normals + b * L::D + d);
-        const float cn0 = d0[0] * n[0] + d0[1] * n[1] + d0[2] * n[2];
-        const float cn1 = d1[0] * n[0] + d1[1] * n[1] + d1[2] * n[2];
-        // element 2m carries direction d_m, element 2m+1 carries -d_m
-        out.x = cn0 > 0.f ? f.y : f.x;
-        out.y = -cn0 > 0.f ? f.x : f.y;
-        out.z = cn1 > 0.f ? f.w : f.z;
-        out.w = -cn1 > 0.f ? f.z : f.w;
+    const int nn = (int)(it.end - it.begin);
+    // filter records of the item's bulk/layer nodes: (weight, index bits)
+    const int nf = (int)max((int64_t)0, min((int64_t)it.end, S.nbl) - (int64_t)it.begin);
+    if (L::D == 3) {
+        stage_tile(tile, S.stF + (int64_t)it.begin * k, nf * k);
     } else {
-        out = f;
+        for (int e = threadIdx.x; e < nf * k; e += blockDim.x) {
+            const float4 r = __ldg(S.stW + (int64_t)it.begin * k + e);
+            tile[e] = make_float2(r.z, r.w);
+        }
     }
-    st4(S.G, i, QP, c, out);
-    NAGA_MT_END
+    __syncthreads();
+    const int64_t i = (int64_t)it.begin + ns;
+    if (ns < nn && c < G::NCH) {
+        const float4 f = ld4rw(S.S1, i, QP, c);
+        float4 out;
+        if (i < S.nbl) {
+            float4 sum = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll 8
+            for (int s = 0; s < k; ++s) {
+                const float2 r = tile[ns * k + s];
+                const float4 v = ld4rw(S.S1, __float_as_uint(r.y), QP, c);
+                sum.x = fmaf(r.x, v.x - f.x, sum.x);
+                sum.y = fmaf(r.x, v.y - f.y, sum.y);
+                sum.z = fmaf(r.x, v.z - f.z, sum.z);
+                sum.w = fmaf(r.x, v.w - f.w, sum.w);
+            }
+            out = make_float4(fmaf(0.75f, sum.x, f.x), fmaf(0.75f, sum.y, f.y), fmaf(0.75f, sum.z, f.z),
+                              fmaf(0.75f, sum.w, f.w));
+        } else if (i - S.nbl < S.nbd) {
+            const int64_t b = i - S.nbl;
+            float n[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+            for (int d = 0; d < L::D; ++d) n[d] = __ldg(S.normals + b * L::D + d);
+            const float cn0 = d0[0] * n[0] + d0[1] * n[1] + d0[2] * n[2];
+            const float cn1 = d1[0] * n[0] + d1[1] * n[1] + d1[2] * n[2];
+            // element 2m carries direction d_m, element 2m+1 carries -d_m
+            out.x = cn0 > 0.f ? f.y : f.x;
+            out.y = -cn0 > 0.f ? f.x : f.y;
+            out.z = cn1 > 0.f ? f.w : f.z;
+            out.w = -cn1 > 0.f ? f.z : f.w;
+        } else {
+            out = f;
+        }
+        st4(S.G, i, QP, c, out);
+    }
     NAGA_END_ITEMS
 }
 
@@ -693,35 +738,40 @@ __global__ void __launch_bounds__(kBlockMT) k_rk(const WorkItem* __restrict__ it
                                                  const SceneDev* __restrict__ scenes) {
     using G = MT<L>;
     constexpr int QP = L::QP;
+    float4* tile = tile_storage<float4, G::NPB, K>();
+    const int c = threadIdx.x % G::TPN, ns = threadIdx.x / G::TPN;
     float d0[3], d1[3];
-    pair_dirs<L>(threadIdx.x % G::TPN < G::NCH ? threadIdx.x % G::TPN : 0, d0, d1);
+    pair_dirs<L>(c < G::NCH ? c : 0, d0, d1);
     NAGA_FOR_ITEMS(items, nitems)
     const int k = K > 0 ? K : S.k;
-    const float* src = (STAGE == 1) ? S.G : (STAGE == 2) ? S.G1 : (STAGE == 3) ? S.G2 : S.G1;
-    NAGA_MT_NODES(G)
-    float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
+    const int nn = (int)(it.end - it.begin);
+    stage_tile(tile, S.stW + (int64_t)it.begin * k, nn * k);
+    __syncthreads();
+    const int64_t i = (int64_t)it.begin + ns;
+    if (ns < nn && c < G::NCH) {
+        const float* src = (STAGE == 1) ? S.G : (STAGE == 2) ? S.G1 : (STAGE == 3) ? S.G2 : S.G1;
+        const float4 f0 = ld4(S.G, i, QP, c);
+        const float4 acc = STAGE == 1 ? make_float4(0.f, 0.f, 0.f, 0.f) : ld4rw(S.ACC, i, QP, c);
+        float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll 8
-    for (int s = 0; s < k; ++s) {
-        float wx, wy, wz;
-        uint32_t j;
-        stencil<L>(S, s, i, wx, wy, wz, j);
-        const float4 v = ld4((int64_t)j < S.nbl ? src : S.G, j, QP, c);
-        const float p0 = d0[0] * wx + d0[1] * wy + d0[2] * wz;
-        const float p1 = d1[0] * wx + d1[1] * wy + d1[2] * wz;
-        r.x = fmaf(p0, v.x, r.x);
-        r.y = fmaf(-p0, v.y, r.y);
-        r.z = fmaf(p1, v.z, r.z);
-        r.w = fmaf(-p1, v.w, r.w);
-    }
-    const float4 kv = make_float4(-r.x, -r.y, -r.z, -r.w);
-    const float4 f0 = ld4(S.G, i, QP, c);
-    if (STAGE == 1) {
-        st4(S.G1, i, QP, c, make_float4(fmaf(S.a_half, kv.x, f0.x), fmaf(S.a_half, kv.y, f0.y),
-                                        fmaf(S.a_half, kv.z, f0.z), fmaf(S.a_half, kv.w, f0.w)));
-        st4(S.ACC, i, QP, c, make_float4(kv.x * S.b1, kv.y * S.b1, kv.z * S.b1, kv.w * S.b1));
-    } else {
-        const float4 acc = ld4rw(S.ACC, i, QP, c);
-        if (STAGE == 4) {
+        for (int s = 0; s < k; ++s) {
+            const float4 rec = tile[ns * k + s];
+            const uint32_t j = __float_as_uint(rec.w);
+            const float wz = L::D == 3 ? rec.z : 0.f;
+            const float4 v = ld4((int64_t)j < S.nbl ? src : S.G, j, QP, c);
+            const float p0 = d0[0] * rec.x + d0[1] * rec.y + d0[2] * wz;
+            const float p1 = d1[0] * rec.x + d1[1] * rec.y + d1[2] * wz;
+            r.x = fmaf(p0, v.x, r.x);
+            r.y = fmaf(-p0, v.y, r.y);
+            r.z = fmaf(p1, v.z, r.z);
+            r.w = fmaf(-p1, v.w, r.w);
+        }
+        const float4 kv = make_float4(-r.x, -r.y, -r.z, -r.w);
+        if (STAGE == 1) {
+            st4(S.G1, i, QP, c, make_float4(fmaf(S.a_half, kv.x, f0.x), fmaf(S.a_half, kv.y, f0.y),
+                                            fmaf(S.a_half, kv.z, f0.z), fmaf(S.a_half, kv.w, f0.w)));
+            st4(S.ACC, i, QP, c, make_float4(kv.x * S.b1, kv.y * S.b1, kv.z * S.b1, kv.w * S.b1));
+        } else if (STAGE == 4) {
             const float4 df = make_float4(acc.x + kv.x * S.b1, acc.y + kv.y * S.b1, acc.z + kv.z * S.b1,
                                           acc.w + kv.w * S.b1);
             st4(S.G, i, QP, c, make_float4(fmaf(S.a_full, df.x, f0.x), fmaf(S.a_full, df.y, f0.y),
@@ -734,33 +784,36 @@ __global__ void __launch_bounds__(kBlockMT) k_rk(const WorkItem* __restrict__ it
                                              acc.w + kv.w * S.b2));
         }
     }
-    NAGA_MT_END
     NAGA_END_ITEMS
 }
 
 // boundary: f = interp(f of bulk + layer) (simulation_engine.cuh:1370)
-template <class L>
+template <class L, int KB>
 __global__ void __launch_bounds__(kBlockMT) k_edge_interp(const WorkItem* __restrict__ items, int nitems,
                                                           const SceneDev* __restrict__ scenes) {
     using G = MT<L>;
     constexpr int QP = L::QP;
+    float2* tile = tile_storage<float2, G::NPB, KB>();
+    const int c = threadIdx.x % G::TPN, ns = threadIdx.x / G::TPN;
     NAGA_FOR_ITEMS(items, nitems)
-    NAGA_MT_NODES(G)
-    const int64_t b = i - S.nbl;
-    if (b < S.nbd) {
+    const int kb = KB > 0 ? KB : S.kb;
+    const int nn = (int)(it.end - it.begin);
+    stage_tile(tile, S.btab + ((int64_t)it.begin - S.nbl) * kb, nn * kb);
+    __syncthreads();
+    const int64_t i = (int64_t)it.begin + ns;
+    if (ns < nn && c < G::NCH) {
         float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-        for (int s = 0; s < S.kb; ++s) {
-            const uint32_t j = __ldg(S.bidx + (int64_t)s * S.nbd + b);
-            const float w = __ldg(S.bw + (int64_t)s * S.nbd + b);
-            const float4 v = ld4rw(S.G, j, QP, c);
-            acc.x = fmaf(w, v.x, acc.x);
-            acc.y = fmaf(w, v.y, acc.y);
-            acc.z = fmaf(w, v.z, acc.z);
-            acc.w = fmaf(w, v.w, acc.w);
+#pragma unroll 8
+        for (int s = 0; s < kb; ++s) {
+            const float2 r = tile[ns * kb + s];
+            const float4 v = ld4rw(S.G, __float_as_uint(r.y), QP, c);
+            acc.x = fmaf(r.x, v.x, acc.x);
+            acc.y = fmaf(r.x, v.y, acc.y);
+            acc.z = fmaf(r.x, v.z, acc.z);
+            acc.w = fmaf(r.x, v.w, acc.w);
         }
         st4(S.G, i, QP, c, acc);
     }
-    NAGA_MT_END
     NAGA_END_ITEMS
 }
 
@@ -795,10 +848,29 @@ const char* kernel_name(int id) {
     return (id >= 0 && id < K_COUNT) ? names[id] : "?";
 }
 int kernel_count() { return K_COUNT; }
+int nodes_per_pass(int dim) { return dim == 2 ? MT<D2Q9>::NPB : MT<D3Q27>::NPB; }
 
-template <class L, int K>
+// dynamic shared memory of the generic (K == 0) variants: NPB x 64 records
+template <class L, int K, class T>
+size_t tile_bytes() {
+    return K > 0 ? 0 : (size_t)MT<L>::NPB * 64 * sizeof(T);
+}
+template <class Kern>
+int allow_smem(Kern kern, size_t bytes) {
+    if (bytes > 48 * 1024) NAGA_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    return NAGA_OK;
+}
+
+template <class L, int K, int KB>
 int enqueue_step_k(const StepLaunch& P, cudaStream_t st) {
     const int cap = sm_count() * 8;
+    const size_t s4 = tile_bytes<L, K, float4>(), s2 = tile_bytes<L, K, float2>(), sb = tile_bytes<L, KB, float2>();
+    int rc;
+    if ((rc = allow_smem(k_pml_gather<L, K>, s4)) || (rc = allow_smem(k_rk<L, K, 1>, s4)) ||
+        (rc = allow_smem(k_rk<L, K, 2>, s4)) || (rc = allow_smem(k_rk<L, K, 3>, s4)) ||
+        (rc = allow_smem(k_rk<L, K, 4>, s4)) || (rc = allow_smem(k_filter<L, K>, s2)) ||
+        (rc = allow_smem(k_edge_collide<L, KB>, sb)) || (rc = allow_smem(k_edge_interp<L, KB>, sb)))
+        return rc;
     auto grid = [&](int n) { return n < cap ? n : cap; };
     const bool prof = prof_on();
 #define LAUNCH(id, n, ...)                      \
@@ -810,33 +882,34 @@ int enqueue_step_k(const StepLaunch& P, cudaStream_t st) {
     LAUNCH(K_MACRO, P.n_all, (k_macro_pml<L><<<grid(P.n_all), kBlock, 0, st>>>(P.all, P.n_all, P.scenes)));
     LAUNCH(K_MEANS, P.nscenes, (k_pml_means<L::QP><<<dim3(P.nscenes, 2 * L::QP), 256, 0, st>>>(P.scenes)));
     LAUNCH(K_PROBE, P.nscenes, (k_probe<<<P.nscenes, 128, 0, st>>>(P.scenes)));
-    LAUNCH(K_PML, P.n_pml, (k_pml_gather<L, K><<<grid(P.n_pml), kBlockMT, 0, st>>>(P.pml, P.n_pml, P.scenes)));
+    LAUNCH(K_PML, P.n_pml, (k_pml_gather<L, K><<<grid(P.n_pml), kBlockMT, s4, st>>>(P.pml, P.n_pml, P.scenes)));
     LAUNCH(K_EDGE_COLLIDE, P.n_edge,
-           (k_edge_collide<L><<<grid(P.n_edge), kBlockMT, 0, st>>>(P.edge, P.n_edge, P.scenes)));
-    LAUNCH(K_FILTER, P.n_all, (k_filter<L, K><<<grid(P.n_all), kBlockMT, 0, st>>>(P.all, P.n_all, P.scenes)));
-    LAUNCH(K_RK1, P.n_fluid, (k_rk<L, K, 1><<<grid(P.n_fluid), kBlockMT, 0, st>>>(P.fluid, P.n_fluid, P.scenes)));
-    LAUNCH(K_RK2, P.n_fluid, (k_rk<L, K, 2><<<grid(P.n_fluid), kBlockMT, 0, st>>>(P.fluid, P.n_fluid, P.scenes)));
-    LAUNCH(K_RK3, P.n_fluid, (k_rk<L, K, 3><<<grid(P.n_fluid), kBlockMT, 0, st>>>(P.fluid, P.n_fluid, P.scenes)));
-    LAUNCH(K_RK4, P.n_fluid, (k_rk<L, K, 4><<<grid(P.n_fluid), kBlockMT, 0, st>>>(P.fluid, P.n_fluid, P.scenes)));
+           (k_edge_collide<L, KB><<<grid(P.n_edge), kBlockMT, sb, st>>>(P.edge, P.n_edge, P.scenes)));
+    LAUNCH(K_FILTER, P.n_all_mt,
+           (k_filter<L, K><<<grid(P.n_all_mt), kBlockMT, s2, st>>>(P.all_mt, P.n_all_mt, P.scenes)));
+    LAUNCH(K_RK1, P.n_fluid, (k_rk<L, K, 1><<<grid(P.n_fluid), kBlockMT, s4, st>>>(P.fluid, P.n_fluid, P.scenes)));
+    LAUNCH(K_RK2, P.n_fluid, (k_rk<L, K, 2><<<grid(P.n_fluid), kBlockMT, s4, st>>>(P.fluid, P.n_fluid, P.scenes)));
+    LAUNCH(K_RK3, P.n_fluid, (k_rk<L, K, 3><<<grid(P.n_fluid), kBlockMT, s4, st>>>(P.fluid, P.n_fluid, P.scenes)));
+    LAUNCH(K_RK4, P.n_fluid, (k_rk<L, K, 4><<<grid(P.n_fluid), kBlockMT, s4, st>>>(P.fluid, P.n_fluid, P.scenes)));
     LAUNCH(K_EDGE_INTERP, P.n_edge,
-           (k_edge_interp<L><<<grid(P.n_edge), kBlockMT, 0, st>>>(P.edge, P.n_edge, P.scenes)));
+           (k_edge_interp<L, KB><<<grid(P.n_edge), kBlockMT, sb, st>>>(P.edge, P.n_edge, P.scenes)));
     LAUNCH(K_STEP_END, P.nscenes, (k_step_end<<<(P.nscenes + 127) / 128, 128, 0, st>>>(P.scenes, P.nscenes)));
 #undef LAUNCH
     NAGA_CUDA_TRY(cudaGetLastError());
     return NAGA_OK;
 }
 
-// k is uniform over a batch (scenes of one batch share k); the common
-// stencil sizes get a fully unrolled gather
-int enqueue_step(int dim, int k, const StepLaunch& P, cudaStream_t st) {
+// k, kb: the batch's common stencil sizes (0 if the members differ); the
+// common sizes get fully unrolled gathers with fixed-size tiles
+int enqueue_step(int dim, int k, int kb, const StepLaunch& P, cudaStream_t st) {
     if (dim == 2) {
-        if (k == 16) return enqueue_step_k<D2Q9, 16>(P, st);
-        if (k == 32) return enqueue_step_k<D2Q9, 32>(P, st);
-        return enqueue_step_k<D2Q9, 0>(P, st);
+        if (k == 16 && kb == 16) return enqueue_step_k<D2Q9, 16, 16>(P, st);
+        if (k == 32 && kb == 32) return enqueue_step_k<D2Q9, 32, 32>(P, st);
+        return enqueue_step_k<D2Q9, 0, 0>(P, st);
     }
-    if (k == 32) return enqueue_step_k<D3Q27, 32>(P, st);
-    if (k == 16) return enqueue_step_k<D3Q27, 16>(P, st);
-    return enqueue_step_k<D3Q27, 0>(P, st);
+    if (k == 32 && kb == 32) return enqueue_step_k<D3Q27, 32, 32>(P, st);
+    if (k == 16 && kb == 16) return enqueue_step_k<D3Q27, 16, 16>(P, st);
+    return enqueue_step_k<D3Q27, 0, 0>(P, st);
 }
 
 }  // namespace naga

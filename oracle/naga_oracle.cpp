@@ -176,6 +176,133 @@ static void knn_grid(const float* src, int64_t n, const float* q, int64_t nq, in
     }
 }
 
+// Restatement of NAGA's own search, used only to show that it returns the
+// same neighbour SETS as the exact search on the benchmark clouds.
+// Cells: nd_cubic_segmentation.cuh:227-303 (FP32 bounds, +1e-3 on a
+// degenerate axis, width = (approx / N * volume)^(1/D), shape = ceil(extent /
+// width)) and get_partition_index :376-392. Search:
+// nearest_neighbors.cuh:207-411 -- Chebyshev rings r = 0, 1, ...; the first k
+// candidates are appended and then sorted (insertion_sort :59-93), later ones
+// replace the last entry only when strictly closer; the search continues
+// while the previous ring added a first-k candidate or fewer than k are
+// known, and stops at radius max((shape + 1) / 2). The reference visits the
+// cells of a ring in a pseudo-random order and a cell's points in the order
+// its atomic scatter left them; here both are in index order, which can
+// change the result only where candidates tie at the k-th distance. The
+// cell index is clamped to the grid (the reference's floor can reach `shape`
+// through rounding).
+static void knn_ring_reference(const float* src, int64_t n, const float* q, int64_t nq, int dim,
+                               int k, int approx, uint32_t* idx, float* d2) {
+    float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    for (int d = 0; d < dim; ++d) {
+        lo[d] = INFINITY;
+        hi[d] = -INFINITY;
+    }
+    for (int64_t j = 0; j < n; ++j)
+        for (int d = 0; d < dim; ++d) {
+            lo[d] = std::min(lo[d], src[j * dim + d]);
+            hi[d] = std::max(hi[d], src[j * dim + d]);
+        }
+    const float tol = 1e-3f;
+    float vol = 1.0f;
+    for (int d = 0; d < dim; ++d) {
+        if (hi[d] - lo[d] < tol) hi[d] = lo[d] + tol;
+        vol *= hi[d] - lo[d];
+    }
+    const float w = std::pow((float)approx / (float)n * vol, 1.0f / (float)dim);
+    int64_t shape[3] = {1, 1, 1};
+    for (int d = 0; d < dim; ++d) {
+        shape[d] = (int64_t)std::ceil((hi[d] - lo[d]) / w);
+        hi[d] = lo[d] + (float)shape[d] * w;
+    }
+    auto cell_of = [&](const float* p, int64_t* c) {
+        for (int d = 0; d < dim; ++d) {
+            if (p[d] < lo[d]) c[d] = 0;
+            else if (p[d] >= hi[d]) c[d] = shape[d] - 1;
+            else c[d] = std::min<int64_t>((int64_t)std::floor((p[d] - lo[d]) / w), shape[d] - 1);
+        }
+    };
+    const int64_t ncell = shape[0] * shape[1] * shape[2];
+    std::vector<int64_t> start(ncell + 1, 0), cell(n);
+    for (int64_t j = 0; j < n; ++j) {
+        int64_t c[3] = {0, 0, 0};
+        cell_of(src + j * dim, c);
+        cell[j] = c[0] + shape[0] * (c[1] + shape[1] * c[2]);
+        start[cell[j] + 1]++;
+    }
+    for (int64_t c = 0; c < ncell; ++c) start[c + 1] += start[c];
+    std::vector<uint32_t> order(n);
+    {
+        std::vector<int64_t> fill(start.begin(), start.end() - 1);
+        for (int64_t j = 0; j < n; ++j) order[fill[cell[j]]++] = (uint32_t)j;
+    }
+    int64_t max_r = 0;
+    for (int d = 0; d < dim; ++d) max_r = std::max<int64_t>(max_r, (shape[d] + 1) / 2);
+#pragma omp parallel
+    {
+        std::vector<float> bd(k);
+        std::vector<uint32_t> bi(k);
+#pragma omp for schedule(dynamic, 64)
+        for (int64_t i = 0; i < nq; ++i) {
+            const float* p = q + i * dim;
+            int64_t c0[3] = {0, 0, 0};
+            cell_of(p, c0);
+            int nf = 0;
+            bool fresh = true;
+            for (int64_t r = 0; (fresh || nf < k) && r <= max_r; ++r) {
+                fresh = false;
+                int64_t a[3], b[3];
+                for (int d = 0; d < 3; ++d) {
+                    a[d] = d < dim ? c0[d] - r : 0;
+                    b[d] = d < dim ? c0[d] + r : 0;
+                }
+                for (int64_t z = std::max<int64_t>(a[2], 0); z <= std::min(b[2], shape[2] - 1); ++z)
+                    for (int64_t y = std::max<int64_t>(a[1], 0); y <= std::min(b[1], shape[1] - 1); ++y)
+                        for (int64_t x = std::max<int64_t>(a[0], 0); x <= std::min(b[0], shape[0] - 1); ++x) {
+                            bool shell = x == a[0] || x == b[0] || (dim > 1 && (y == a[1] || y == b[1])) ||
+                                         (dim > 2 && (z == a[2] || z == b[2]));
+                            if (!shell) continue;
+                            int64_t cid = x + shape[0] * (y + shape[1] * z);
+                            for (int64_t t = start[cid]; t < start[cid + 1]; ++t) {
+                                const uint32_t j = order[t];
+                                const float dd = dist2f(p, src + (int64_t)j * dim, dim);
+                                if (nf < k) {
+                                    bd[nf] = dd;
+                                    bi[nf] = j;
+                                    if (++nf == k) {
+                                        for (int u = 1; u < k; ++u) {  // stable insertion sort
+                                            float kd = bd[u];
+                                            uint32_t ki = bi[u];
+                                            int v = u - 1;
+                                            for (; v >= 0 && bd[v] > kd; --v) {
+                                                bd[v + 1] = bd[v];
+                                                bi[v + 1] = bi[v];
+                                            }
+                                            bd[v + 1] = kd;
+                                            bi[v + 1] = ki;
+                                        }
+                                    }
+                                    fresh = true;
+                                } else if (dd < bd[k - 1]) {
+                                    int v = k - 1;
+                                    for (; v > 0 && bd[v - 1] > dd; --v) {
+                                        bd[v] = bd[v - 1];
+                                        bi[v] = bi[v - 1];
+                                    }
+                                    bd[v] = dd;
+                                    bi[v] = j;
+                                }
+                            }
+                        }
+            }
+            for (int s = 0; s < k; ++s) {
+                idx[i * k + s] = s < nf ? bi[s] : 0xffffffffu;
+                d2[i * k + s] = s < nf ? bd[s] : INFINITY;
+            }
+        }
+    }
+}
+
 // ================================================================== LU
 // LU with partial pivoting (first row of maximal |a| in the column), as
 // LAPACK getrf; cuBLAS {S,D}getrfBatched is called with these semantics at
@@ -287,6 +414,13 @@ extern "C" int orc_knn(const float* src, int64_t n, const float* qry, int64_t nq
         knn_grid(src, n, qry, nq, dim, k, idx, d2);
     else
         knn_brute(src, n, qry, nq, dim, k, idx, d2);
+    return 0;
+}
+
+extern "C" int orc_knn_ring_reference(const float* src, int64_t n, const float* qry, int64_t nq,
+                                      int dim, int k, int approx, uint32_t* idx, float* d2) {
+    if (dim < 1 || dim > 3 || k < 1 || n < 1 || nq < 0 || approx < 1) return 1;
+    knn_ring_reference(src, n, qry, nq, dim, k, approx, idx, d2);
     return 0;
 }
 

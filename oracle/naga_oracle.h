@@ -28,6 +28,14 @@ extern "C" {
 int orc_knn(const float* src, int64_t n, const float* qry, int64_t nq, int dim,
             int k, int grid, uint32_t* idx, float* d2);
 
+/* ---- NAGA's own ring search (cells of ~approx points, stops one ring
+ * after the k-th candidate), restated to compare neighbour SETS with the
+ * exact search: nd_cubic_segmentation.cuh:227-303, nearest_neighbors.cuh:
+ * 207-411. Cells are visited in index order, not NAGA's random order.    */
+int orc_knn_ring_reference(const float* src, int64_t n, const float* qry,
+                           int64_t nq, int dim, int k, int approx,
+                           uint32_t* idx, float* d2);
+
 /* ---- batched LU inverse (getrf + getri semantics), FP64 -------------- */
 /* A, Ainv: [batch][n][n] column-major per matrix; info[batch] (0 = ok,
  * j>0 = U(j,j) exactly zero, LAPACK convention).                          */

@@ -49,6 +49,7 @@ def lib(path: str | None = None):
     L = C.CDLL(p)
     vp, i64, i32, dbl = C.c_void_p, C.c_int64, C.c_int, C.c_double
     L.orc_knn.argtypes = [vp, i64, vp, i64, i32, i32, i32, vp, vp]
+    L.orc_knn_ring_reference.argtypes = [vp, i64, vp, i64, i32, i32, i32, vp, vp]
     L.orc_batched_inverse_f64.argtypes = [vp, i32, i64, vp, vp]
     L.orc_rbf_weights.argtypes = [vp, i64, i32, vp, i32, vp, i64, i32, dbl, i32, vp]
     L.orc_divergence_stencil.argtypes = [vp, i64, i32, i32, i32, vp, vp, vp]
@@ -80,6 +81,18 @@ def knn(src, qry, k, grid=True):
     idx = np.zeros((qry.shape[0], k), np.uint32)
     d2 = np.zeros((qry.shape[0], k), np.float32)
     rc = lib().orc_knn(_p(src), src.shape[0], _p(qry), qry.shape[0], dim, k, int(grid), _p(idx), _p(d2))
+    assert rc == 0, rc
+    return idx, d2
+
+
+def knn_ring_reference(src, qry, k, approx=None):
+    """NAGA's ring search restated (cells of ~approx points, default k)."""
+    src = np.ascontiguousarray(src, np.float32)
+    qry = np.ascontiguousarray(qry, np.float32)
+    idx = np.zeros((qry.shape[0], k), np.uint32)
+    d2 = np.zeros((qry.shape[0], k), np.float32)
+    rc = lib().orc_knn_ring_reference(_p(src), src.shape[0], _p(qry), qry.shape[0], src.shape[1], k,
+                                      int(approx or k), _p(idx), _p(d2))
     assert rc == 0, rc
     return idx, d2
 
