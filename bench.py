@@ -83,8 +83,11 @@ def kernel_bytes(dim, N, nb, nl, nbd, k, kb):
     st = 4 * k * (dim + 1)  # weights + index per neighbour
     nbl = nb + nl
     return {
-        "macro_pml": N * (4 * row + 32),
-        "pml_gather": nbl * (st + 2 * row) + nl * 2 * row,
+        # G, Q1_prev in; Q1, S1 out (+ S1P on sources, not counted); M in/out;
+        # the PML field rows of the layer out
+        "macro_pml": N * (4 * row + 32) + nl * row,
+        # stencil + S1 read/write + PV per node, the layer's field rows once
+        "pml_gather": nbl * (st + 2 * row + 32) + nl * row,
         "edge_collide": nbd * (2 * row + 8 * kb),
         "filter": N * 2 * row + nbl * 8 * k,
         "rk_stage1": nbl * (st + 3 * row),

@@ -254,8 +254,12 @@ int scene_setup(naga_scene* s) {
 
     // divergence stencil + filter weights over the domain [0, nd)
     const int k = d.k;
+    const int npb = nodes_per_pass(D);
     StencilOut out{};
     out.filter_sigma = d.nodal_spacing / 2.5;
+    out.split = s->nbl;
+    out.n_total = N;
+    out.npb = npb;
     uint32_t* knn_idx = nullptr;
     if ((rc = s->alloc(&knn_idx, s->nd * k))) return rc;
     float4* W = nullptr;
@@ -273,6 +277,18 @@ int scene_setup(naga_scene* s) {
     }
     rc = divergence_build_device(pts, s->nd, D, k, d.shape, d.weight_precision, knn_idx, out, st);
     if (rc) return rc;
+    // PML: field rows of the layer nodes and the per-node mean vectors
+    float* phi = nullptr;
+    float4* pv = nullptr;
+    if (s->nl > 0) {
+        if ((rc = s->alloc(&phi, s->nl * QP))) return rc;
+        NAGA_CUDA_TRY(cudaMemsetAsync(phi, 0, sizeof(float) * s->nl * QP, st));
+    }
+    if ((rc = s->alloc(&pv, 2 * std::max<int64_t>(s->nbl, 1)))) return rc;
+    NAGA_CUDA_TRY(cudaMemsetAsync(pv, 0, sizeof(float4) * 2 * std::max<int64_t>(s->nbl, 1), st));
+    if (s->nl > 0 && (rc = pml_vectors_device(D, W, V.sigma, s->nb, s->nl, s->nbl, N, k, pv, st))) return rc;
+    V.PHI = phi;
+    V.PV = pv;
 
     // boundary interpolation: kNN among bulk + layer, RPIM at the boundary
     // node with the nodal spacing (detail/simulation_engine.cuh:223-258)
@@ -325,15 +341,16 @@ int scene_setup(naga_scene* s) {
             NAGA_CUDA_TRY(cudaMemcpyAsync(*w_out, tw.data(), sizeof(float) * nq * kk, cudaMemcpyHostToDevice, st));
             NAGA_CUDA_TRY(cudaStreamSynchronize(st));
         } else {
-            // boundary: node-major (weight, index bits) records
+            // boundary: (weight, index bits) records in pass order
             std::vector<float2> rec(nq * kk);
-            for (int64_t q = 0; q < nq * kk; ++q) {
-                float2 v;
-                v.x = (float)hw[q];
-                std::memcpy(&v.y, &hi[q], 4);
-                rec[q] = v;
-                is_src[hi[q]] = 1;
-            }
+            for (int64_t q = 0; q < nq; ++q)
+                for (int t = 0; t < kk; ++t) {
+                    float2 v;
+                    v.x = (float)hw[q * kk + t];
+                    std::memcpy(&v.y, &hi[q * kk + t], 4);
+                    rec[pass_record(q, t, kk, nq, nq, npb)] = v;
+                    is_src[hi[q * kk + t]] = 1;
+                }
             if ((r = s->alloc(rec_out, nq * kk))) return r;
             NAGA_CUDA_TRY(cudaMemcpyAsync(*rec_out, rec.data(), sizeof(float2) * nq * kk, cudaMemcpyHostToDevice, st));
             NAGA_CUDA_TRY(cudaStreamSynchronize(st));
@@ -364,9 +381,17 @@ int scene_setup(naga_scene* s) {
     NAGA_CUDA_TRY(cudaMemsetAsync(ring, 0, sizeof(float) * V.probe_cap * std::max(1, d.n_probes), st));
     V.probe_ring = ring;
 
-    const int npb = nodes_per_pass(D);
     make_items(0, N, s->items_all);
-    make_items(0, N, s->items_all_mt, npb);
+    // pass-sized items follow the pass order of the tables: [0, nbl), [nbl, N)
+    make_items(0, s->nbl, s->items_all_mt, npb);
+    {
+        std::vector<WorkItem> rest;
+        make_items(s->nbl, N, rest, npb);
+        for (WorkItem it : rest) {
+            it.local = (uint32_t)s->items_all_mt.size();
+            s->items_all_mt.push_back(it);
+        }
+    }
     make_items(0, s->nbl, s->items_fluid, npb);
     make_items(s->nbl, s->nbl + s->nbd, s->items_edge, npb);
     // bulk/layer items with at least one stencil support in the layer
@@ -617,7 +642,7 @@ extern "C" int naga_scene_step(naga_scene* s, int nsteps) {
 extern "C" int naga_scene_sync(naga_scene* s) {
     if (!s) return set_error(NAGA_EINVAL, "naga_scene_sync: null scene");
     NAGA_CUDA_TRY(cudaStreamSynchronize(active_stream(s)));
-    return NAGA_OK;
+    return tile_timeout_check(active_stream(s));
 }
 
 extern "C" int64_t naga_scene_step_count(const naga_scene* s) { return s ? s->steps : -1; }
@@ -628,12 +653,14 @@ extern "C" int naga_scene_read_probes(naga_scene* s, int64_t first, int64_t coun
     if (first < 0 || count < 0 || first + count > s->steps || first < s->steps - cap)
         return set_error(NAGA_EINVAL, "naga_scene_read_probes: requested steps are not in the probe ring");
     if (np == 0 || count == 0) return NAGA_OK;
-    NAGA_CUDA_TRY(cudaStreamSynchronize(active_stream(s)));
-    std::vector<float> ring((size_t)cap * np);
-    NAGA_CUDA_TRY(cudaMemcpyAsync(ring.data(), s->dev.probe_ring, sizeof(float) * ring.size(), cudaMemcpyDeviceToHost, active_stream(s)));
-    NAGA_CUDA_TRY(cudaStreamSynchronize(active_stream(s)));
-    for (int64_t t = 0; t < count; ++t)
-        std::memcpy(out + t * np, ring.data() + ((first + t) % cap) * np, sizeof(float) * np);
+    // the requested steps occupy at most two runs of the ring
+    cudaStream_t st = active_stream(s);
+    const int64_t a = first % cap, n1 = std::min<int64_t>(count, cap - a);
+    NAGA_CUDA_TRY(cudaMemcpyAsync(out, s->dev.probe_ring + a * np, sizeof(float) * n1 * np, cudaMemcpyDeviceToHost, st));
+    if (count > n1)
+        NAGA_CUDA_TRY(cudaMemcpyAsync(out + n1 * np, s->dev.probe_ring, sizeof(float) * (count - n1) * np,
+                                      cudaMemcpyDeviceToHost, st));
+    NAGA_CUDA_TRY(cudaStreamSynchronize(st));
     return NAGA_OK;
 }
 
@@ -672,34 +699,43 @@ extern "C" int naga_scene_read_tables(naga_scene* s, uint32_t* idx, float* W, fl
                                       uint32_t* pidx, float* pw) {
     if (!s) return set_error(NAGA_EINVAL, "naga_scene_read_tables: null scene");
     NAGA_CUDA_TRY(cudaStreamSynchronize(active_stream(s)));
-    const int k = s->desc.k, D = s->dim;
+    const int k = s->desc.k, D = s->dim, npb = nodes_per_pass(D);
     const int64_t N = s->N;
+    // the device tables are in pass order; the outputs are node-major
     if (idx || W || (fw && D == 2)) {
         std::vector<float4> wv((size_t)k * N);
         NAGA_CUDA_TRY(cudaMemcpy(wv.data(), s->dev.stW, sizeof(float4) * wv.size(), cudaMemcpyDeviceToHost));
-        for (size_t e = 0; e < wv.size(); ++e) {
-            if (W) {
-                W[e * D + 0] = wv[e].x;
-                W[e * D + 1] = wv[e].y;
-                if (D == 3) W[e * D + 2] = wv[e].z;
+        for (int64_t i = 0; i < N; ++i)
+            for (int t = 0; t < k; ++t) {
+                const size_t e = (size_t)i * k + t;
+                const float4 r = wv[pass_record(i, t, k, s->nbl, N, npb)];
+                if (W) {
+                    W[e * D + 0] = r.x;
+                    W[e * D + 1] = r.y;
+                    if (D == 3) W[e * D + 2] = r.z;
+                }
+                if (idx) std::memcpy(&idx[e], &r.w, 4);
+                if (fw && D == 2) fw[e] = r.z;
             }
-            if (idx) std::memcpy(&idx[e], &wv[e].w, 4);
-            if (fw && D == 2) fw[e] = wv[e].z;
-        }
     }
     if (fw && D == 3) {
         std::vector<float2> fv((size_t)k * N);
         NAGA_CUDA_TRY(cudaMemcpy(fv.data(), s->dev.stF, sizeof(float2) * fv.size(), cudaMemcpyDeviceToHost));
-        for (size_t e = 0; e < fv.size(); ++e) fw[e] = fv[e].x;
+        for (int64_t i = 0; i < N; ++i)
+            for (int t = 0; t < k; ++t) fw[(size_t)i * k + t] = fv[pass_record(i, t, k, s->nbl, N, npb)].x;
     }
     if ((bidx || bw) && s->nbd > 0) {
-        const size_t n = (size_t)s->nbd * s->desc.k_boundary;
+        const int kb = s->desc.k_boundary;
+        const size_t n = (size_t)s->nbd * kb;
         std::vector<float2> bv(n);
         NAGA_CUDA_TRY(cudaMemcpy(bv.data(), s->dev.btab, sizeof(float2) * n, cudaMemcpyDeviceToHost));
-        for (size_t e = 0; e < n; ++e) {
-            if (bw) bw[e] = bv[e].x;
-            if (bidx) std::memcpy(&bidx[e], &bv[e].y, 4);
-        }
+        for (int64_t q = 0; q < s->nbd; ++q)
+            for (int t = 0; t < kb; ++t) {
+                const size_t e = (size_t)q * kb + t;
+                const float2 r = bv[pass_record(q, t, kb, s->nbd, s->nbd, npb)];
+                if (bw) bw[e] = r.x;
+                if (bidx) std::memcpy(&bidx[e], &r.y, 4);
+            }
     }
     auto tr = [&](const void* dsrc_i, const float* dsrc_w, int64_t nq, int kk, uint32_t* oi, float* ow) -> int {
         if (nq == 0) return NAGA_OK;
@@ -790,7 +826,7 @@ extern "C" int naga_batch_step(naga_batch* b, int nsteps) {
 extern "C" int naga_batch_sync(naga_batch* b) {
     if (!b) return set_error(NAGA_EINVAL, "naga_batch_sync: null batch");
     NAGA_CUDA_TRY(cudaStreamSynchronize(b->stream));
-    return NAGA_OK;
+    return tile_timeout_check(b->stream);
 }
 
 // --------------------------------------------------------------- profiling

@@ -407,11 +407,12 @@ __global__ void divergence_build_kernel(const float* __restrict__ pts, int64_t n
             if (out.W64)
 #pragma unroll
                 for (int d = 0; d < D; ++d) out.W64[(i * k + t) * D + d] = Wt[d];
+            const int64_t at = out.npb > 0 ? pass_record(i, t, k, out.split, out.n_total, out.npb) : i * k + t;
             if (out.Wf) {
                 const float fz = D == 3 ? (float)Wt[D - 1] : (float)(r == 0 ? fw0 : fw1);
-                out.Wf[i * k + t] = make_float4((float)Wt[0], (float)Wt[1], fz, __uint_as_float(jl[r]));
+                out.Wf[at] = make_float4((float)Wt[0], (float)Wt[1], fz, __uint_as_float(jl[r]));
             }
-            if (out.Ff) out.Ff[i * k + t] = make_float2((float)(r == 0 ? fw0 : fw1), __uint_as_float(jl[r]));
+            if (out.Ff) out.Ff[at] = make_float2((float)(r == 0 ? fw0 : fw1), __uint_as_float(jl[r]));
         }
         if (out.delta && lane == 0) out.delta[i] = delta;
         __syncwarp();

@@ -7,13 +7,22 @@
 //                 populations in paired slot order (common.cuh)
 //   Q1a, Q1b      PML trapezoid integrals, rows of QP floats, ping-pong
 //                 by step parity
+//   PHI           rows of the layer nodes' PML field -2 sigma Q1 + sigma^2 Q2
+//   PV            per bulk/layer node: sum_s W_s sigma_j and sum_s W_s
+//                 sigma_j^2 over its layer supports (two float4)
 //   M             float4 per node: (rho - 1, ux, uy, uz) in lattice units
-//   stencil       node-major [N][k] float4 records: D3Q27 (Wx, Wy, Wz,
-//                 index bits); D2Q9 (Wx, Wy, filter weight, index bits)
-//   filter        D3Q27: node-major [N][k] float2 (weight, index bits)
-//   boundary      node-major [nbd][kb] float2 (weight, index bits);
+//   stencil       [N][k] float4 records in pass order (below): D3Q27 (Wx,
+//                 Wy, Wz, index bits); D2Q9 (Wx, Wy, filter weight, index
+//                 bits)
+//   filter        D3Q27: [N][k] float2 (weight, index bits), pass order
+//   boundary      [nbd][kb] float2 (weight, index bits), pass order;
 //                 probes [kp][np] indices + weights
-// Node-major records put a work item's stencil in one contiguous block.
+// Pass order: the nodes are cut into passes of npb consecutive nodes
+// (npb = nodes_per_pass), separately over [0, nbl) and [nbl, N) (boundary
+// tables: over [0, nbd)). A pass's records form one contiguous block (one
+// bulk copy into shared memory) and are neighbour-major inside it: record
+// (node b + r, neighbour s) of the pass [b, b + nn) sits at b k + s nn + r,
+// so the nodes a warp gathers for read consecutive records of the tile.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -45,9 +54,11 @@ struct SceneDev {
     float* S1P;
     float* Q1a;
     float* Q1b;
+    float* PHI;  // [nl][QP] PML field -2 sigma Q1 + sigma^2 Q2 of each layer node
     float4* M;
     // tables
     const float4* stW;
+    const float4* PV;  // [nbl][2]: (V1, V2) = sum over layer supports of W_s sigma_j, W_s sigma_j^2
     const float2* stF;
     const float* sigma;
     const float* normals;
@@ -61,6 +72,16 @@ struct SceneDev {
     float* means;      // [2 QP], slot order
     unsigned long long* step;
 };
+
+// position of record (node i, neighbour t) in pass order; the passes of
+// [0, split) and [split, n) are cut separately
+__host__ __device__ inline int64_t pass_record(int64_t i, int t, int k, int64_t split, int64_t n, int npb) {
+    const int64_t base = i < split ? 0 : split;
+    const int64_t end = i < split ? split : n;
+    const int64_t b = base + (i - base) / npb * npb;
+    const int64_t nn = end - b < npb ? end - b : npb;
+    return b * k + (int64_t)t * nn + (i - b);
+}
 
 struct WorkItem {
     uint32_t scene;
@@ -80,6 +101,10 @@ struct StencilOut {
     float4* Wf;           // scene records [n][k]: (Wx, Wy, Wz | filter weight, index bits)
     float2* Ff;           // D == 3 filter records [n][k] (weight, index bits)
     double filter_sigma;  // Gaussian sigma of the selective filter (h / 2.5)
+    // pass order of Wf / Ff: passes of npb nodes over [0, split) and
+    // [split, n_total); npb = 0 keeps node-major order
+    int64_t split, n_total;
+    int npb;
 };
 
 // One step's launch parameters for a batch of scenes.
@@ -104,6 +129,12 @@ int enqueue_step(int dim, int k, int kb, const StepLaunch& P, cudaStream_t st);
 int nodes_per_pass(int dim);
 const char* kernel_name(int id);
 int kernel_count();
+// NAGA_ETIMEOUT (and clears the flag) if a step kernel gave up waiting for a
+// table copy since the last check; synchronises `st`
+int tile_timeout_check(cudaStream_t st);
+// the per-node PML vectors PV of a scene (stW in pass order)
+int pml_vectors_device(int dim, const float4* stW, const float* sigma, int64_t nb, int64_t nl, int64_t nbl, int64_t n,
+                       int k, float4* PV, cudaStream_t st);
 void prof_begin(int id, cudaStream_t st);
 void prof_end(int id, cudaStream_t st);
 bool prof_on();

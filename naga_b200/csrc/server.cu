@@ -71,6 +71,8 @@ extern "C" int64_t naga_scene_estimate_bytes(const naga_scene_desc* d) {
     int64_t b = N * (8 * QP * 4 + 16 + 1 + (int64_t)d->k * (rec + 8 + 4) + 4 * d->dim);
     b += (int64_t)d->n_boundary * d->k_boundary * 8 + (int64_t)d->n_probes * d->k_probe * 8;
     b += ((N + 127) / 128) * 2 * QP * 8 + (int64_t)std::max(1, d->probe_capacity) * std::max(1, d->n_probes) * 4;
+    // PML field rows of the layer and the per-node mean vectors
+    b += d->n_layer * QP * 4 + (d->n_bulk + d->n_layer + 1) * 32;
     // set-up scratch: kNN sort + distances, nearest-neighbour means
     b += N * (16 + 12 + (int64_t)d->k * 4 + 8);
     return b;

@@ -31,6 +31,11 @@
 // float4 chunk c of the node's row, so one warp-wide load of neighbour rows
 // touches 4 (8) rows instead of 32, and each thread holds two opposite
 // population pairs of its chunk.
+#include <map>
+#include <mutex>
+#include <type_traits>
+#include <utility>
+
 #include "common.cuh"
 #include "scene_dev.hpp"
 
@@ -417,11 +422,13 @@ __device__ __forceinline__ void load_scene(SceneDev& dst, const SceneDev* src) {
 // The item's rows of G and Q1_prev are staged in shared memory by coalesced
 // loads of the whole block before the (register-heavy) per-node work.
 template <class L>
-__global__ void __launch_bounds__(kBlock) k_macro_pml(const WorkItem* __restrict__ items, int nitems,
-                                                      const SceneDev* __restrict__ scenes) {
+__global__ void __launch_bounds__(kBlock, 4) k_macro_pml(const WorkItem* __restrict__ items, int nitems,
+                                                         const SceneDev* __restrict__ scenes) {
     constexpr int Q = L::Q, QP = L::QP;
-    __shared__ double red[kBlock / 32][2 * QP];
+    // rows of the item's nodes: G and Q1_prev in, then the layer terms
+    // (Q1, Q2 of layer nodes, zero elsewhere) for the item's column sums
     __shared__ float4 rowG[kBlock * QP / 4], rowQ[kBlock * QP / 4];
+    __shared__ double red[2][2 * QP];
     NAGA_FOR_ITEMS(items, nitems)
     const int par = (int)(*S.step & 1ull);
     float* Q1cur = par ? S.Q1b : S.Q1a;
@@ -439,26 +446,27 @@ __global__ void __launch_bounds__(kBlock) k_macro_pml(const WorkItem* __restrict
     const int64_t i = (int64_t)it.begin + threadIdx.x;
     const bool active = (int)threadIdx.x < nn;
     const bool layer = active && i >= S.nb && i < S.nb + S.nl;
-    float s1[QP], s2[QP];
-#pragma unroll
-    for (int t = 0; t < QP; ++t) s1[t] = s2[t] = 0.f;
+    float* myG = reinterpret_cast<float*>(rowG) + threadIdx.x * QP;
+    float* myQ = reinterpret_cast<float*>(rowQ) + threadIdx.x * QP;
     if (active) {
-        const float* row = reinterpret_cast<const float*>(rowG) + threadIdx.x * QP;
-        const float* q1p = reinterpret_cast<const float*>(rowQ) + threadIdx.x * QP;
         float g[Q];
 #pragma unroll
-        for (int a = 0; a < Q; ++a) g[a] = row[L::pos(a)];
+        for (int a = 0; a < Q; ++a) g[a] = myG[L::pos(a)];
         float drho, u[3] = {0.f, 0.f, 0.f};
         macros<L>(g, drho, u);
         const float4 mp = S.M[i];
         const float up[3] = {mp.y, mp.z, mp.w};
         S.M[i] = make_float4(drho, u[0], u[1], L::D == 3 ? u[2] : 0.f);
         const float sg = layer ? __ldg(S.sigma + (i - S.nb)) : 0.f;
+        // node i carries NAGA's PML field of layer node i + pml_shift
+        const int64_t jf = i + S.pml_shift;
+        const bool field = jf >= S.nb && jf < S.nb + S.nl;
+        const float sf = field ? __ldg(S.sigma + (jf - S.nb)) : 0.f;
         float dcol[Q];
         collide<L>(g, drho, u, S, dcol);
-        float q1[QP], out[QP];
+        float q1[QP], out[QP], phi[QP];
 #pragma unroll
-        for (int t = 0; t < QP; ++t) q1[t] = out[t] = 0.f;
+        for (int t = 0; t < QP; ++t) q1[t] = out[t] = phi[t] = 0.f;
         const bool src = i < S.nbl && S.is_src[i];
 #pragma unroll
         for (int a = 0; a < Q; ++a) {
@@ -466,14 +474,14 @@ __global__ void __launch_bounds__(kBlock) k_macro_pml(const WorkItem* __restrict
             const float ft = feq_c<L>(a, drho, u);
             const float ftp = feq_c<L>(a, mp.x, up);
             q1[t] = (ft + ftp) * S.dt_lat / 2.f;
-            const float q2 = (q1[t] + q1p[t]) * S.dt_lat / 2.f;
-            if (layer) {
-                s1[t] = q1[t];
-                s2[t] = q2;
-            }
+            const float q2 = (q1[t] + myQ[t]) * S.dt_lat / 2.f;
+            phi[t] = -2.f * sf * q1[t] + sf * sf * q2;
+            myG[t] = layer ? q1[t] : 0.f;
+            myQ[t] = layer ? q2 : 0.f;
             out[t] = layer ? g[a] - sg * (3.f * ft + 3.f * sg * q1[t] + sg * sg * q2) : g[a];
         }
         store_row<L>(Q1cur, i, q1);
+        if (field) store_row<L>(S.PHI, jf - S.nb, phi);
         if (src) store_row<L>(S.S1P, i, out);
         const bool boundary = i >= S.nbl && i < S.nbl + S.nbd;
 #pragma unroll
@@ -482,28 +490,27 @@ __global__ void __launch_bounds__(kBlock) k_macro_pml(const WorkItem* __restrict
             out[t] = boundary ? dcol[a] : out[t] + dcol[a];
         }
         store_row<L>(S.S1, i, out);
-    }
-    // per-item layer sums in FP64, fixed order
-    const bool touches = (int64_t)it.end > S.nb && (int64_t)it.begin < S.nb + S.nl;
-    if (touches) {
-        const int wid = threadIdx.x >> 5;
+    } else {
 #pragma unroll
-        for (int t = 0; t < QP; ++t) {
-            double v1 = warp_sum((double)s1[t]);
-            double v2 = warp_sum((double)s2[t]);
-            if (lane_id() == 0) {
-                red[wid][t] = v1;
-                red[wid][QP + t] = v2;
-            }
-        }
+        for (int t = 0; t < QP; ++t) myG[t] = myQ[t] = 0.f;
+    }
+    // per-item layer sums of Q1 and Q2 in FP64, fixed order: column t of
+    // the rows, two halves of the item summed in node order, then added
+    const bool touches = (int64_t)it.end > S.nb && (int64_t)it.begin < S.nb + S.nl;
+    __syncthreads();
+    if (touches && threadIdx.x < 4 * QP) {
+        const int col = threadIdx.x % (2 * QP), half = threadIdx.x / (2 * QP);
+        const float* base = col < QP ? reinterpret_cast<const float*>(rowG) : reinterpret_cast<const float*>(rowQ);
+        const int t = col < QP ? col : col - QP;
+        const int r0 = half * (kBlock / 2), r1 = min(nn, r0 + kBlock / 2);
+        double v = 0.0;
+        for (int r = r0; r < r1; ++r) v += (double)base[r * QP + t];
+        red[half][col] = v;
     }
     __syncthreads();
-    if (threadIdx.x < 2 * QP) {
-        double v = 0.0;
-        if (touches)
-            for (int wv = 0; wv < kBlock / 32; ++wv) v += red[wv][threadIdx.x];
-        S.partials[(int64_t)it.local * 2 * QP + threadIdx.x] = v;
-    }
+    if (threadIdx.x < 2 * QP)
+        S.partials[(int64_t)it.local * 2 * QP + threadIdx.x] =
+            touches ? red[0][threadIdx.x] + red[1][threadIdx.x] : 0.0;
     NAGA_END_ITEMS
 }
 
@@ -546,84 +553,223 @@ __global__ void k_probe(const SceneDev* __restrict__ scenes) {
 
 // Multi-thread-per-node kernels: one work item = one pass of <= NPB
 // consecutive nodes; thread c of node slot ns owns float4 chunk c of node
-// i = begin + ns. The item's node-major stencil records are first copied to
-// shared memory by coalesced loads of the whole block, so the neighbour loop
-// only waits on the (mostly L2-resident) neighbour rows.
-template <class T>
-__device__ __forceinline__ void stage_tile(T* tile, const T* src, int count) {
-    for (int e = threadIdx.x; e < count; e += blockDim.x) tile[e] = __ldg(src + e);
+// i = begin + ns. The pass's table records (one contiguous block, see
+// scene_dev.hpp) are double-buffered in shared memory: while the block
+// gathers for item w, one thread has already started the bulk copy
+// (cp.async.bulk, completion on an mbarrier) of item w + gridDim.x's
+// records, so the neighbour loop waits only on the neighbour rows. Inside a
+// tile, record (s, ns) sits at s * nn + ns: a warp's four (eight) nodes read
+// consecutive records, free of bank conflicts.
+struct TileSrc {
+    const void* p;
+    uint32_t bytes;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+// one bulk copy global -> shared, completing on `bar` (16-byte aligned
+// addresses, size a multiple of 16: checked by the caller)
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
 }
 
-// tile storage: fixed-size static shared memory for the unrolled stencil
-// sizes, dynamic shared memory (NPB x 64 records) for any other size
-template <class T, int N>
-__device__ __forceinline__ T* static_tile() {
-    __shared__ T t[N];
+// bounded wait for the phase of `bar` with the given parity; false if the
+// copy did not complete within the limit
+constexpr int kTileWaitLimit = 1 << 22;
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    for (int it = 0; it < kTileWaitLimit; ++it) {
+        uint32_t ok;
+        asm volatile(
+            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+            : "=r"(ok)
+            : "r"(smem_u32(bar)), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+}  // namespace
+
+// set (never cleared by the kernels) when a tile wait ran out: the step
+// kernels then return early and the host reports NAGA_ETIMEOUT
+__device__ unsigned int g_tile_timeout;
+
+namespace {
+
+template <class T>
+__device__ __forceinline__ void copy_tile(T* tile, TileSrc src) {
+    const T* g = static_cast<const T*>(src.p);
+    const int count = (int)(src.bytes / sizeof(T));
+    for (int e = threadIdx.x; e < count; e += blockDim.x) tile[e] = __ldg(g + e);
+}
+
+// two tile buffers of CAP records: static shared memory for the unrolled
+// stencil sizes, dynamic shared memory for any other size
+template <class T, int CAP>
+__device__ __forceinline__ T* static_tiles() {
+    __shared__ __align__(128) T t[2 * CAP];
     return t;
 }
 template <class T>
-__device__ __forceinline__ T* dynamic_tile() {
-    extern __shared__ __align__(16) unsigned char dyn_smem[];
+__device__ __forceinline__ T* dynamic_tiles() {
+    extern __shared__ __align__(128) unsigned char dyn_smem[];
     return reinterpret_cast<T*>(dyn_smem);
 }
 template <class T, int NPB, int K>
-__device__ __forceinline__ T* tile_storage() {
+__device__ __forceinline__ T* tile_pair() {
     if constexpr (K > 0)
-        return static_tile<T, NPB * K>();
+        return static_tiles<T, NPB * K>();
     else
-        return dynamic_tile<T>();
+        return dynamic_tiles<T>();
+}
+// records per tile buffer (the generic kernels take stencils of up to 64)
+template <int NPB, int K>
+constexpr int tile_cap() {
+    return NPB * (K > 0 ? K : 64);
 }
 
+// Item loop of the gather kernels. SRC(scene, item) names the item's table
+// block (TileSrc); inside the loop, `S` is the item's scene, `it` the item
+// and `tile` its records.
+#define NAGA_PIPE_BEGIN(T, CAP, SRC)                                                                   \
+    __shared__ SceneDev S;                                                                             \
+    __shared__ __align__(8) uint64_t pipe_bar_[2];                                                     \
+    __shared__ int pipe_bulk_[2];                                                                      \
+    T* const pipe_buf_ = tile_pair<T, G::NPB, K_>();                                                   \
+    if (threadIdx.x == 0) {                                                                            \
+        mbar_init(&pipe_bar_[0]);                                                                      \
+        mbar_init(&pipe_bar_[1]);                                                                      \
+        mbar_init_fence();                                                                             \
+    }                                                                                                  \
+    __syncthreads();                                                                                   \
+    auto pipe_issue_ = [&](int w, int b) {                                                             \
+        const WorkItem itn = items[w];                                                                 \
+        const TileSrc ts = SRC(scenes[itn.scene], itn);                                                \
+        const bool bulk = ts.bytes > 0 && ts.bytes % 16 == 0 && ((uintptr_t)ts.p & 15) == 0 &&         \
+                          ts.bytes <= (uint32_t)(CAP * sizeof(T));                                     \
+        pipe_bulk_[b] = bulk;                                                                          \
+        if (bulk) bulk_load(pipe_buf_ + b * (CAP), ts.p, ts.bytes, &pipe_bar_[b]);                      \
+    };                                                                                                 \
+    uint32_t pipe_par_ = 0;                                                                            \
+    if (threadIdx.x == 0 && (int)blockIdx.x < nitems) pipe_issue_(blockIdx.x, 0);                      \
+    int pipe_t_ = 0;                                                                                   \
+    for (int w_ = blockIdx.x; w_ < nitems; w_ += gridDim.x, ++pipe_t_) {                               \
+        const int b_ = pipe_t_ & 1;                                                                    \
+        const WorkItem it = items[w_];                                                                 \
+        __syncthreads();                                                                               \
+        load_scene(S, scenes + it.scene);                                                              \
+        const bool more_ = w_ + (int)gridDim.x < nitems;                                               \
+        if (threadIdx.x == 0 && more_) pipe_issue_(w_ + gridDim.x, b_ ^ 1);                            \
+        __syncthreads();                                                                               \
+        T* const tile = pipe_buf_ + b_ * (CAP);                                                        \
+        if (pipe_bulk_[b_]) {                                                                          \
+            const bool ok_ = mbar_wait(&pipe_bar_[b_], (pipe_par_ >> b_) & 1u);                        \
+            pipe_par_ ^= 1u << b_;                                                                     \
+            if (__syncthreads_or(!ok_)) {                                                              \
+                if (threadIdx.x == 0) {                                                                \
+                    atomicOr(&g_tile_timeout, 1u);                                                     \
+                    if (more_ && pipe_bulk_[b_ ^ 1])                                                   \
+                        mbar_wait(&pipe_bar_[b_ ^ 1], (pipe_par_ >> (b_ ^ 1)) & 1u);                   \
+                }                                                                                      \
+                return;                                                                                \
+            }                                                                                          \
+        } else {                                                                                       \
+            TileSrc ts_ = SRC(S, it);                                                                  \
+            if (ts_.bytes > (uint32_t)((CAP) * sizeof(T))) ts_.bytes = (uint32_t)((CAP) * sizeof(T));  \
+            copy_tile(tile, ts_);                                                                      \
+            __syncthreads();                                                                           \
+        }
+
+#define NAGA_PIPE_END }
+
+// table blocks of the gather kernels
+struct StencilSrc {  // divergence stencil (Wx, Wy, Wz | filter weight, index)
+    __device__ TileSrc operator()(const SceneDev& sc, const WorkItem& w) const {
+        const int k = sc.k;
+        return {sc.stW + (int64_t)w.begin * k, (uint32_t)((w.end - w.begin) * k * sizeof(float4))};
+    }
+};
+struct FilterSrc {  // D3Q27 filter records of the item's bulk/layer nodes
+    __device__ TileSrc operator()(const SceneDev& sc, const WorkItem& w) const {
+        const int k = sc.k;
+        const int64_t nf = (int64_t)w.begin < sc.nbl ? (int64_t)w.end - w.begin : 0;
+        return {sc.stF + (int64_t)w.begin * k, (uint32_t)(nf * k * sizeof(float2))};
+    }
+};
+struct FilterSrc2 {  // D2Q9: the stencil records carry the filter weights
+    __device__ TileSrc operator()(const SceneDev& sc, const WorkItem& w) const {
+        const int k = sc.k;
+        const int64_t nf = (int64_t)w.begin < sc.nbl ? (int64_t)w.end - w.begin : 0;
+        return {sc.stW + (int64_t)w.begin * k, (uint32_t)(nf * k * sizeof(float4))};
+    }
+};
+struct EdgeSrc {  // boundary interpolation records
+    __device__ TileSrc operator()(const SceneDev& sc, const WorkItem& w) const {
+        const int kb = sc.kb;
+        return {sc.btab + ((int64_t)w.begin - sc.nbl) * kb, (uint32_t)((w.end - w.begin) * kb * sizeof(float2))};
+    }
+};
 
 // PML divergence gathers of pml_absorption.inl:770-855 on bulk/layer nodes
-// whose stencil reaches into the layer: for support j in the layer the field
-// is -2 c sigma_j (Q1 - <Q1>) + c sigma_j^2 (Q2 - <Q2>), read at node
-// j - pml_shift (NAGA's field maps index Q by the layer position,
-// pml_absorption.inl:438-448). Adds to S1 and, on interpolation sources, S1P.
+// whose stencils reach into the layer. NAGA adds div(-2 c sigma (Q1 - <Q1>))
+// + div(c sigma^2 (Q2 - <Q2>)), with sigma of the support node j and Q read
+// at node j - pml_shift (its field maps index Q by the layer position,
+// pml_absorption.inl:438-448). By linearity this is
+//   sum_s (c . W_s) phi_j  +  c . (2 <Q1> V1 - <Q2> V2),
+// phi_j = -2 sigma_j Q1 + sigma_j^2 Q2 (one row per layer node, written by
+// the macro kernel) and V1 = sum_s W_s sigma_j, V2 = sum_s W_s sigma_j^2
+// over the node's layer supports (set-up). Adds to S1 and, on
+// interpolation sources, S1P.
 template <class L, int K>
 __global__ void __launch_bounds__(kBlockMT) k_pml_gather(const WorkItem* __restrict__ items, int nitems,
                                                          const SceneDev* __restrict__ scenes) {
     using G = MT<L>;
-    constexpr int QP = L::QP;
-    float4* tile = tile_storage<float4, G::NPB, K>();
+    constexpr int QP = L::QP, K_ = K;
     const int c = threadIdx.x % G::TPN, ns = threadIdx.x / G::TPN;
     float d0[3], d1[3];
     pair_dirs<L>(c < G::NCH ? c : 0, d0, d1);
-    NAGA_FOR_ITEMS(items, nitems)
+    NAGA_PIPE_BEGIN(float4, (tile_cap<G::NPB, K>()), StencilSrc{})
     const int k = K > 0 ? K : S.k;
     const int nn = (int)(it.end - it.begin);
-    stage_tile(tile, S.stW + (int64_t)it.begin * k, nn * k);
-    __syncthreads();
     const int64_t i = (int64_t)it.begin + ns;
     if (ns < nn && c < G::NCH) {
-        const int par = (int)(*S.step & 1ull);
-        const float* Q1cur = par ? S.Q1b : S.Q1a;
-        const float* Q1prev = par ? S.Q1a : S.Q1b;
-        const float4 m1 = *reinterpret_cast<const float4*>(S.means + 4 * c);
-        const float4 m2 = *reinterpret_cast<const float4*>(S.means + QP + 4 * c);
-        const float dt = S.dt_lat;
         float4 dv = make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll 4
+#pragma unroll 8
         for (int s = 0; s < k; ++s) {
-            const float4 rec = tile[ns * k + s];
-            const uint32_t j = __float_as_uint(rec.w);
-            if ((int64_t)j < S.nb || (int64_t)j >= S.nb + S.nl) continue;
+            const float4 rec = tile[s * nn + ns];
+            const int64_t jl = (int64_t)__float_as_uint(rec.w) - S.nb;
+            if (jl < 0 || jl >= S.nl) continue;
             const float wz = L::D == 3 ? rec.z : 0.f;
-            const float sg = __ldg(S.sigma + ((int64_t)j - S.nb));
-            const int64_t jq = (int64_t)j - S.pml_shift;
-            const float4 a = ld4(Q1cur, jq, QP, c), b = ld4(Q1prev, jq, QP, c);
+            const float4 v = ld4(S.PHI, jl, QP, c);
             const float p0 = d0[0] * rec.x + d0[1] * rec.y + d0[2] * wz;
             const float p1 = d1[0] * rec.x + d1[1] * rec.y + d1[2] * wz;
-            const float sg2 = sg * sg, m2s = -2.f * sg;
-            const float f0 = m2s * (a.x - m1.x) + sg2 * ((a.x + b.x) * dt / 2.f - m2.x);
-            const float f1 = m2s * (a.y - m1.y) + sg2 * ((a.y + b.y) * dt / 2.f - m2.y);
-            const float f2 = m2s * (a.z - m1.z) + sg2 * ((a.z + b.z) * dt / 2.f - m2.z);
-            const float f3 = m2s * (a.w - m1.w) + sg2 * ((a.w + b.w) * dt / 2.f - m2.w);
-            dv.x = fmaf(p0, f0, dv.x);
-            dv.y = fmaf(-p0, f1, dv.y);
-            dv.z = fmaf(p1, f2, dv.z);
-            dv.w = fmaf(-p1, f3, dv.w);
+            dv.x = fmaf(p0, v.x, dv.x);
+            dv.y = fmaf(-p0, v.y, dv.y);
+            dv.z = fmaf(p1, v.z, dv.z);
+            dv.w = fmaf(-p1, v.w, dv.w);
         }
+        const float4 m1 = *reinterpret_cast<const float4*>(S.means + 4 * c);
+        const float4 m2 = *reinterpret_cast<const float4*>(S.means + QP + 4 * c);
+        const float4 v1 = __ldg(S.PV + 2 * i), v2 = __ldg(S.PV + 2 * i + 1);
+        const float e1 = d0[0] * v1.x + d0[1] * v1.y + d0[2] * v1.z;
+        const float e2 = d0[0] * v2.x + d0[1] * v2.y + d0[2] * v2.z;
+        const float f1 = d1[0] * v1.x + d1[1] * v1.y + d1[2] * v1.z;
+        const float f2 = d1[0] * v2.x + d1[1] * v2.y + d1[2] * v2.z;
+        dv.x += 2.f * m1.x * e1 - m2.x * e2;
+        dv.y -= 2.f * m1.y * e1 - m2.y * e2;
+        dv.z += 2.f * m1.z * f1 - m2.z * f2;
+        dv.w -= 2.f * m1.w * f1 - m2.w * f2;
         const float4 o = ld4rw(S.S1, i, QP, c);
         st4(S.S1, i, QP, c, make_float4(o.x + dv.x, o.y + dv.y, o.z + dv.z, o.w + dv.w));
         if (S.is_src[i]) {
@@ -631,7 +777,7 @@ __global__ void __launch_bounds__(kBlockMT) k_pml_gather(const WorkItem* __restr
             st4(S.S1P, i, QP, c, make_float4(q.x + dv.x, q.y + dv.y, q.z + dv.z, q.w + dv.w));
         }
     }
-    NAGA_END_ITEMS
+    NAGA_PIPE_END
 }
 
 // boundary: s1 = interp(s1 of bulk + layer, before collision) + collision
@@ -640,20 +786,17 @@ template <class L, int KB>
 __global__ void __launch_bounds__(kBlockMT) k_edge_collide(const WorkItem* __restrict__ items, int nitems,
                                                            const SceneDev* __restrict__ scenes) {
     using G = MT<L>;
-    constexpr int QP = L::QP;
-    float2* tile = tile_storage<float2, G::NPB, KB>();
+    constexpr int QP = L::QP, K_ = KB;
     const int c = threadIdx.x % G::TPN, ns = threadIdx.x / G::TPN;
-    NAGA_FOR_ITEMS(items, nitems)
+    NAGA_PIPE_BEGIN(float2, (tile_cap<G::NPB, KB>()), EdgeSrc{})
     const int kb = KB > 0 ? KB : S.kb;
     const int nn = (int)(it.end - it.begin);
-    stage_tile(tile, S.btab + ((int64_t)it.begin - S.nbl) * kb, nn * kb);
-    __syncthreads();
     const int64_t i = (int64_t)it.begin + ns;
     if (ns < nn && c < G::NCH) {
         float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll 8
         for (int s = 0; s < kb; ++s) {
-            const float2 r = tile[ns * kb + s];
+            const float2 r = tile[s * nn + ns];
             const float4 v = ld4(S.S1P, __float_as_uint(r.y), QP, c);
             acc.x = fmaf(r.x, v.x, acc.x);
             acc.y = fmaf(r.x, v.y, acc.y);
@@ -663,7 +806,7 @@ __global__ void __launch_bounds__(kBlockMT) k_edge_collide(const WorkItem* __res
         const float4 d = ld4rw(S.S1, i, QP, c);
         st4(S.S1, i, QP, c, make_float4(acc.x + d.x, acc.y + d.y, acc.z + d.z, acc.w + d.w));
     }
-    NAGA_END_ITEMS
+    NAGA_PIPE_END
 }
 
 // bulk + layer: f = s1 + 0.75 sum_s w_s (s1_s - s1) (simulation_engine.cuh:
@@ -673,25 +816,17 @@ template <class L, int K>
 __global__ void __launch_bounds__(kBlockMT) k_filter(const WorkItem* __restrict__ items, int nitems,
                                                      const SceneDev* __restrict__ scenes) {
     using G = MT<L>;
-    constexpr int QP = L::QP;
-    float2* tile = tile_storage<float2, G::NPB, K>();
+    constexpr int QP = L::QP, K_ = K;
+    // D3Q27: (weight, index) filter records; D2Q9: the stencil records,
+    // whose z and w carry the filter weight and the index
+    using T = typename std::conditional<L::D == 3, float2, float4>::type;
+    using Src = typename std::conditional<L::D == 3, FilterSrc, FilterSrc2>::type;
     const int c = threadIdx.x % G::TPN, ns = threadIdx.x / G::TPN;
     float d0[3], d1[3];
     pair_dirs<L>(c < G::NCH ? c : 0, d0, d1);
-    NAGA_FOR_ITEMS(items, nitems)
+    NAGA_PIPE_BEGIN(T, (tile_cap<G::NPB, K>()), Src{})
     const int k = K > 0 ? K : S.k;
     const int nn = (int)(it.end - it.begin);
-    // filter records of the item's bulk/layer nodes: (weight, index bits)
-    const int nf = (int)max((int64_t)0, min((int64_t)it.end, S.nbl) - (int64_t)it.begin);
-    if (L::D == 3) {
-        stage_tile(tile, S.stF + (int64_t)it.begin * k, nf * k);
-    } else {
-        for (int e = threadIdx.x; e < nf * k; e += blockDim.x) {
-            const float4 r = __ldg(S.stW + (int64_t)it.begin * k + e);
-            tile[e] = make_float2(r.z, r.w);
-        }
-    }
-    __syncthreads();
     const int64_t i = (int64_t)it.begin + ns;
     if (ns < nn && c < G::NCH) {
         const float4 f = ld4rw(S.S1, i, QP, c);
@@ -700,7 +835,12 @@ __global__ void __launch_bounds__(kBlockMT) k_filter(const WorkItem* __restrict_
             float4 sum = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll 8
             for (int s = 0; s < k; ++s) {
-                const float2 r = tile[ns * k + s];
+                const T rt = tile[s * nn + ns];
+                float2 r;
+                if constexpr (L::D == 3)
+                    r = rt;
+                else
+                    r = make_float2(rt.z, rt.w);
                 const float4 v = ld4rw(S.S1, __float_as_uint(r.y), QP, c);
                 sum.x = fmaf(r.x, v.x - f.x, sum.x);
                 sum.y = fmaf(r.x, v.y - f.y, sum.y);
@@ -726,7 +866,7 @@ __global__ void __launch_bounds__(kBlockMT) k_filter(const WorkItem* __restrict_
         }
         st4(S.G, i, QP, c, out);
     }
-    NAGA_END_ITEMS
+    NAGA_PIPE_END
 }
 
 // RK4 stage STAGE (detail/rk4_solver.cuh:48-171) with the streaming rates
@@ -737,16 +877,13 @@ template <class L, int K, int STAGE>
 __global__ void __launch_bounds__(kBlockMT) k_rk(const WorkItem* __restrict__ items, int nitems,
                                                  const SceneDev* __restrict__ scenes) {
     using G = MT<L>;
-    constexpr int QP = L::QP;
-    float4* tile = tile_storage<float4, G::NPB, K>();
+    constexpr int QP = L::QP, K_ = K;
     const int c = threadIdx.x % G::TPN, ns = threadIdx.x / G::TPN;
     float d0[3], d1[3];
     pair_dirs<L>(c < G::NCH ? c : 0, d0, d1);
-    NAGA_FOR_ITEMS(items, nitems)
+    NAGA_PIPE_BEGIN(float4, (tile_cap<G::NPB, K>()), StencilSrc{})
     const int k = K > 0 ? K : S.k;
     const int nn = (int)(it.end - it.begin);
-    stage_tile(tile, S.stW + (int64_t)it.begin * k, nn * k);
-    __syncthreads();
     const int64_t i = (int64_t)it.begin + ns;
     if (ns < nn && c < G::NCH) {
         const float* src = (STAGE == 1) ? S.G : (STAGE == 2) ? S.G1 : (STAGE == 3) ? S.G2 : S.G1;
@@ -755,7 +892,7 @@ __global__ void __launch_bounds__(kBlockMT) k_rk(const WorkItem* __restrict__ it
         float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll 8
         for (int s = 0; s < k; ++s) {
-            const float4 rec = tile[ns * k + s];
+            const float4 rec = tile[s * nn + ns];
             const uint32_t j = __float_as_uint(rec.w);
             const float wz = L::D == 3 ? rec.z : 0.f;
             const float4 v = ld4((int64_t)j < S.nbl ? src : S.G, j, QP, c);
@@ -784,7 +921,7 @@ __global__ void __launch_bounds__(kBlockMT) k_rk(const WorkItem* __restrict__ it
                                              acc.w + kv.w * S.b2));
         }
     }
-    NAGA_END_ITEMS
+    NAGA_PIPE_END
 }
 
 // boundary: f = interp(f of bulk + layer) (simulation_engine.cuh:1370)
@@ -792,20 +929,17 @@ template <class L, int KB>
 __global__ void __launch_bounds__(kBlockMT) k_edge_interp(const WorkItem* __restrict__ items, int nitems,
                                                           const SceneDev* __restrict__ scenes) {
     using G = MT<L>;
-    constexpr int QP = L::QP;
-    float2* tile = tile_storage<float2, G::NPB, KB>();
+    constexpr int QP = L::QP, K_ = KB;
     const int c = threadIdx.x % G::TPN, ns = threadIdx.x / G::TPN;
-    NAGA_FOR_ITEMS(items, nitems)
+    NAGA_PIPE_BEGIN(float2, (tile_cap<G::NPB, KB>()), EdgeSrc{})
     const int kb = KB > 0 ? KB : S.kb;
     const int nn = (int)(it.end - it.begin);
-    stage_tile(tile, S.btab + ((int64_t)it.begin - S.nbl) * kb, nn * kb);
-    __syncthreads();
     const int64_t i = (int64_t)it.begin + ns;
     if (ns < nn && c < G::NCH) {
         float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll 8
         for (int s = 0; s < kb; ++s) {
-            const float2 r = tile[ns * kb + s];
+            const float2 r = tile[s * nn + ns];
             const float4 v = ld4rw(S.G, __float_as_uint(r.y), QP, c);
             acc.x = fmaf(r.x, v.x, acc.x);
             acc.y = fmaf(r.x, v.y, acc.y);
@@ -814,7 +948,7 @@ __global__ void __launch_bounds__(kBlockMT) k_edge_interp(const WorkItem* __rest
         }
         st4(S.G, i, QP, c, acc);
     }
-    NAGA_END_ITEMS
+    NAGA_PIPE_END
 }
 
 __global__ void k_step_end(const SceneDev* __restrict__ scenes, int nscenes) {
@@ -848,12 +982,62 @@ const char* kernel_name(int id) {
     return (id >= 0 && id < K_COUNT) ? names[id] : "?";
 }
 int kernel_count() { return K_COUNT; }
+
+namespace {
+// V1 = sum_s W_s sigma_j, V2 = sum_s W_s sigma_j^2 over the layer supports j
+// of each bulk/layer node, in support order (the mean part of the PML
+// gather, see k_pml_gather)
+__global__ void pml_vectors_kernel(const float4* __restrict__ stW, const float* __restrict__ sigma, int64_t nb,
+                                   int64_t nl, int64_t nbl, int64_t n, int k, int npb, int dim,
+                                   float4* __restrict__ PV) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nbl) return;
+    float4 v1 = make_float4(0.f, 0.f, 0.f, 0.f), v2 = v1;
+    for (int s = 0; s < k; ++s) {
+        const float4 r = stW[pass_record(i, s, k, nbl, n, npb)];
+        const int64_t jl = (int64_t)__float_as_uint(r.w) - nb;
+        if (jl < 0 || jl >= nl) continue;
+        const float sg = sigma[jl], sg2 = sg * sg;
+        v1.x = fmaf(r.x, sg, v1.x);
+        v1.y = fmaf(r.y, sg, v1.y);
+        v2.x = fmaf(r.x, sg2, v2.x);
+        v2.y = fmaf(r.y, sg2, v2.y);
+        if (dim == 3) {  // D2Q9 records carry the filter weight in z
+            v1.z = fmaf(r.z, sg, v1.z);
+            v2.z = fmaf(r.z, sg2, v2.z);
+        }
+    }
+    PV[2 * i] = v1;
+    PV[2 * i + 1] = v2;
+}
+}  // namespace
+
+int pml_vectors_device(int dim, const float4* stW, const float* sigma, int64_t nb, int64_t nl, int64_t nbl, int64_t n,
+                       int k, float4* PV, cudaStream_t st) {
+    if (nbl <= 0) return NAGA_OK;
+    const int npb = nodes_per_pass(dim);
+    pml_vectors_kernel<<<(unsigned)((nbl + 255) / 256), 256, 0, st>>>(stW, sigma, nb, nl, nbl, n, k, npb, dim, PV);
+    NAGA_CUDA_TRY(cudaGetLastError());
+    return NAGA_OK;
+}
+
+int tile_timeout_check(cudaStream_t st) {
+    unsigned int flag = 0;
+    NAGA_CUDA_TRY(cudaMemcpyFromSymbolAsync(&flag, g_tile_timeout, sizeof(flag), 0, cudaMemcpyDeviceToHost, st));
+    NAGA_CUDA_TRY(cudaStreamSynchronize(st));
+    if (!flag) return NAGA_OK;
+    const unsigned int zero = 0;
+    NAGA_CUDA_TRY(cudaMemcpyToSymbolAsync(g_tile_timeout, &zero, sizeof(zero), 0, cudaMemcpyHostToDevice, st));
+    NAGA_CUDA_TRY(cudaStreamSynchronize(st));
+    return set_error(NAGA_ETIMEOUT, "step kernel: a table copy into shared memory did not complete in time");
+}
 int nodes_per_pass(int dim) { return dim == 2 ? MT<D2Q9>::NPB : MT<D3Q27>::NPB; }
 
-// dynamic shared memory of the generic (K == 0) variants: NPB x 64 records
+// dynamic shared memory of the generic (K == 0) variants: two buffers of
+// NPB x 64 records
 template <class L, int K, class T>
 size_t tile_bytes() {
-    return K > 0 ? 0 : (size_t)MT<L>::NPB * 64 * sizeof(T);
+    return K > 0 ? 0 : 2 * (size_t)MT<L>::NPB * 64 * sizeof(T);
 }
 template <class Kern>
 int allow_smem(Kern kern, size_t bytes) {
@@ -861,10 +1045,27 @@ int allow_smem(Kern kern, size_t bytes) {
     return NAGA_OK;
 }
 
+// resident blocks per SM of a kernel at its launch shape (occupancy
+// calculator, cached per kernel)
+template <class Kern>
+int resident_blocks(Kern kern, int block, size_t smem) {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, size_t>, int> cache;
+    const auto key = std::make_pair(reinterpret_cast<const void*>(kern), smem);
+    std::lock_guard<std::mutex> lk(mu);
+    auto f = cache.find(key);
+    if (f != cache.end()) return f->second;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, block, smem) != cudaSuccess || n < 1) n = 1;
+    cache[key] = n;
+    return n;
+}
+
 template <class L, int K, int KB>
 int enqueue_step_k(const StepLaunch& P, cudaStream_t st) {
     const int cap = sm_count() * 8;
-    const size_t s4 = tile_bytes<L, K, float4>(), s2 = tile_bytes<L, K, float2>(), sb = tile_bytes<L, KB, float2>();
+    using TF = typename std::conditional<L::D == 3, float2, float4>::type;  // filter records
+    const size_t s4 = tile_bytes<L, K, float4>(), s2 = tile_bytes<L, K, TF>(), sb = tile_bytes<L, KB, float2>();
     int rc;
     if ((rc = allow_smem(k_pml_gather<L, K>, s4)) || (rc = allow_smem(k_rk<L, K, 1>, s4)) ||
         (rc = allow_smem(k_rk<L, K, 2>, s4)) || (rc = allow_smem(k_rk<L, K, 3>, s4)) ||
@@ -872,6 +1073,13 @@ int enqueue_step_k(const StepLaunch& P, cudaStream_t st) {
         (rc = allow_smem(k_edge_collide<L, KB>, sb)) || (rc = allow_smem(k_edge_interp<L, KB>, sb)))
         return rc;
     auto grid = [&](int n) { return n < cap ? n : cap; };
+    // the pipelined gather kernels loop over their items: one wave of
+    // resident blocks
+    const int sms = sm_count();
+    auto pgrid = [&](auto kern, size_t smem, int n) {
+        const int g = resident_blocks(kern, kBlockMT, smem) * sms;
+        return n < g ? n : g;
+    };
     const bool prof = prof_on();
 #define LAUNCH(id, n, ...)                      \
     if ((n) > 0) {                              \
@@ -882,17 +1090,17 @@ int enqueue_step_k(const StepLaunch& P, cudaStream_t st) {
     LAUNCH(K_MACRO, P.n_all, (k_macro_pml<L><<<grid(P.n_all), kBlock, 0, st>>>(P.all, P.n_all, P.scenes)));
     LAUNCH(K_MEANS, P.nscenes, (k_pml_means<L::QP><<<dim3(P.nscenes, 2 * L::QP), 256, 0, st>>>(P.scenes)));
     LAUNCH(K_PROBE, P.nscenes, (k_probe<<<P.nscenes, 128, 0, st>>>(P.scenes)));
-    LAUNCH(K_PML, P.n_pml, (k_pml_gather<L, K><<<grid(P.n_pml), kBlockMT, s4, st>>>(P.pml, P.n_pml, P.scenes)));
+    LAUNCH(K_PML, P.n_pml, (k_pml_gather<L, K><<<pgrid(k_pml_gather<L, K>, s4, P.n_pml), kBlockMT, s4, st>>>(P.pml, P.n_pml, P.scenes)));
     LAUNCH(K_EDGE_COLLIDE, P.n_edge,
-           (k_edge_collide<L, KB><<<grid(P.n_edge), kBlockMT, sb, st>>>(P.edge, P.n_edge, P.scenes)));
+           (k_edge_collide<L, KB><<<pgrid(k_edge_collide<L, KB>, sb, P.n_edge), kBlockMT, sb, st>>>(P.edge, P.n_edge, P.scenes)));
     LAUNCH(K_FILTER, P.n_all_mt,
-           (k_filter<L, K><<<grid(P.n_all_mt), kBlockMT, s2, st>>>(P.all_mt, P.n_all_mt, P.scenes)));
-    LAUNCH(K_RK1, P.n_fluid, (k_rk<L, K, 1><<<grid(P.n_fluid), kBlockMT, s4, st>>>(P.fluid, P.n_fluid, P.scenes)));
-    LAUNCH(K_RK2, P.n_fluid, (k_rk<L, K, 2><<<grid(P.n_fluid), kBlockMT, s4, st>>>(P.fluid, P.n_fluid, P.scenes)));
-    LAUNCH(K_RK3, P.n_fluid, (k_rk<L, K, 3><<<grid(P.n_fluid), kBlockMT, s4, st>>>(P.fluid, P.n_fluid, P.scenes)));
-    LAUNCH(K_RK4, P.n_fluid, (k_rk<L, K, 4><<<grid(P.n_fluid), kBlockMT, s4, st>>>(P.fluid, P.n_fluid, P.scenes)));
+           (k_filter<L, K><<<pgrid(k_filter<L, K>, s2, P.n_all_mt), kBlockMT, s2, st>>>(P.all_mt, P.n_all_mt, P.scenes)));
+    LAUNCH(K_RK1, P.n_fluid, (k_rk<L, K, 1><<<pgrid(k_rk<L, K, 1>, s4, P.n_fluid), kBlockMT, s4, st>>>(P.fluid, P.n_fluid, P.scenes)));
+    LAUNCH(K_RK2, P.n_fluid, (k_rk<L, K, 2><<<pgrid(k_rk<L, K, 2>, s4, P.n_fluid), kBlockMT, s4, st>>>(P.fluid, P.n_fluid, P.scenes)));
+    LAUNCH(K_RK3, P.n_fluid, (k_rk<L, K, 3><<<pgrid(k_rk<L, K, 3>, s4, P.n_fluid), kBlockMT, s4, st>>>(P.fluid, P.n_fluid, P.scenes)));
+    LAUNCH(K_RK4, P.n_fluid, (k_rk<L, K, 4><<<pgrid(k_rk<L, K, 4>, s4, P.n_fluid), kBlockMT, s4, st>>>(P.fluid, P.n_fluid, P.scenes)));
     LAUNCH(K_EDGE_INTERP, P.n_edge,
-           (k_edge_interp<L, KB><<<grid(P.n_edge), kBlockMT, sb, st>>>(P.edge, P.n_edge, P.scenes)));
+           (k_edge_interp<L, KB><<<pgrid(k_edge_interp<L, KB>, sb, P.n_edge), kBlockMT, sb, st>>>(P.edge, P.n_edge, P.scenes)));
     LAUNCH(K_STEP_END, P.nscenes, (k_step_end<<<(P.nscenes + 127) / 128, 128, 0, st>>>(P.scenes, P.nscenes)));
 #undef LAUNCH
     NAGA_CUDA_TRY(cudaGetLastError());
@@ -903,8 +1111,8 @@ int enqueue_step_k(const StepLaunch& P, cudaStream_t st) {
 // common sizes get fully unrolled gathers with fixed-size tiles
 int enqueue_step(int dim, int k, int kb, const StepLaunch& P, cudaStream_t st) {
     if (dim == 2) {
+        // unrolled variants whose two tile buffers fit static shared memory
         if (k == 16 && kb == 16) return enqueue_step_k<D2Q9, 16, 16>(P, st);
-        if (k == 32 && kb == 32) return enqueue_step_k<D2Q9, 32, 32>(P, st);
         return enqueue_step_k<D2Q9, 0, 0>(P, st);
     }
     if (k == 32 && kb == 32) return enqueue_step_k<D3Q27, 32, 32>(P, st);
