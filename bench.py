@@ -259,16 +259,23 @@ def run_naga(args, rank, world, local_rank):
         total_ms = float(t.item())
     value = world * N * K / (total_ms * 1e-3) / 1e6
 
-    # ---- end to end through the public API with host buffers
-    host_drho = np.ascontiguousarray(drho, np.float32)
+    # ---- end to end through the public API with host buffers: the initial
+    # density goes up from page-locked host memory, and every step's probe
+    # samples come back (the observer read of each step, queued behind the
+    # step so the device never waits for the host)
+    host_drho = torch.empty(N, dtype=torch.float32, pin_memory=True).numpy()
+    host_drho[:] = drho
+    np_ = len(cfg["probes"])
+    host_probes = torch.empty((K, np_), dtype=torch.float32, pin_memory=True)
     barrier()
     t0 = time.perf_counter()
     scene.set_density(host_drho)
     for t in range(K):
         scene.step(1)
-        scene.probes(t, 1)
-    torch.cuda.synchronize()
+        scene.probes_async(t, 1, host_probes.data_ptr() + 4 * np_ * t)
+    scene.sync()
     e2e_s = time.perf_counter() - t0
+    e2e_trace_ok = bool(np.array_equal(host_probes.numpy(), scene.probes(0, K)))
     if dist:
         t = torch.tensor([e2e_s], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -339,8 +346,9 @@ def run_naga(args, rank, world, local_rank):
         "p50_step_ms": float(np.percentile(per, 50)), "p99_step_ms": float(np.percentile(per, 99)),
         "roofline": roof, "cpu_baseline": cb,
         "e2e": {"value": e2e, "unit": "MNUPS", "h2d_bytes_per_step": int(N * 4 / K),
-                "d2h_bytes_per_step": 4 * len(cfg["probes"])},
+                "d2h_bytes_per_step": 4 * len(cfg["probes"]), "probe_trace_read_back": e2e_trace_ok},
         "gpu_launches": int(gpu_launches), "clocks": clk.summary(), "batched": batched,
+        "launch_shapes": naga.tuning_report().strip().splitlines(),
     }
     print(json.dumps(line), flush=True)
     if dist:

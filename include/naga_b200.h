@@ -218,6 +218,18 @@ int64_t naga_scene_step_count(const naga_scene* scene);
  * last probe_capacity steps. Synchronises the scene's stream.            */
 int naga_scene_read_probes(naga_scene* scene, int64_t first, int64_t count,
                            float* out);
+/* as naga_scene_read_probes, but only enqueues the copy on the scene's
+ * stream behind the steps already enqueued and returns: out (page-locked
+ * host memory for a truly asynchronous copy) is filled once the stream
+ * reaches it, e.g. after naga_scene_sync. An observer of a running
+ * simulation reads every step this way without stalling the device
+ * (NAGA's density_observer reads inside step_forward,
+ * density_observer.cuh:99-113). first + count may run up to the steps
+ * enqueued so far; the ring must still hold step `first` when the copy
+ * runs (count <= probe_capacity, and at most probe_capacity - count steps
+ * enqueued after it).                                                     */
+int naga_scene_read_probes_async(naga_scene* scene, int64_t first,
+                                 int64_t count, float* out);
 /* centred populations g = f - w, host [N][Q], and rho - rho0, host [N]   */
 int naga_scene_read_state(naga_scene* scene, float* g, float* drho);
 int naga_scene_write_state(naga_scene* scene, const float* g);
@@ -302,6 +314,18 @@ int naga_profile_reset(void);
 /* names[i] (static strings), launches[i], ms[i] for i < *count (in/out)  */
 int naga_profile_read(int* count, const char** names, int64_t* launches,
                       double* ms);
+
+/* ---------------------------------------------------------- launch shapes */
+/* The gather kernels' resident blocks per SM are tuned once per batch
+ * shape (lattice, stencil sizes, size class) the first time such a batch
+ * steps: RK stage 1 is timed on the batch's own items for each candidate
+ * (the driver's default shared-memory carveout, then 2 .. max blocks per
+ * SM) and the fastest kept; NAGA_GATHER_BPS=<n> in the environment fixes
+ * it instead. Results never depend on the shape. No NAGA counterpart (its
+ * launch shapes are fixed by its runtime). Writes the tuner's log (one line
+ * per tuned shape: candidates and microseconds per launch) into buf
+ * (NUL-terminated, truncated to cap) and returns its full length.         */
+int64_t naga_tuning_report(char* buf, int64_t cap);
 
 #ifdef __cplusplus
 }

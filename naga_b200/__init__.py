@@ -109,6 +109,8 @@ _SIGS = {
     "naga_server_result": ([C.c_void_p, C.c_int64, C.c_void_p], C.c_int),
     "naga_server_read_stats": ([C.c_void_p, C.c_void_p], C.c_int),
     "naga_profile_enable": ([C.c_int], C.c_int),
+    "naga_tuning_report": ([C.c_char_p, C.c_int64], C.c_int64),
+    "naga_scene_read_probes_async": ([C.c_void_p, C.c_int64, C.c_int64, C.c_void_p], C.c_int),
     "naga_profile_reset": ([], C.c_int),
     "naga_profile_read": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
 }
@@ -251,6 +253,12 @@ class Scene:
         out = np.zeros((count, self.n_probes), np.float32)
         _check(lib().naga_scene_read_probes(self.h, first, count, _p(out)))
         return out
+
+    def probes_async(self, first: int, count: int, out) -> None:
+        """Enqueue the copy of steps [first, first + count) to host address
+        `out` (>= count * n_probes floats, ideally page-locked, kept alive
+        until the next sync); returns at once."""
+        _check(lib().naga_scene_read_probes_async(self.h, first, count, C.c_void_p(int(out))))
 
     def state(self):
         g = np.zeros((self.N, self.Q), np.float32)
@@ -521,3 +529,11 @@ def read_profile() -> dict:
     ms = np.zeros(64, np.float64)
     _check(lib().naga_profile_read(C.byref(n), names, _p(launches), _p(ms)))
     return {names[i].decode(): (int(launches[i]), float(ms[i])) for i in range(n.value)}
+
+
+def tuning_report() -> str:
+    """The launch-shape tuner's log (one line per tuned batch shape)."""
+    n = lib().naga_tuning_report(None, 0)
+    buf = C.create_string_buffer(int(n) + 1)
+    lib().naga_tuning_report(buf, n + 1)
+    return buf.value.decode()

@@ -507,6 +507,7 @@ int batch_step(naga_batch* b, int nsteps) {
     int rc;
     if (b->dirty && (rc = batch_rebuild(b))) return rc;
     StepLaunch P = launch_of(b);
+    if (!b->exec && (rc = tune_step_shapes(b->dim, b->k, b->kb, P, b->stream))) return rc;
     if (prof_on()) {
         for (int n = 0; n < nsteps; ++n)
             if ((rc = enqueue_step(b->dim, b->k, b->kb, P, b->stream))) return rc;
@@ -607,15 +608,21 @@ extern "C" int naga_scene_set_density(naga_scene* s, const float* drho) {
     if (!s) return set_error(NAGA_EINVAL, "naga_scene_set_density: null scene");
     cudaStream_t st = active_stream(s);
     NAGA_CUDA_TRY(cudaStreamSynchronize(st));
-    const int Q = s->Q, QP = s->QP;
-    std::vector<float> g((size_t)s->N * QP, 0.f);
-    if (drho) {
-        auto w = [&](int a) { return s->dim == 2 ? LatticeTables<D2Q9>::w(a) : LatticeTables<D3Q27>::w(a); };
-        for (int64_t i = 0; i < s->N; ++i)
-            for (int a = 0; a < Q; ++a) g[(size_t)i * QP + slot_of(s->dim, a)] = w(a) * drho[i];
-    }
+    const int QP = s->QP;
     SceneDev& V = s->dev;
-    NAGA_CUDA_TRY(cudaMemcpyAsync(V.G, g.data(), sizeof(float) * g.size(), cudaMemcpyHostToDevice, st));
+    // upload the N densities and expand them to population rows on the device
+    float* d = nullptr;
+    if (drho) {
+        NAGA_CUDA_TRY(cudaMallocAsync(&d, sizeof(float) * std::max<int64_t>(s->N, 1), st));
+        cudaError_t e = cudaMemcpyAsync(d, drho, sizeof(float) * s->N, cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) {
+            cudaFreeAsync(d, st);
+            return set_error(NAGA_ECUDA, std::string("naga_scene_set_density: ") + cudaGetErrorString(e));
+        }
+    }
+    int rc = density_rows_device(s->dim, d, s->N, V.G, st);
+    if (d) cudaFreeAsync(d, st);
+    if (rc) return rc;
     NAGA_CUDA_TRY(cudaMemsetAsync(V.M, 0, sizeof(float4) * s->N, st));
     NAGA_CUDA_TRY(cudaMemsetAsync(V.Q1a, 0, sizeof(float) * s->N * QP, st));
     NAGA_CUDA_TRY(cudaMemsetAsync(V.Q1b, 0, sizeof(float) * s->N * QP, st));
@@ -661,6 +668,21 @@ extern "C" int naga_scene_read_probes(naga_scene* s, int64_t first, int64_t coun
         NAGA_CUDA_TRY(cudaMemcpyAsync(out + n1 * np, s->dev.probe_ring, sizeof(float) * (count - n1) * np,
                                       cudaMemcpyDeviceToHost, st));
     NAGA_CUDA_TRY(cudaStreamSynchronize(st));
+    return NAGA_OK;
+}
+
+extern "C" int naga_scene_read_probes_async(naga_scene* s, int64_t first, int64_t count, float* out) {
+    if (!s || (!out && count > 0)) return set_error(NAGA_EINVAL, "naga_scene_read_probes_async: null argument");
+    const int np = s->dev.np, cap = s->dev.probe_cap;
+    if (first < 0 || count < 0 || count > cap || first + count > s->steps || first < s->steps - cap)
+        return set_error(NAGA_EINVAL, "naga_scene_read_probes_async: requested steps are not in the probe ring");
+    if (np == 0 || count == 0) return NAGA_OK;
+    cudaStream_t st = active_stream(s);
+    const int64_t a = first % cap, n1 = std::min<int64_t>(count, cap - a);
+    NAGA_CUDA_TRY(cudaMemcpyAsync(out, s->dev.probe_ring + a * np, sizeof(float) * n1 * np, cudaMemcpyDeviceToHost, st));
+    if (count > n1)
+        NAGA_CUDA_TRY(cudaMemcpyAsync(out + n1 * np, s->dev.probe_ring, sizeof(float) * (count - n1) * np,
+                                      cudaMemcpyDeviceToHost, st));
     return NAGA_OK;
 }
 
@@ -827,6 +849,16 @@ extern "C" int naga_batch_sync(naga_batch* b) {
     if (!b) return set_error(NAGA_EINVAL, "naga_batch_sync: null batch");
     NAGA_CUDA_TRY(cudaStreamSynchronize(b->stream));
     return tile_timeout_check(b->stream);
+}
+
+extern "C" int64_t naga_tuning_report(char* buf, int64_t cap) {
+    const std::string r = tuning_report();
+    if (buf && cap > 0) {
+        const int64_t n = std::min<int64_t>(cap - 1, (int64_t)r.size());
+        std::memcpy(buf, r.data(), (size_t)n);
+        buf[n] = 0;
+    }
+    return (int64_t)r.size();
 }
 
 // --------------------------------------------------------------- profiling

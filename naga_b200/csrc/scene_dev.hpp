@@ -27,6 +27,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <string>
+
 namespace naga {
 
 struct SceneDev {
@@ -132,6 +134,14 @@ int kernel_count();
 // NAGA_ETIMEOUT (and clears the flag) if a step kernel gave up waiting for a
 // table copy since the last check; synchronises `st`
 int tile_timeout_check(cudaStream_t st);
+// G rows of the rest state plus a density perturbation (device drho [n],
+// or null for the rest state)
+int density_rows_device(int dim, const float* drho, int64_t n, float* G, cudaStream_t st);
+// chooses the gather kernels' resident blocks per SM for this batch shape
+// (once per shape; must not run during stream capture)
+int tune_step_shapes(int dim, int k, int kb, const StepLaunch& P, cudaStream_t st);
+// the tuner's measurements, one line per tuned shape
+std::string tuning_report();
 // the per-node PML vectors PV of a scene (stW in pass order)
 int pml_vectors_device(int dim, const float4* stW, const float* sigma, int64_t nb, int64_t nl, int64_t nbl, int64_t n,
                        int k, float4* PV, cudaStream_t st);

@@ -31,8 +31,14 @@
 // float4 chunk c of the node's row, so one warp-wide load of neighbour rows
 // touches 4 (8) rows instead of 32, and each thread holds two opposite
 // population pairs of its chunk.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <map>
 #include <mutex>
+#include <string>
+#include <tuple>
 #include <type_traits>
 #include <utility>
 
@@ -1021,6 +1027,30 @@ int pml_vectors_device(int dim, const float4* stW, const float* sigma, int64_t n
     return NAGA_OK;
 }
 
+namespace {
+// rest state plus a density perturbation: g = f - w = w drho (u = 0)
+template <class L>
+__global__ void density_rows_kernel(const float* __restrict__ drho, int64_t n, float* __restrict__ G) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n * L::QP) return;
+    const int64_t i = e / L::QP;
+    const int a = L::row((int)(e - i * L::QP));
+    G[e] = (a < 0 || !drho) ? 0.f : LatticeTables<L>::w(a) * drho[i];
+}
+}  // namespace
+
+int density_rows_device(int dim, const float* drho, int64_t n, float* G, cudaStream_t st) {
+    const int QP = dim == 2 ? D2Q9::QP : D3Q27::QP;
+    const unsigned blocks = (unsigned)((n * QP + 255) / 256);
+    if (blocks == 0) return NAGA_OK;
+    if (dim == 2)
+        density_rows_kernel<D2Q9><<<blocks, 256, 0, st>>>(drho, n, G);
+    else
+        density_rows_kernel<D3Q27><<<blocks, 256, 0, st>>>(drho, n, G);
+    NAGA_CUDA_TRY(cudaGetLastError());
+    return NAGA_OK;
+}
+
 int tile_timeout_check(cudaStream_t st) {
     unsigned int flag = 0;
     NAGA_CUDA_TRY(cudaMemcpyFromSymbolAsync(&flag, g_tile_timeout, sizeof(flag), 0, cudaMemcpyDeviceToHost, st));
@@ -1061,6 +1091,89 @@ int resident_blocks(Kern kern, int block, size_t smem) {
     return n;
 }
 
+// ------------------------------------------------------------ launch shapes
+// The gather kernels share the SM's unified L1 / shared-memory storage
+// between their tile buffers and the L1 cache that absorbs the neighbour-row
+// re-reads: more resident blocks hide more latency but leave less L1. The
+// number of resident blocks per SM (bps) is set through the shared-memory
+// carveout and chosen per (lattice, k, kb, batch size) by tune_step_shapes;
+// bps = 0 keeps the driver's default carveout and the occupancy maximum.
+struct ShapeKey {
+    int dim, k, kb, bucket;
+    bool operator<(const ShapeKey& o) const {
+        return std::tie(dim, k, kb, bucket) < std::tie(o.dim, o.k, o.kb, o.bucket);
+    }
+};
+std::mutex g_shape_mu;
+std::map<ShapeKey, int> g_shape;  // tuned bps per batch shape
+std::string g_tune_log;
+
+int smem_per_sm() {
+    static int v = 0;
+    if (!v) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess || v <= 0)
+            v = 228 * 1024;
+    }
+    return v;
+}
+
+// carveout (percent of the maximum shared memory) that holds bps blocks of
+// the kernel; bps = 0 restores the default preference
+template <class Kern>
+int set_blocks_per_sm(Kern kern, size_t dyn_smem, int bps) {
+    int pct = -1;  // cudaSharedmemCarveoutDefault
+    if (bps > 0) {
+        cudaFuncAttributes fa{};
+        NAGA_CUDA_TRY(cudaFuncGetAttributes(&fa, kern));
+        const double need = (double)bps * (double)(fa.sharedSizeBytes + dyn_smem + 1024);
+        pct = (int)std::ceil(100.0 * need / smem_per_sm());
+        pct = pct < 1 ? 1 : (pct > 100 ? 100 : pct);
+    }
+    NAGA_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+    return NAGA_OK;
+}
+
+ShapeKey shape_key(int dim, int k, int kb, int n_items) {
+    int b = 0;
+    while ((1 << (b + 1)) <= n_items) ++b;
+    return {dim, k, kb, b};
+}
+
+int tuned_bps(const ShapeKey& key) {
+    std::lock_guard<std::mutex> lk(g_shape_mu);
+    auto f = g_shape.find(key);
+    return f == g_shape.end() ? 0 : f->second;
+}
+
+template <class L, int K, int KB>
+struct AppliedShape {
+    static int bps;  // carveout currently set on the instantiation's kernels (-2: unknown)
+};
+template <class L, int K, int KB>
+int AppliedShape<L, K, KB>::bps = -2;
+
+// carveout of every gather kernel of an instantiation (set only when the
+// shape changes)
+template <class L, int K, int KB>
+int apply_shape(int bps) {
+    int& applied = AppliedShape<L, K, KB>::bps;
+    std::lock_guard<std::mutex> lk(g_shape_mu);
+    if (applied == bps) return NAGA_OK;
+    using TF = typename std::conditional<L::D == 3, float2, float4>::type;
+    const size_t s4 = tile_bytes<L, K, float4>(), s2 = tile_bytes<L, K, TF>(), sb = tile_bytes<L, KB, float2>();
+    int rc;
+    if ((rc = set_blocks_per_sm(k_pml_gather<L, K>, s4, bps)) || (rc = set_blocks_per_sm(k_rk<L, K, 1>, s4, bps)) ||
+        (rc = set_blocks_per_sm(k_rk<L, K, 2>, s4, bps)) || (rc = set_blocks_per_sm(k_rk<L, K, 3>, s4, bps)) ||
+        (rc = set_blocks_per_sm(k_rk<L, K, 4>, s4, bps)) || (rc = set_blocks_per_sm(k_filter<L, K>, s2, bps)) ||
+        (rc = set_blocks_per_sm(k_edge_collide<L, KB>, sb, bps)) ||
+        (rc = set_blocks_per_sm(k_edge_interp<L, KB>, sb, bps)))
+        return rc;
+    applied = bps;
+    return NAGA_OK;
+}
+
 template <class L, int K, int KB>
 int enqueue_step_k(const StepLaunch& P, cudaStream_t st) {
     const int cap = sm_count() * 8;
@@ -1074,10 +1187,14 @@ int enqueue_step_k(const StepLaunch& P, cudaStream_t st) {
         return rc;
     auto grid = [&](int n) { return n < cap ? n : cap; };
     // the pipelined gather kernels loop over their items: one wave of
-    // resident blocks
+    // resident blocks, bps per SM when the tuned shape fixes it
     const int sms = sm_count();
+    const int bps = tuned_bps(shape_key(L::D, K, KB, P.n_fluid));
+    if ((rc = apply_shape<L, K, KB>(bps))) return rc;
     auto pgrid = [&](auto kern, size_t smem, int n) {
-        const int g = resident_blocks(kern, kBlockMT, smem) * sms;
+        int r = resident_blocks(kern, kBlockMT, smem);
+        if (bps > 0 && bps < r) r = bps;
+        const int g = r * sms;
         return n < g ? n : g;
     };
     const bool prof = prof_on();
@@ -1105,6 +1222,90 @@ int enqueue_step_k(const StepLaunch& P, cudaStream_t st) {
 #undef LAUNCH
     NAGA_CUDA_TRY(cudaGetLastError());
     return NAGA_OK;
+}
+
+// Launch-shape tuner: times RK stage 1 (it reads G and overwrites only the
+// stage scratch G1 and ACC, so it can run between steps) on the batch's own
+// items for each candidate -- the default carveout (0), then 2 .. max
+// resident blocks per SM -- and keeps the fastest (a fixed carveout only
+// when it beats the default by 3%). NAGA_GATHER_BPS=<n>
+// fixes the choice instead (0: default carveout).
+template <class L, int K, int KB>
+int tune_k(const StepLaunch& P, cudaStream_t st) {
+    if (P.n_fluid <= 0) return NAGA_OK;
+    const ShapeKey key = shape_key(L::D, K, KB, P.n_fluid);
+    {
+        std::lock_guard<std::mutex> lk(g_shape_mu);
+        if (g_shape.count(key)) return NAGA_OK;
+    }
+    const size_t s4 = tile_bytes<L, K, float4>();
+    int rc;
+    if ((rc = allow_smem(k_rk<L, K, 1>, s4))) return rc;
+    char line[160];
+    if (const char* env = std::getenv("NAGA_GATHER_BPS")) {
+        const int v = std::atoi(env);
+        std::lock_guard<std::mutex> lk(g_shape_mu);
+        g_shape[key] = v > 0 ? v : 0;
+        std::snprintf(line, sizeof line, "dim %d k %d kb %d items 2^%d: bps %d (NAGA_GATHER_BPS)\n", key.dim, key.k,
+                      key.kb, key.bucket, g_shape[key]);
+        g_tune_log += line;
+        return NAGA_OK;
+    }
+    if ((rc = set_blocks_per_sm(k_rk<L, K, 1>, s4, 0))) return rc;
+    int maxr = 0;
+    NAGA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxr, k_rk<L, K, 1>, kBlockMT, s4));
+    maxr = std::max(maxr, 1);
+    const int sms = sm_count();
+    cudaEvent_t e0, e1;
+    NAGA_CUDA_TRY(cudaEventCreate(&e0));
+    NAGA_CUDA_TRY(cudaEventCreate(&e1));
+    int best = -1;
+    float best_ms = 0.f;
+    std::string log;
+    for (int bps = 0; bps <= maxr; bps = bps == 0 ? 2 : bps + 1) {
+        if ((rc = set_blocks_per_sm(k_rk<L, K, 1>, s4, bps))) break;
+        const int g = std::min(P.n_fluid, (bps > 0 ? bps : maxr) * sms);
+        for (int r = 0; r < 2; ++r) k_rk<L, K, 1><<<g, kBlockMT, s4, st>>>(P.fluid, P.n_fluid, P.scenes);
+        cudaEventRecord(e0, st);
+        for (int r = 0; r < 5; ++r) k_rk<L, K, 1><<<g, kBlockMT, s4, st>>>(P.fluid, P.n_fluid, P.scenes);
+        cudaEventRecord(e1, st);
+        if (cudaEventSynchronize(e1) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+            rc = set_error(NAGA_ECUDA, "launch-shape tuning: a trial launch failed");
+            break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        std::snprintf(line, sizeof line, " %d:%.1fus", bps, ms * 1000.f / 5);
+        log += line;
+        // a fixed carveout must beat the default by 3% to be kept: it also
+        // binds the other gather kernels, whose best split may differ
+        if (best < 0 || ms < best_ms * (best == 0 ? 0.97f : 1.f)) {
+            best = bps;
+            best_ms = ms;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    AppliedShape<L, K, KB>::bps = -2;  // the trials changed rk stage 1's carveout
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(g_shape_mu);
+    g_shape[key] = best < 0 ? 0 : best;
+    std::snprintf(line, sizeof line, "dim %d k %d kb %d items 2^%d: bps %d of", key.dim, key.k, key.kb, key.bucket,
+                  g_shape[key]);
+    g_tune_log += line + log + "\n";
+    return NAGA_OK;
+}
+
+int tune_step_shapes(int dim, int k, int kb, const StepLaunch& P, cudaStream_t st) {
+    if (dim == 2) return k == 16 && kb == 16 ? tune_k<D2Q9, 16, 16>(P, st) : tune_k<D2Q9, 0, 0>(P, st);
+    if (k == 32 && kb == 32) return tune_k<D3Q27, 32, 32>(P, st);
+    if (k == 16 && kb == 16) return tune_k<D3Q27, 16, 16>(P, st);
+    return tune_k<D3Q27, 0, 0>(P, st);
+}
+
+std::string tuning_report() {
+    std::lock_guard<std::mutex> lk(g_shape_mu);
+    return g_tune_log;
 }
 
 // k, kb: the batch's common stencil sizes (0 if the members differ); the

@@ -115,3 +115,66 @@ def test_step_is_deterministic(naga, oracle):
     b.step(10)
     assert np.array_equal(a.state()[0], b.state()[0])
     assert np.array_equal(a.probes(), b.probes())
+
+
+_SHAPE_RUN = """
+import sys, numpy as np
+sys.path.insert(0, {root!r})
+import naga_b200 as naga
+g = naga.generate_grid(3, 20, 3, 4)
+s = naga.Scene(g, k=32, shape=0, probes=np.array({probes!r}, np.float32))
+s.set_density(naga.gaussian_pulse(g["points"], [0.5] * 3, 1e-3, 0.05))
+s.step(15)
+np.save({out!r}, np.concatenate([s.state()[0].ravel(), s.probes().ravel()]))
+print(naga.tuning_report())
+"""
+
+
+def test_launch_shape_does_not_change_results(tmp_path):
+    """The tuner's choice of resident blocks per SM changes only the grid:
+    a run with the tuned shape and one forced to 2 blocks per SM agree bit
+    for bit, and the tuner logs what it measured."""
+    import os
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    outs, logs = [], []
+    for env_bps in (None, "2"):
+        out = str(tmp_path / f"run_{env_bps}.npy")
+        env = dict(os.environ)
+        env.pop("NAGA_GATHER_BPS", None)
+        if env_bps:
+            env["NAGA_GATHER_BPS"] = env_bps
+        code = _SHAPE_RUN.format(root=root, probes=PROBES3.tolist(), out=out)
+        r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+        outs.append(np.load(out))
+        logs.append(r.stdout)
+    assert np.array_equal(outs[0], outs[1])
+    assert "dim 3 k 32 kb 32" in logs[0] and " 0:" in logs[0]
+    assert "bps 2 (NAGA_GATHER_BPS)" in logs[1]
+
+
+def test_async_probe_reads_match_synchronous(naga, oracle):
+    """Probe samples queued every step behind the step (page-locked host
+    buffer, one sync at the end) equal the synchronous read, including a
+    read that wraps around the ring."""
+    import torch
+
+    g = naga.generate_grid(2, 30, 3, 7)
+    s = naga.Scene(g, k=16, probes=PROBES2, probe_capacity=16)
+    s.set_density(naga.gaussian_pulse(g["points"], [0.5, 0.5], 1e-3, 0.08))
+    out = torch.zeros((40, 4), dtype=torch.float32, pin_memory=True)
+    for t in range(40):
+        s.step(1)
+        s.probes_async(t, 1, out.data_ptr() + 16 * t)
+    s.sync()
+    ref = naga.Scene(g, k=16, probes=PROBES2, probe_capacity=64)
+    ref.set_density(naga.gaussian_pulse(g["points"], [0.5, 0.5], 1e-3, 0.08))
+    ref.step(40)
+    assert np.array_equal(out.numpy(), ref.probes(0, 40))
+    wrap = torch.zeros((10, 4), dtype=torch.float32, pin_memory=True)
+    s.probes_async(30, 10, wrap.data_ptr())  # ring slots 14, 15, 0, ..., 7
+    s.sync()
+    assert np.array_equal(wrap.numpy(), ref.probes(30, 10))
