@@ -6,11 +6,13 @@
 // a fixed sequence of fused kernels over work items (<= 128 consecutive nodes
 // of one scene), so one launch covers every scene of a batch:
 //
-//   macro_pml     all nodes   rho, u; PML trapezoid integrals Q1, Q2 and the
-//                             local absorption term; central-moment collision;
-//                             per-item layer sums of Q1, Q2
-//   pml_means     per scene   layer means of Q1, Q2 (fixed-order sums)
-//   probe         per scene   RPIM probe of rho at the start of the step
+//   macro_pml     all nodes   rho, u; PML trapezoid integrals Q1, Q2, the
+//                             local absorption term and the layer field rows
+//                             phi; central-moment collision; per-item layer
+//                             sums of Q1, Q2
+//   scene_tail    per scene   layer means of Q1, Q2 (fixed-order sums); RPIM
+//                             probe of rho at the start of the step; step
+//                             counter
 //   pml_gather    layer-adjacent bulk+layer nodes: the two PML divergence
 //                             gathers div(-2 c sigma (Q1 - <Q1>)) and
 //                             div(c sigma^2 (Q2 - <Q2>))
@@ -18,7 +20,6 @@
 //   filter        all nodes   selective Gaussian filter; bounce-back
 //   rk(1..4)      bulk+layer  streaming gather + RK4 stage update
 //   edge_interp   boundary    RPIM boundary interpolation of the result
-//   step_end      per scene   step counter
 //
 // Arithmetic is FP32 on centred populations g = f - w and rho - 1: the
 // reference keeps f itself in FP32 (T = float), which quantises a 1e-4
@@ -520,30 +521,31 @@ __global__ void __launch_bounds__(kBlock, 4) k_macro_pml(const WorkItem* __restr
     NAGA_END_ITEMS
 }
 
-// layer means of Q1 and Q2 per scene (the reductions of
-// pml_absorption.inl:776-836); block (scene, slot), summed in item order
-// strided over the block, then a fixed tree
+// Per-scene tail of the node-local pass, one launch for all scenes:
+// blocks (scene, t < 2 QP) reduce the layer means of Q1 and Q2 (the
+// reductions of pml_absorption.inl:776-836; item partials summed in item
+// order strided over the block, then a fixed tree); block (scene, 2 QP)
+// samples the probe densities rho - rho0 from the RPIM probe weights
+// (simulation_observers/density_observer.cuh:99-113) into the ring slot of
+// the current step and then advances the scene's step counter (no later
+// kernel of the step reads it).
 template <int QP>
-__global__ void k_pml_means(const SceneDev* __restrict__ scenes) {
+__global__ void __launch_bounds__(256) k_scene_tail(const SceneDev* __restrict__ scenes) {
     __shared__ double red[256];
     const SceneDev& S = scenes[blockIdx.x];
     const int t = blockIdx.y;
-    double acc = 0.0;
-    for (int it = threadIdx.x; it < S.n_all_items; it += blockDim.x) acc += S.partials[(int64_t)it * 2 * QP + t];
-    red[threadIdx.x] = acc;
-    __syncthreads();
-    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-        if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    if (t < 2 * QP) {
+        double acc = 0.0;
+        for (int it = threadIdx.x; it < S.n_all_items; it += blockDim.x) acc += S.partials[(int64_t)it * 2 * QP + t];
+        red[threadIdx.x] = acc;
         __syncthreads();
+        for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+            if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) S.means[t] = S.nl > 0 ? (float)red[0] / (float)S.nl : 0.f;
+        return;
     }
-    if (threadIdx.x == 0) S.means[t] = S.nl > 0 ? (float)red[0] / (float)S.nl : 0.f;
-}
-
-// probe densities (rho - rho0) from the RPIM probe weights
-// (simulation_observers/density_observer.cuh:99-113)
-__global__ void k_probe(const SceneDev* __restrict__ scenes) {
-    const SceneDev& S = scenes[blockIdx.x];
-    if (S.np == 0) return;
     const unsigned long long step = *S.step;
     const int slot = (int)(step % (unsigned long long)S.probe_cap);
     for (int p = threadIdx.x >> 5; p < S.np; p += blockDim.x >> 5) {
@@ -555,6 +557,8 @@ __global__ void k_probe(const SceneDev* __restrict__ scenes) {
         v = warp_sum(v);
         if (lane_id() == 0) S.probe_ring[(int64_t)slot * S.np + p] = v * S.rho0;
     }
+    __syncthreads();
+    if (threadIdx.x == 0) *S.step = step + 1ull;
 }
 
 // Multi-thread-per-node kernels: one work item = one pass of <= NPB
@@ -871,6 +875,13 @@ __global__ void __launch_bounds__(kBlockMT) k_filter(const WorkItem* __restrict_
             out = f;
         }
         st4(S.G, i, QP, c, out);
+        if (i >= S.nbl) {
+            // boundary and ghost rows keep their values through the RK
+            // stages: the stage buffers carry them so the gathers read
+            // every support from one array
+            st4(S.G1, i, QP, c, out);
+            st4(S.G2, i, QP, c, out);
+        }
     }
     NAGA_PIPE_END
 }
@@ -878,7 +889,8 @@ __global__ void __launch_bounds__(kBlockMT) k_filter(const WorkItem* __restrict_
 // RK4 stage STAGE (detail/rk4_solver.cuh:48-171) with the streaming rates
 // rate_a(i) = -sum_s (c_a . W_s) g_a(j_s) (pde_right_hand_side.cuh:82-176,
 // divergence.cuh:377-488). Boundary and ghost nodes keep zero rates, so
-// their stage values equal the step's start values (read from G).
+// their stage values equal the step's start values, which the filter kernel
+// also wrote into the stage buffers G1 and G2.
 template <class L, int K, int STAGE>
 __global__ void __launch_bounds__(kBlockMT) k_rk(const WorkItem* __restrict__ items, int nitems,
                                                  const SceneDev* __restrict__ scenes) {
@@ -901,7 +913,7 @@ __global__ void __launch_bounds__(kBlockMT) k_rk(const WorkItem* __restrict__ it
             const float4 rec = tile[s * nn + ns];
             const uint32_t j = __float_as_uint(rec.w);
             const float wz = L::D == 3 ? rec.z : 0.f;
-            const float4 v = ld4((int64_t)j < S.nbl ? src : S.G, j, QP, c);
+            const float4 v = ld4(src, j, QP, c);
             const float p0 = d0[0] * rec.x + d0[1] * rec.y + d0[2] * wz;
             const float p1 = d1[0] * rec.x + d1[1] * rec.y + d1[2] * wz;
             r.x = fmaf(p0, v.x, r.x);
@@ -957,18 +969,12 @@ __global__ void __launch_bounds__(kBlockMT) k_edge_interp(const WorkItem* __rest
     NAGA_PIPE_END
 }
 
-__global__ void k_step_end(const SceneDev* __restrict__ scenes, int nscenes) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s < nscenes) *scenes[s].step += 1ull;
-}
-
 }  // namespace
 
 // ------------------------------------------------------------- launches
 enum {
     K_MACRO = 0,
-    K_MEANS,
-    K_PROBE,
+    K_TAIL,
     K_PML,
     K_EDGE_COLLIDE,
     K_FILTER,
@@ -977,14 +983,13 @@ enum {
     K_RK3,
     K_RK4,
     K_EDGE_INTERP,
-    K_STEP_END,
     K_COUNT
 };
 
 const char* kernel_name(int id) {
-    static const char* names[K_COUNT] = {"macro_pml", "pml_means", "probe", "pml_gather", "edge_collide", "filter",
-                                         "rk_stage1", "rk_stage2", "rk_stage3", "rk_stage4", "edge_interp",
-                                         "step_end"};
+    static const char* names[K_COUNT] = {"macro_pml",    "means_probe", "pml_gather", "edge_collide",
+                                         "filter",       "rk_stage1",   "rk_stage2",  "rk_stage3",
+                                         "rk_stage4",    "edge_interp"};
     return (id >= 0 && id < K_COUNT) ? names[id] : "?";
 }
 int kernel_count() { return K_COUNT; }
@@ -1031,17 +1036,18 @@ namespace {
 // rest state plus a density perturbation: g = f - w = w drho (u = 0)
 template <class L>
 __global__ void density_rows_kernel(const float* __restrict__ drho, int64_t n, float* __restrict__ G) {
-    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= n * L::QP) return;
-    const int64_t i = e / L::QP;
-    const int a = L::row((int)(e - i * L::QP));
-    G[e] = (a < 0 || !drho) ? 0.f : LatticeTables<L>::w(a) * drho[i];
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float d = drho ? drho[i] : 0.f;
+    float v[L::QP];
+#pragma unroll
+    for (int t = 0; t < L::QP; ++t) v[t] = L::row(t) < 0 ? 0.f : LatticeTables<L>::w(L::row(t)) * d;
+    store_row<L>(G, i, v);
 }
 }  // namespace
 
 int density_rows_device(int dim, const float* drho, int64_t n, float* G, cudaStream_t st) {
-    const int QP = dim == 2 ? D2Q9::QP : D3Q27::QP;
-    const unsigned blocks = (unsigned)((n * QP + 255) / 256);
+    const unsigned blocks = (unsigned)((n + 255) / 256);
     if (blocks == 0) return NAGA_OK;
     if (dim == 2)
         density_rows_kernel<D2Q9><<<blocks, 256, 0, st>>>(drho, n, G);
@@ -1205,8 +1211,7 @@ int enqueue_step_k(const StepLaunch& P, cudaStream_t st) {
         if (prof) prof_end(id, st);             \
     }
     LAUNCH(K_MACRO, P.n_all, (k_macro_pml<L><<<grid(P.n_all), kBlock, 0, st>>>(P.all, P.n_all, P.scenes)));
-    LAUNCH(K_MEANS, P.nscenes, (k_pml_means<L::QP><<<dim3(P.nscenes, 2 * L::QP), 256, 0, st>>>(P.scenes)));
-    LAUNCH(K_PROBE, P.nscenes, (k_probe<<<P.nscenes, 128, 0, st>>>(P.scenes)));
+    LAUNCH(K_TAIL, P.nscenes, (k_scene_tail<L::QP><<<dim3(P.nscenes, 2 * L::QP + 1), 256, 0, st>>>(P.scenes)));
     LAUNCH(K_PML, P.n_pml, (k_pml_gather<L, K><<<pgrid(k_pml_gather<L, K>, s4, P.n_pml), kBlockMT, s4, st>>>(P.pml, P.n_pml, P.scenes)));
     LAUNCH(K_EDGE_COLLIDE, P.n_edge,
            (k_edge_collide<L, KB><<<pgrid(k_edge_collide<L, KB>, sb, P.n_edge), kBlockMT, sb, st>>>(P.edge, P.n_edge, P.scenes)));
@@ -1218,7 +1223,6 @@ int enqueue_step_k(const StepLaunch& P, cudaStream_t st) {
     LAUNCH(K_RK4, P.n_fluid, (k_rk<L, K, 4><<<pgrid(k_rk<L, K, 4>, s4, P.n_fluid), kBlockMT, s4, st>>>(P.fluid, P.n_fluid, P.scenes)));
     LAUNCH(K_EDGE_INTERP, P.n_edge,
            (k_edge_interp<L, KB><<<pgrid(k_edge_interp<L, KB>, sb, P.n_edge), kBlockMT, sb, st>>>(P.edge, P.n_edge, P.scenes)));
-    LAUNCH(K_STEP_END, P.nscenes, (k_step_end<<<(P.nscenes + 127) / 128, 128, 0, st>>>(P.scenes, P.nscenes)));
 #undef LAUNCH
     NAGA_CUDA_TRY(cudaGetLastError());
     return NAGA_OK;
