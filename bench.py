@@ -59,17 +59,24 @@ def make_scene(naga, cfg, seed=None, width=None, center=None):
     return s, g, drho
 
 
-def batched_scenes(naga, n_scenes=256, lo=2e3, hi=1e5):
-    """256 D2Q9 scenes, point counts log-uniform in [2k, 100k], seeds 100..355,
-    pulse width U(0.03, 0.08), pulse centre U(0.3, 0.7)^2 per scene."""
+def batched_specs(n_scenes=256, lo=2e3, hi=1e5):
+    """The batched 2-D workload: n_scenes D2Q9 scenes, point counts
+    log-uniform in [2k, 100k] (jittered grids, seeds 100..), pulse width
+    U(0.03, 0.08) and centre U(0.3, 0.7)^2 per scene. Returns per scene
+    (grid side, seed, width, centre)."""
     out = []
     for t in range(n_scenes):
         rng = np.random.default_rng(100 + t)
         n = float(np.exp(rng.uniform(np.log(lo), np.log(hi))))
         n_side = max(24, int(round(np.sqrt(n))))
-        cfg = dict(CONFIG2, n_side=n_side, seed=100 + t)
-        s, g, _ = make_scene(naga, cfg, width=float(rng.uniform(0.03, 0.08)),
-                             center=list(rng.uniform(0.3, 0.7, 2)))
+        out.append((n_side, 100 + t, float(rng.uniform(0.03, 0.08)), list(rng.uniform(0.3, 0.7, 2))))
+    return out
+
+
+def build_batched(naga, specs):
+    out = []
+    for n_side, seed, width, center in specs:
+        s, _, _ = make_scene(naga, dict(CONFIG2, n_side=n_side, seed=seed), width=width, center=center)
         out.append(s)
     return out
 
@@ -205,6 +212,152 @@ def cpu_baseline(cfg, max_seconds=20.0):
                       f"OpenMP, {arch or 'generic x86-64'}"}
 
 
+# ------------------------------------------------------------ extra blocks
+def batched_block(naga, torch, args, rank, world, dist, W, K):
+    """256 D2Q9 scenes stepped as one batch (one launch per kernel, CUDA
+    graph), sharded over the ranks by size, against the plain 20,164-node
+    D2Q9 scene stepped alone (one replica per rank)."""
+    from naga_b200 import replicas
+
+    plain2, _, _ = make_scene(naga, CONFIG2)
+    p_ms, _ = time_steps(torch, lambda: plain2.step(1), plain2.stream, W, K)
+    p_ms = replicas.max_over_ranks(p_ms, dist, "cuda")
+    plain_mnups = world * plain2.N * K / (p_ms * 1e-3) / 1e6
+    plain2.close()
+    specs = batched_specs(args.batched_scenes)
+    mine = replicas.shard([sp[0] ** 2 for sp in specs], rank, world)
+    scenes = build_batched(naga, [specs[i] for i in mine])
+    b = naga.Batch(2)
+    for s in scenes:
+        b.add(s)
+    b.prepare()
+    b_ms, b_per = time_steps(torch, lambda: b.step(1), b.stream, W, K)
+    b_ms = replicas.max_over_ranks(b_ms, dist, "cuda")
+    nodes = int(replicas.sum_over_ranks(sum(s.N for s in scenes), dist, "cuda"))
+    p99 = replicas.max_over_ranks(float(np.percentile(b_per, 99)), dist, "cuda")
+    bm = nodes * K / (b_ms * 1e-3) / 1e6
+    b.close()
+    for s in scenes:
+        s.close()
+    return {"scenes": len(specs), "nodes": nodes, "mnups": bm, "plain_2d_mnups": plain_mnups,
+            "ratio_vs_plain": bm / plain_mnups, "p50_step_ms": float(np.percentile(b_per, 50)),
+            "p99_step_ms": p99, "sharding": f"{world} rank(s), size-balanced"}
+
+
+def serving_block(naga, torch, args, rank, world, dist):
+    """The continuous-batching loop on the 3-D serving workload, for a
+    bounded window: requests arrive as a Poisson process (20/s, seeded) with
+    point counts log-uniform in [1e4, 1e6] (jittered unit cubes seeded per
+    request), 2000 steps each, refined-FP32 weights, admitted under a 150 GB
+    device budget; each rank serves the requests the deterministic router
+    gives it. Requests still running at the end of the window count by the
+    steps they took."""
+    from naga_b200 import replicas
+
+    rng = np.random.default_rng(2024)
+    T = args.serving_seconds
+    arrivals, t = [], 0.0
+    while True:
+        t += float(rng.exponential(1 / 20.0))
+        if t >= T:
+            break
+        n = float(np.exp(rng.uniform(np.log(1e4), np.log(1e6))))
+        arrivals.append((t, max(16, int(round(n ** (1 / 3)))), len(arrivals)))
+    router = replicas.Router(world)
+    owner = [router.place(n_side ** 3, 2000) for (_, n_side, _) in arrivals]
+    server = naga.Server(3, memory_budget=150 * 10 ** 9, steps_per_tick=20)
+    probes = np.array(PROBES3, np.float32)
+    nxt, submitted = 0, 0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    while True:
+        el = time.perf_counter() - t0
+        if el >= T:
+            break
+        while nxt < len(arrivals) and arrivals[nxt][0] <= el:
+            at, n_side, seed = arrivals[nxt]
+            if owner[nxt] == rank:
+                g = naga.generate_grid(3, n_side, max(2, n_side // 8), 1000 + seed)
+                drho = naga.gaussian_pulse(g["points"], [0.5] * 3, 1e-3, 0.05)
+                server.submit(g, drho, 2000, k=32, shape=0, weight_precision=1, probes=probes,
+                              probe_capacity=2048)
+                submitted += 1
+            nxt += 1
+        server.tick()
+    torch.cuda.synchronize()
+    st = server.stats()
+    server.close()
+    node_updates = replicas.sum_over_ranks(st["node_updates"], dist, "cuda")
+    busy = replicas.max_over_ranks(st["busy_ms"], dist, "cuda")
+    return {"window_s": T, "arrivals": len(arrivals), "submitted_rank0": submitted,
+            "node_updates": int(node_updates), "mnups_busy": node_updates / max(busy, 1e-9) / 1e3,
+            "mnups_wall": node_updates / T / 1e6,
+            "p50_step_ms": replicas.max_over_ranks(st["p50_step_ms"], dist, "cuda"),
+            "p99_step_ms": replicas.max_over_ranks(st["p99_step_ms"], dist, "cuda"),
+            "ticks_rank0": st["ticks"], "done": st["done"], "active_at_end": st["active"],
+            "queued_at_end": st["queued"], "failed": st["failed"], "peak_bytes_rank0": st["peak_bytes"]}
+
+
+def setup_block(naga, torch, args):
+    """Set-up microbench: exact kNN (k = 32) over 64 clouds with point
+    counts log-uniform in [5k, 200k] (uniform in the unit cube, seed 2) in
+    one batched call; then the inverses of `setup_systems` 36 x 36 augmented
+    r^3 RBF moment matrices (random k = 32 stencils of those clouds, centred
+    and scaled), FP64 LU against FP32 LU with FP64-residual refinement, with
+    the error of each against a CPU FP64 inverse (LAPACK through numpy) on
+    a sample of 512 systems."""
+    rng = np.random.default_rng(2)
+    sizes = np.exp(rng.uniform(np.log(5e3), np.log(2e5), 64)).astype(np.int64)
+    pts = torch.from_numpy(rng.random((int(sizes.sum()), 3)).astype(np.float32)).cuda()
+    off = np.concatenate([[0], np.cumsum(sizes)])
+    naga.knn_clouds(pts, off, 32)  # warm-up at full size (grows the allocation pool)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    idx, _ = naga.knn_clouds(pts, off, 32)
+    e1.record()
+    torch.cuda.synchronize()
+    knn_ms = e0.elapsed_time(e1)
+    # moment matrices of random stencils: centre, scale to unit box, r^3 + [1, x]
+    n = args.setup_systems
+    gen = torch.Generator(device="cuda").manual_seed(3)
+    centre = torch.randint(0, pts.shape[0], (n,), device="cuda", generator=gen)
+    X = pts.double()[idx[centre].long()] - pts.double()[centre][:, None]
+    X /= X.abs().amax(dim=(1, 2), keepdim=True)
+    A = torch.zeros((n, 36, 36), dtype=torch.float64, device="cuda")
+    A[:, :32, :32] = torch.cdist(X, X) ** 3
+    A[:, :32, 32] = 1.0
+    A[:, 32, :32] = 1.0
+    A[:, :32, 33:] = X
+    A[:, 33:, :32] = X.transpose(1, 2)
+    del X
+    torch.cuda.synchronize()
+    out = {"knn_clouds": 64, "knn_points": int(sizes.sum()), "knn_ms": knn_ms,
+           "knn_mqueries_per_s": int(sizes.sum()) / knn_ms / 1e3, "inverse_systems": n}
+    sample = np.random.default_rng(4).choice(n, 512, replace=False)
+    # column-major storage: the inverse of the stored (transposed) matrix is
+    # the transpose of the inverse, so compare in the same storage order
+    ref = np.linalg.inv(A[torch.from_numpy(sample).cuda()].cpu().numpy().transpose(0, 2, 1)).transpose(0, 2, 1)
+    for name, fn in (("f64", lambda: naga.batched_inverse_f64(A)),
+                     ("f32r", lambda: naga.batched_inverse_f32r(A, max_iter=30, rel_tol=1e-14))):
+        fn()
+        torch.cuda.synchronize()
+        e0.record()
+        inv, info = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        got = inv[torch.from_numpy(sample).cuda()].cpu().numpy()
+        err = np.abs(got - ref).max(axis=(1, 2)) / np.abs(ref).max(axis=(1, 2))
+        out[f"inverse_{name}_ms"] = ms
+        out[f"inverse_{name}_gflops"] = 2 * 36 ** 3 * n / (ms * 1e-3) / 1e9
+        out[f"inverse_{name}_max_rel_err"] = float(err.max())
+        out[f"inverse_{name}_flagged"] = int((info != 0).sum().item())
+        del inv, info
+    out["refinement_fallbacks"] = naga.refinement_fallbacks()
+    return out
+
+
 # ------------------------------------------------------------------ arms
 def run_reference(args, rank, world):
     cfg = CONFIG3
@@ -227,6 +380,7 @@ def run_naga(args, rank, world, local_rank):
     import torch
 
     import naga_b200 as naga
+    from naga_b200 import replicas
 
     global CONFIG3
     if args.n_side != CONFIG3["n_side"]:
@@ -253,10 +407,7 @@ def run_naga(args, rank, world, local_rank):
     with ClockSampler(local_rank) as clk:
         total_ms, per = time_steps(torch, lambda: scene.step(1), scene.stream, W, K)
     barrier()
-    if dist:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = replicas.max_over_ranks(total_ms, dist, "cuda")
     value = world * N * K / (total_ms * 1e-3) / 1e6
 
     # ---- end to end through the public API with host buffers: the initial
@@ -276,11 +427,21 @@ def run_naga(args, rank, world, local_rank):
     scene.sync()
     e2e_s = time.perf_counter() - t0
     e2e_trace_ok = bool(np.array_equal(host_probes.numpy(), scene.probes(0, K)))
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = replicas.max_over_ranks(e2e_s, dist, "cuda")
     e2e = world * N * K / e2e_s / 1e6
+
+    # ---- batched form (every rank steps its size-balanced share of the
+    # scenes; time = slowest rank) vs the plain single 2-D scene
+    batched = None
+    if not args.no_batched:
+        batched = batched_block(naga, torch, args, rank, world, dist, W, K)
+    # ---- serving loop and set-up microbench (bounded samples)
+    serving = None
+    if not args.no_serving:
+        serving = serving_block(naga, torch, args, rank, world, dist)
+    setup = None
+    if not args.no_setup and rank == 0:
+        setup = setup_block(naga, torch, args)
 
     if rank != 0:
         if dist:
@@ -299,7 +460,7 @@ def run_naga(args, rank, world, local_rank):
     achieved = kb[top] / (tot / launches * 1e-3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tpath):
+    if os.path.exists(tpath) and args.n_side == 63:
         traffic = json.load(open(tpath)).get(top)
     roof = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": traffic,
@@ -307,28 +468,6 @@ def run_naga(args, rank, world, local_rank):
             "algorithmic_bytes_per_launch": kb[top], "avg_launch_ms": tot / launches,
             "kernel_share": {n: round(prof[n][1] / 5 / step_ms, 4) for n in prof if prof[n][0]}}
     gpu_launches = sum(l for (l, _) in prof.values()) // 5 * K
-
-    # ---- batched form vs plain single scene (D2Q9)
-    batched = None
-    if not args.no_batched:
-        plain2, g2, _ = make_scene(naga, CONFIG2)
-        p_ms, _ = time_steps(torch, lambda: plain2.step(1), plain2.stream, W, K)
-        plain_mnups = plain2.N * K / (p_ms * 1e-3) / 1e6
-        scenes = batched_scenes(naga, args.batched_scenes)
-        b = naga.Batch(2)
-        for s in scenes:
-            b.add(s)
-        nodes = sum(s.N for s in scenes)
-        b_ms, b_per = time_steps(torch, lambda: b.step(1), b.stream, W, K)
-        bm = nodes * K / (b_ms * 1e-3) / 1e6
-        batched = {"scenes": len(scenes), "nodes": nodes, "mnups": bm,
-                   "plain_2d_mnups": plain_mnups, "ratio_vs_plain": bm / plain_mnups,
-                   "p50_step_ms": float(np.percentile(b_per, 50)),
-                   "p99_step_ms": float(np.percentile(b_per, 99))}
-        b.close()
-        for s in scenes:
-            s.close()
-        plain2.close()
 
     cb = None
     if world == 1 and not args.no_cpu_baseline:
@@ -348,6 +487,7 @@ def run_naga(args, rank, world, local_rank):
         "e2e": {"value": e2e, "unit": "MNUPS", "h2d_bytes_per_step": int(N * 4 / K),
                 "d2h_bytes_per_step": 4 * len(cfg["probes"]), "probe_trace_read_back": e2e_trace_ok},
         "gpu_launches": int(gpu_launches), "clocks": clk.summary(), "batched": batched,
+        "serving": serving, "setup": setup,
         "launch_shapes": naga.tuning_report().strip().splitlines(),
     }
     print(json.dumps(line), flush=True)
@@ -365,6 +505,10 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batched-scenes", type=int, default=256)
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serving-seconds", type=float, default=12.0)
+    ap.add_argument("--no-setup", action="store_true")
+    ap.add_argument("--setup-systems", type=int, default=1_000_000)
     ap.add_argument("--n-side", type=int, default=63,
                     help="grid nodes per side of the 3-D scene (63 = the benchmark workload; "
                          "smaller values give profiling cases)")

@@ -257,6 +257,11 @@ int naga_batch_add(naga_batch* batch, naga_scene* scene);
 int naga_batch_remove(naga_batch* batch, naga_scene* scene);
 int naga_batch_size(const naga_batch* batch);
 void* naga_batch_stream(naga_batch* batch);
+/* applies pending membership changes now: rebuilds the work lists, tunes
+ * the launch shape of a new batch shape (naga_tuning_report) and captures
+ * the step graph; naga_batch_step does the same when it is still pending.
+ * Lets a caller keep that one-off work out of a timed window.            */
+int naga_batch_prepare(naga_batch* batch);
 /* enqueue nsteps steps of every member scene (asynchronous)              */
 int naga_batch_step(naga_batch* batch, int nsteps);
 int naga_batch_sync(naga_batch* batch);
@@ -267,8 +272,12 @@ int naga_batch_sync(naga_batch* batch);
  * steps_per_tick steps as one batch while queued requests that fit the
  * device-memory budget and the slot limit are set up on their own streams,
  * then retires finished requests (their probe traces kept on the host) and
- * admits the new ones into the batch. No reference counterpart: NAGA steps
- * one engine at a time (simulation_engine.cuh:76).                        */
+ * admits the new ones into the batch. Set-ups in one tick stop once their
+ * host time exceeds the previous tick's step time (at least one per tick),
+ * so a burst of arrivals does not stall the running scenes. Batch changes
+ * (naga_batch_prepare) happen before the timed steps of a tick, so the
+ * latency samples are the steps themselves. No reference counterpart: NAGA
+ * steps one engine at a time (simulation_engine.cuh:76).                  */
 typedef struct naga_server naga_server;
 
 typedef struct naga_server_config {

@@ -99,6 +99,7 @@ _SIGS = {
     "naga_batch_size": ([C.c_void_p], C.c_int),
     "naga_batch_stream": ([C.c_void_p], C.c_void_p),
     "naga_batch_step": ([C.c_void_p, C.c_int], C.c_int),
+    "naga_batch_prepare": ([C.c_void_p], C.c_int),
     "naga_batch_sync": ([C.c_void_p], C.c_int),
     "naga_scene_estimate_bytes": ([C.c_void_p], C.c_int64),
     "naga_server_create": ([C.c_void_p, C.c_void_p], C.c_int),
@@ -303,6 +304,10 @@ class Batch:
     def remove(self, s: Scene):
         _check(lib().naga_batch_remove(self.h, s.h))
         self.scenes.remove(s)
+
+    def prepare(self):
+        """Apply membership changes now (rebuild, shape tuning, graph capture)."""
+        _check(lib().naga_batch_prepare(self.h))
 
     def step(self, n: int = 1):
         _check(lib().naga_batch_step(self.h, n))

@@ -143,6 +143,23 @@ struct naga_batch {
     }
 };
 
+// flag[w] = 1 when a node of item w has a stencil support in the layer
+// [nb, nb + nl) (idx: node-major [n][k] kNN indices)
+__global__ void layer_touch_kernel(const uint32_t* __restrict__ idx, int k, const WorkItem* __restrict__ items,
+                                   int nitems, int64_t nb, int64_t nl, uint8_t* __restrict__ flag) {
+    const int w = blockIdx.x;
+    if (w >= nitems) return;
+    const WorkItem it = items[w];
+    const int64_t n = (int64_t)(it.end - it.begin) * k;
+    int touch = 0;
+    for (int64_t e = threadIdx.x; e < n && !touch; e += blockDim.x) {
+        const int64_t j = idx[(int64_t)it.begin * k + e];
+        touch = j >= nb && j < nb + nl;
+    }
+    touch = __syncthreads_or(touch);
+    if (threadIdx.x == 0) flag[w] = (uint8_t)touch;
+}
+
 namespace {
 
 cudaStream_t active_stream(naga_scene* s) { return s->owner ? s->owner->stream : s->stream; }
@@ -396,19 +413,25 @@ int scene_setup(naga_scene* s) {
     make_items(s->nbl, s->nbl + s->nbd, s->items_edge, npb);
     // bulk/layer items with at least one stencil support in the layer
     s->items_pml.clear();
-    if (s->nl > 0) {
-        std::vector<uint32_t> hidx((size_t)s->nd * k);
-        NAGA_CUDA_TRY(cudaMemcpyAsync(hidx.data(), knn_idx, sizeof(uint32_t) * hidx.size(), cudaMemcpyDeviceToHost, st));
-        NAGA_CUDA_TRY(cudaStreamSynchronize(st));
-        for (const WorkItem& it : s->items_fluid) {
-            bool touch = false;
-            for (uint32_t i = it.begin; i < it.end && !touch; ++i)
-                for (int t = 0; t < k && !touch; ++t) {
-                    const int64_t j = hidx[(size_t)i * k + t];
-                    touch = j >= s->nb && j < s->nb + s->nl;
-                }
-            if (touch) s->items_pml.push_back(it);
+    if (s->nl > 0 && !s->items_fluid.empty()) {
+        const int nf = (int)s->items_fluid.size();
+        WorkItem* ditems = nullptr;
+        uint8_t* dflag = nullptr;
+        NAGA_CUDA_TRY(cudaMallocAsync(&ditems, sizeof(WorkItem) * nf, st));
+        NAGA_CUDA_TRY(cudaMallocAsync(&dflag, nf, st));
+        std::vector<uint8_t> flag(nf, 0);
+        cudaError_t e = cudaMemcpyAsync(ditems, s->items_fluid.data(), sizeof(WorkItem) * nf, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) {
+            layer_touch_kernel<<<nf, 256, 0, st>>>(knn_idx, k, ditems, nf, s->nb, s->nl, dflag);
+            e = cudaGetLastError();
         }
+        if (e == cudaSuccess) e = cudaMemcpyAsync(flag.data(), dflag, nf, cudaMemcpyDeviceToHost, st);
+        cudaFreeAsync(ditems, st);
+        cudaFreeAsync(dflag, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return set_error(NAGA_ECUDA, std::string("layer items: ") + cudaGetErrorString(e));
+        for (int w = 0; w < nf; ++w)
+            if (flag[w]) s->items_pml.push_back(s->items_fluid[w]);
     }
     V.n_all_items = (int)s->items_all.size();
     double* partials = nullptr;
@@ -501,30 +524,41 @@ StepLaunch launch_of(naga_batch* b) {
     return P;
 }
 
-int batch_step(naga_batch* b, int nsteps) {
-    if (nsteps < 0) return set_error(NAGA_EINVAL, "step: negative step count");
-    if (b->members.empty() || nsteps == 0) return NAGA_OK;
+// rebuilds the batch's item lists after a membership change, tunes the
+// launch shape of a new batch shape and captures the step graph, so that
+// the next batch_step only launches
+int batch_prepare(naga_batch* b) {
+    if (b->members.empty()) return NAGA_OK;
     int rc;
     if (b->dirty && (rc = batch_rebuild(b))) return rc;
     StepLaunch P = launch_of(b);
     if (!b->exec && (rc = tune_step_shapes(b->dim, b->k, b->kb, P, b->stream))) return rc;
+    if (!b->exec && !prof_on()) {
+        NAGA_CUDA_TRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        rc = enqueue_step(b->dim, b->k, b->kb, P, b->stream);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+        if (rc) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (e != cudaSuccess) return set_error(NAGA_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+        b->graph = g;
+        NAGA_CUDA_TRY(cudaGraphInstantiate(&b->exec, g, 0));
+    }
+    return NAGA_OK;
+}
+
+int batch_step(naga_batch* b, int nsteps) {
+    if (nsteps < 0) return set_error(NAGA_EINVAL, "step: negative step count");
+    if (b->members.empty() || nsteps == 0) return NAGA_OK;
+    int rc;
+    if ((rc = batch_prepare(b))) return rc;
+    StepLaunch P = launch_of(b);
     if (prof_on()) {
         for (int n = 0; n < nsteps; ++n)
             if ((rc = enqueue_step(b->dim, b->k, b->kb, P, b->stream))) return rc;
     } else {
-        if (!b->exec) {
-            NAGA_CUDA_TRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-            rc = enqueue_step(b->dim, b->k, b->kb, P, b->stream);
-            cudaGraph_t g = nullptr;
-            cudaError_t e = cudaStreamEndCapture(b->stream, &g);
-            if (rc) {
-                if (g) cudaGraphDestroy(g);
-                return rc;
-            }
-            if (e != cudaSuccess) return set_error(NAGA_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
-            b->graph = g;
-            NAGA_CUDA_TRY(cudaGraphInstantiate(&b->exec, g, 0));
-        }
         for (int n = 0; n < nsteps; ++n) NAGA_CUDA_TRY(cudaGraphLaunch(b->exec, b->stream));
     }
     for (auto* s : b->members) s->steps += nsteps;
@@ -839,6 +873,11 @@ extern "C" int naga_batch_remove(naga_batch* b, naga_scene* s) {
 
 extern "C" int naga_batch_size(const naga_batch* b) { return b ? (int)b->members.size() : 0; }
 extern "C" void* naga_batch_stream(naga_batch* b) { return b ? (void*)b->stream : nullptr; }
+
+extern "C" int naga_batch_prepare(naga_batch* b) {
+    if (!b) return set_error(NAGA_EINVAL, "naga_batch_prepare: null batch");
+    return batch_prepare(b);
+}
 
 extern "C" int naga_batch_step(naga_batch* b, int nsteps) {
     if (!b) return set_error(NAGA_EINVAL, "naga_batch_step: null batch");

@@ -12,44 +12,60 @@
 // normal (ranges/uniform_grid.cuh:255-293) negated to point inward.
 //
 // Node order within each class is Morton order of the grid indices, which
-// keeps stencil neighbours close in memory for the GPU gathers.
+// keeps stencil neighbours close in memory for the GPU gathers. The per-node
+// loops run on all host threads; the result does not depend on their number.
 #include "naga_b200.h"
 #include "naga_internal.hpp"
 
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 namespace naga {
 
 namespace {
 
-inline uint64_t splitmix64(uint64_t& s) {
-    uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+// splitmix64: draw k (0-based) of the stream seeded with `seed` is the mix
+// of seed + (k + 1) * gamma, so any draw can be computed directly
+inline uint64_t splitmix64_at(uint64_t seed, uint64_t k) {
+    uint64_t z = seed + (k + 1) * 0x9E3779B97F4A7C15ull;
     z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
     z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
     return z ^ (z >> 31);
 }
-inline double uniform01(uint64_t& s) { return (double)(splitmix64(s) >> 11) * (1.0 / 9007199254740992.0); }
-
-inline uint64_t spread_bits3(uint64_t v) {
-    v &= 0x1fffff;
-    v = (v | v << 32) & 0x1f00000000ffffull;
-    v = (v | v << 16) & 0x1f0000ff0000ffull;
-    v = (v | v << 8) & 0x100f00f00f00f00full;
-    v = (v | v << 4) & 0x10c30c30c30c30c3ull;
-    v = (v | v << 2) & 0x1249249249249249ull;
-    return v;
+inline double uniform01_at(uint64_t seed, uint64_t k) {
+    return (double)(splitmix64_at(seed, k) >> 11) * (1.0 / 9007199254740992.0);
 }
-inline uint64_t spread_bits2(uint64_t v) {
-    v &= 0xffffffff;
-    v = (v | v << 16) & 0x0000ffff0000ffffull;
-    v = (v | v << 8) & 0x00ff00ff00ff00ffull;
-    v = (v | v << 4) & 0x0f0f0f0f0f0f0f0full;
-    v = (v | v << 2) & 0x3333333333333333ull;
-    v = (v | v << 1) & 0x5555555555555555ull;
-    return v;
+
+// fn(begin, end) over [0, n) in contiguous chunks on the host's threads
+template <class Fn>
+void parallel_for(int64_t n, Fn fn) {
+    const int64_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const int64_t nt = std::max<int64_t>(1, std::min<int64_t>(hw, n / 16384));
+    if (nt == 1) {
+        fn((int64_t)0, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (int64_t t = 0; t < nt; ++t) th.emplace_back(fn, n * t / nt, n * (t + 1) / nt);
+    for (auto& x : th) x.join();
+}
+
+// row-major grid indices of the n1^dim grid in increasing Morton order
+// (interleaved bits, x lowest), by walking the octants (quadrants) in order
+void morton_walk(int dim, int64_t n1, int64_t x0, int64_t y0, int64_t z0, int64_t size,
+                 std::vector<int64_t>& out) {
+    if (x0 >= n1 || y0 >= n1 || z0 >= n1) return;
+    if (size == 1) {
+        out.push_back(x0 + n1 * (y0 + n1 * z0));
+        return;
+    }
+    const int64_t hs = size / 2;
+    const int nc = dim == 3 ? 8 : 4;
+    for (int c = 0; c < nc; ++c)
+        morton_walk(dim, n1, x0 + (c & 1) * hs, y0 + ((c >> 1) & 1) * hs, z0 + ((c >> 2) & 1) * hs, hs, out);
 }
 
 // squared distance with the highest dimension added last, FP32
@@ -61,11 +77,6 @@ inline float d2_ref(const float* a, const float* b, int dim) {
     }
     return s;
 }
-
-struct GridNode {
-    uint64_t morton;
-    int64_t lin;  // row-major grid index
-};
 
 }  // namespace
 
@@ -82,75 +93,77 @@ int build_grid_scene(const naga_grid_spec& sp, GridScene& out) {
     out.h = h;
 
     // positions in row-major order (x fastest); every node draws `dim`
-    // uniforms so the stream does not depend on the node's class
+    // uniforms (draws n dim + d of the seed's stream), so the stream does not
+    // depend on the node's class
     std::vector<float> pos((size_t)total * dim);
     std::vector<char> is_bnd(total, 0);
-    uint64_t state = sp.seed;
-    for (int64_t n = 0; n < total; ++n) {
-        int64_t g[3] = {n % n1, (n / n1) % n1, dim == 3 ? n / (n1 * n1) : 0};
-        bool bnd = false;
-        for (int d = 0; d < dim; ++d) bnd = bnd || g[d] == 0 || g[d] == n1 - 1;
-        is_bnd[n] = bnd;
-        for (int d = 0; d < dim; ++d) {
-            double u = uniform01(state);
-            double x = (double)g[d] * h;
-            if (!bnd) x += (2.0 * u - 1.0) * sp.jitter * h;
-            pos[(size_t)n * dim + d] = (float)x;
+    const uint64_t seed = sp.seed;
+    parallel_for(total, [&](int64_t b0, int64_t b1) {
+        for (int64_t n = b0; n < b1; ++n) {
+            int64_t g[3] = {n % n1, (n / n1) % n1, dim == 3 ? n / (n1 * n1) : 0};
+            bool bnd = false;
+            for (int d = 0; d < dim; ++d) bnd = bnd || g[d] == 0 || g[d] == n1 - 1;
+            is_bnd[n] = bnd;
+            for (int d = 0; d < dim; ++d) {
+                double u = uniform01_at(seed, (uint64_t)n * dim + d);
+                double x = (double)g[d] * h;
+                if (!bnd) x += (2.0 * u - 1.0) * sp.jitter * h;
+                pos[(size_t)n * dim + d] = (float)x;
+            }
         }
-    }
+    });
 
     // nearest boundary node: the boundary nodes of each wall form a regular
     // grid, so the nearest one on a wall is found by rounding the in-wall
     // coordinates (neighbours +-1 are checked to stay exact in FP32)
     const float Lt = (float)sp.n_layers * (float)h;
     std::vector<float> dist2(total, INFINITY);
-    for (int64_t n = 0; n < total; ++n) {
-        if (is_bnd[n]) continue;
-        const float* p = &pos[(size_t)n * dim];
-        float best = INFINITY;
-        for (int wd = 0; wd < dim; ++wd)
-            for (int side = 0; side < 2; ++side) {
-                int64_t base[3];
-                for (int d = 0; d < dim; ++d)
-                    base[d] = std::min<int64_t>(std::max<int64_t>(std::llround((double)p[d] / h), 0), n1 - 1);
-                base[wd] = side ? n1 - 1 : 0;
-                int64_t lo0 = -1, hi0 = 1;
-                for (int64_t a = lo0; a <= hi0; ++a)
-                    for (int64_t b = (dim == 3 ? lo0 : 0); b <= (dim == 3 ? hi0 : 0); ++b) {
-                        int64_t g[3] = {base[0], base[1], base[2]};
-                        int od[2], c = 0;
-                        for (int d = 0; d < dim; ++d)
-                            if (d != wd) od[c++] = d;
-                        g[od[0]] += a;
-                        if (dim == 3) g[od[1]] += b;
-                        bool ok = true;
-                        for (int d = 0; d < dim; ++d) ok = ok && g[d] >= 0 && g[d] < n1;
-                        if (!ok) continue;
-                        float q[3];
-                        for (int d = 0; d < dim; ++d) q[d] = (float)((double)g[d] * h);
-                        best = std::min(best, d2_ref(p, q, dim));
-                    }
-            }
-        dist2[n] = best;
-    }
+    parallel_for(total, [&](int64_t b0, int64_t b1) {
+        for (int64_t n = b0; n < b1; ++n) {
+            if (is_bnd[n]) continue;
+            const float* p = &pos[(size_t)n * dim];
+            float best = INFINITY;
+            for (int wd = 0; wd < dim; ++wd)
+                for (int side = 0; side < 2; ++side) {
+                    int64_t base[3];
+                    for (int d = 0; d < dim; ++d)
+                        base[d] = std::min<int64_t>(std::max<int64_t>(std::llround((double)p[d] / h), 0), n1 - 1);
+                    base[wd] = side ? n1 - 1 : 0;
+                    for (int64_t a = -1; a <= 1; ++a)
+                        for (int64_t b = (dim == 3 ? -1 : 0); b <= (dim == 3 ? 1 : 0); ++b) {
+                            int64_t g[3] = {base[0], base[1], base[2]};
+                            int od[2], c = 0;
+                            for (int d = 0; d < dim; ++d)
+                                if (d != wd) od[c++] = d;
+                            g[od[0]] += a;
+                            if (dim == 3) g[od[1]] += b;
+                            bool ok = true;
+                            for (int d = 0; d < dim; ++d) ok = ok && g[d] >= 0 && g[d] < n1;
+                            if (!ok) continue;
+                            float q[3];
+                            for (int d = 0; d < dim; ++d) q[d] = (float)((double)g[d] * h);
+                            best = std::min(best, d2_ref(p, q, dim));
+                        }
+                }
+            dist2[n] = best;
+        }
+    });
 
-    std::vector<GridNode> bulk, layer, bnd;
-    for (int64_t n = 0; n < total; ++n) {
-        int64_t g[3] = {n % n1, (n / n1) % n1, dim == 3 ? n / (n1 * n1) : 0};
-        uint64_t m = dim == 3 ? (spread_bits3(g[0]) | spread_bits3(g[1]) << 1 | spread_bits3(g[2]) << 2)
-                              : (spread_bits2(g[0]) | spread_bits2(g[1]) << 1);
-        GridNode gn{m, n};
+    // classes in Morton order of the grid indices
+    std::vector<int64_t> order;
+    order.reserve((size_t)total);
+    int64_t size = 1;
+    while (size < n1) size *= 2;
+    morton_walk(dim, n1, 0, 0, 0, size, order);
+    std::vector<int64_t> bulk, layer, bnd;  // row-major grid indices
+    for (int64_t n : order) {
         if (is_bnd[n])
-            bnd.push_back(gn);
+            bnd.push_back(n);
         else if (sp.n_layers > 0 && dist2[n] <= Lt * Lt)
-            layer.push_back(gn);
+            layer.push_back(n);
         else
-            bulk.push_back(gn);
+            bulk.push_back(n);
     }
-    auto by_morton = [](const GridNode& a, const GridNode& b) { return a.morton < b.morton; };
-    std::sort(bulk.begin(), bulk.end(), by_morton);
-    std::sort(layer.begin(), layer.end(), by_morton);
-    std::sort(bnd.begin(), bnd.end(), by_morton);
 
     out.n_bulk = (int64_t)bulk.size();
     out.n_layer = (int64_t)layer.size();
@@ -160,20 +173,20 @@ int build_grid_scene(const naga_grid_spec& sp, GridScene& out) {
     out.sigma.resize((size_t)out.n_layer);
     out.grid_index.resize((size_t)total);
     int64_t w = 0;
-    auto emit = [&](const GridNode& gn) {
-        std::memcpy(&out.points[(size_t)w * dim], &pos[(size_t)gn.lin * dim], sizeof(float) * dim);
-        out.grid_index[w] = gn.lin;
+    auto emit = [&](int64_t lin) {
+        std::memcpy(&out.points[(size_t)w * dim], &pos[(size_t)lin * dim], sizeof(float) * dim);
+        out.grid_index[w] = lin;
         ++w;
     };
-    for (auto& gn : bulk) emit(gn);
+    for (int64_t n : bulk) emit(n);
     for (size_t t = 0; t < layer.size(); ++t) {
-        float d = std::sqrt(dist2[layer[t].lin]);
+        float d = std::sqrt(dist2[layer[t]]);
         float r = (Lt - d) / Lt;
         out.sigma[t] = (float)sp.sigma_peak * (r * r);
         emit(layer[t]);
     }
     for (size_t t = 0; t < bnd.size(); ++t) {
-        int64_t n = bnd[t].lin;
+        int64_t n = bnd[t];
         int64_t g[3] = {n % n1, (n / n1) % n1, dim == 3 ? n / (n1 * n1) : 0};
         float nv[3] = {0, 0, 0};
         for (int d = 0; d < dim; ++d) nv[d] = g[d] == 0 ? -1.f : (g[d] == n1 - 1 ? 1.f : 0.f);
@@ -190,12 +203,43 @@ int build_grid_scene(const naga_grid_spec& sp, GridScene& out) {
 
 using namespace naga;
 
+namespace {
+// the last grid built on this thread: the usual call pair (counts to size
+// the buffers, then generate) builds it once
+struct GridCache {
+    bool valid = false;
+    naga_grid_spec spec{};
+    GridScene scene;
+};
+thread_local GridCache g_grid_cache;
+
+bool same_spec(const naga_grid_spec& a, const naga_grid_spec& b) {
+    return a.dim == b.dim && a.n_layers == b.n_layers && a.n_side == b.n_side && a.jitter == b.jitter &&
+           a.sigma_peak == b.sigma_peak && a.seed == b.seed;
+}
+
+int cached_grid(const naga_grid_spec& spec, const GridScene** out) {
+    GridCache& c = g_grid_cache;
+    if (!c.valid || !same_spec(c.spec, spec)) {
+        c.valid = false;
+        c.scene = GridScene{};
+        int rc = build_grid_scene(spec, c.scene);
+        if (rc) return rc;
+        c.spec = spec;
+        c.valid = true;
+    }
+    *out = &c.scene;
+    return NAGA_OK;
+}
+}  // namespace
+
 extern "C" int naga_grid_counts(const naga_grid_spec* spec, int64_t* n_bulk, int64_t* n_layer,
                                 int64_t* n_boundary) {
     if (!spec) return set_error(NAGA_EINVAL, "naga_grid_counts: null spec");
-    GridScene s;
-    int rc = build_grid_scene(*spec, s);
+    const GridScene* sp = nullptr;
+    int rc = cached_grid(*spec, &sp);
     if (rc) return set_error(rc, "naga_grid_counts: invalid grid spec");
+    const GridScene& s = *sp;
     if (n_bulk) *n_bulk = s.n_bulk;
     if (n_layer) *n_layer = s.n_layer;
     if (n_boundary) *n_boundary = s.n_boundary;
@@ -205,9 +249,10 @@ extern "C" int naga_grid_counts(const naga_grid_spec* spec, int64_t* n_bulk, int
 extern "C" int naga_grid_generate(const naga_grid_spec* spec, float* points, float* normals,
                                   float* sigma, double* nodal_spacing) {
     if (!spec) return set_error(NAGA_EINVAL, "naga_grid_generate: null spec");
-    GridScene s;
-    int rc = build_grid_scene(*spec, s);
+    const GridScene* sp = nullptr;
+    int rc = cached_grid(*spec, &sp);
     if (rc) return set_error(rc, "naga_grid_generate: invalid grid spec");
+    const GridScene& s = *sp;
     if (points) std::memcpy(points, s.points.data(), s.points.size() * sizeof(float));
     if (normals) std::memcpy(normals, s.normals.data(), s.normals.size() * sizeof(float));
     if (sigma) std::memcpy(sigma, s.sigma.data(), s.sigma.size() * sizeof(float));

@@ -20,6 +20,7 @@
 #include "scene_dev.hpp"
 
 #include <algorithm>
+#include <chrono>
 #include <deque>
 #include <map>
 #include <memory>
@@ -56,6 +57,7 @@ struct naga_server {
     int64_t bytes_in_use = 0, peak_bytes = 0;
     int64_t ticks = 0, steps = 0, node_updates = 0;
     double busy_ms = 0;
+    double last_tick_ms = 0;     // device time of the previous tick's steps
     std::vector<float> step_ms;  // per-step latency samples
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int64_t done = 0, failed = 0;
@@ -176,13 +178,27 @@ extern "C" int naga_server_tick(naga_server* s, int* n_active, int* n_queued) {
     cudaStream_t bst = (cudaStream_t)naga_batch_stream(s->batch);
     int rc;
     if (stepping) {
+        // membership changes (rebuild, first-time shape tuning, graph
+        // capture) happen here, outside the timed window of the steps
+        if ((rc = naga_batch_prepare(s->batch))) return rc;
         NAGA_CUDA_TRY(cudaEventRecord(s->ev0, bst));
         if ((rc = naga_batch_step(s->batch, spt))) return rc;
         NAGA_CUDA_TRY(cudaEventRecord(s->ev1, bst));
     }
-    // 2. admissions, overlapping the batch on the device
+    // 2. admissions, overlapping the batch on the device. Set-up (kNN,
+    // stencil and weight solves) runs on the host thread while the batch
+    // steps; once this tick's set-up time exceeds the device time of the
+    // previous tick's steps the rest waits, so a burst of arrivals does not
+    // stall the running scenes (at least one request is admitted per tick).
     std::vector<int64_t> admitted;
+    const auto t_admit = std::chrono::steady_clock::now();
+    const double admit_budget_ms = std::max(5.0, s->last_tick_ms);
     while (!s->queue.empty()) {
+        if (!admitted.empty() && stepping) {
+            const double spent =
+                std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_admit).count();
+            if (spent > admit_budget_ms) break;
+        }
         Request& r = *s->reqs[s->queue.front()];
         const int slots_used = (int)(s->active.size() + admitted.size());
         if (s->cfg.max_active > 0 && slots_used >= s->cfg.max_active) break;
@@ -215,6 +231,7 @@ extern "C" int naga_server_tick(naga_server* s, int* n_active, int* n_queued) {
         float ms = 0;
         NAGA_CUDA_TRY(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
         s->busy_ms += ms;
+        s->last_tick_ms = ms;
         for (int t = 0; t < spt; ++t) s->step_ms.push_back(ms / spt);
         s->ticks++;
         s->steps += spt;
