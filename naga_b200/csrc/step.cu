@@ -106,6 +106,25 @@ __device__ __forceinline__ void store_row(float* base, int64_t i, const float* v
 __device__ __forceinline__ float4 ld4(const float* base, int64_t i, int qp, int c) {
     return __ldg(reinterpret_cast<const float4*>(base + i * qp) + c);
 }
+// neighbour-row gathers cached in L2 only (.cg): the rows of a pass's
+// neighbours are re-read by other passes long after L1 would have evicted
+// them, and allocating them in L1 costs more than it saves (D3Q27 RK gather:
+// 85 -> 80 us per 250k-node launch)
+__device__ __forceinline__ float4 ld4cg(const float* base, int64_t i, int qp, int c) {
+    const float4* a = reinterpret_cast<const float4*>(base + i * qp) + c;
+    float4 v;
+    asm volatile("ld.global.cg.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(a));
+    return v;
+}
+// the gather load of a lattice: D3Q27 rows (112 B) bypass L1; D2Q9 rows
+// (48 B, 4.6x more nodes per line) keep the L1 reuse (measured both ways)
+template <class L>
+__device__ __forceinline__ float4 ld4g(const float* base, int64_t i, int c) {
+    if constexpr (L::D == 3)
+        return ld4cg(base, i, L::QP, c);
+    else
+        return __ldg(reinterpret_cast<const float4*>(base + i * L::QP) + c);
+}
 __device__ __forceinline__ float4 ld4rw(const float* base, int64_t i, int qp, int c) {
     return reinterpret_cast<const float4*>(base + i * qp)[c];
 }
@@ -761,7 +780,7 @@ __global__ void __launch_bounds__(kBlockMT) k_pml_gather(const WorkItem* __restr
             const int64_t jl = (int64_t)__float_as_uint(rec.w) - S.nb;
             if (jl < 0 || jl >= S.nl) continue;
             const float wz = L::D == 3 ? rec.z : 0.f;
-            const float4 v = ld4(S.PHI, jl, QP, c);
+            const float4 v = ld4g<L>(S.PHI, jl, c);
             const float p0 = d0[0] * rec.x + d0[1] * rec.y + d0[2] * wz;
             const float p1 = d1[0] * rec.x + d1[1] * rec.y + d1[2] * wz;
             dv.x = fmaf(p0, v.x, dv.x);
@@ -807,7 +826,7 @@ __global__ void __launch_bounds__(kBlockMT) k_edge_collide(const WorkItem* __res
 #pragma unroll 8
         for (int s = 0; s < kb; ++s) {
             const float2 r = tile[s * nn + ns];
-            const float4 v = ld4(S.S1P, __float_as_uint(r.y), QP, c);
+            const float4 v = ld4g<L>(S.S1P, __float_as_uint(r.y), c);
             acc.x = fmaf(r.x, v.x, acc.x);
             acc.y = fmaf(r.x, v.y, acc.y);
             acc.z = fmaf(r.x, v.z, acc.z);
@@ -851,7 +870,7 @@ __global__ void __launch_bounds__(kBlockMT) k_filter(const WorkItem* __restrict_
                     r = rt;
                 else
                     r = make_float2(rt.z, rt.w);
-                const float4 v = ld4rw(S.S1, __float_as_uint(r.y), QP, c);
+                const float4 v = ld4g<L>(S.S1, __float_as_uint(r.y), c);
                 sum.x = fmaf(r.x, v.x - f.x, sum.x);
                 sum.y = fmaf(r.x, v.y - f.y, sum.y);
                 sum.z = fmaf(r.x, v.z - f.z, sum.z);
@@ -908,12 +927,12 @@ __global__ void __launch_bounds__(kBlockMT) k_rk(const WorkItem* __restrict__ it
         const float4 f0 = ld4(S.G, i, QP, c);
         const float4 acc = STAGE == 1 ? make_float4(0.f, 0.f, 0.f, 0.f) : ld4rw(S.ACC, i, QP, c);
         float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll 8
+#pragma unroll 16
         for (int s = 0; s < k; ++s) {
             const float4 rec = tile[s * nn + ns];
             const uint32_t j = __float_as_uint(rec.w);
             const float wz = L::D == 3 ? rec.z : 0.f;
-            const float4 v = ld4(src, j, QP, c);
+            const float4 v = ld4g<L>(src, j, c);
             const float p0 = d0[0] * rec.x + d0[1] * rec.y + d0[2] * wz;
             const float p1 = d1[0] * rec.x + d1[1] * rec.y + d1[2] * wz;
             r.x = fmaf(p0, v.x, r.x);
@@ -958,7 +977,7 @@ __global__ void __launch_bounds__(kBlockMT) k_edge_interp(const WorkItem* __rest
 #pragma unroll 8
         for (int s = 0; s < kb; ++s) {
             const float2 r = tile[s * nn + ns];
-            const float4 v = ld4rw(S.G, __float_as_uint(r.y), QP, c);
+            const float4 v = ld4g<L>(S.G, __float_as_uint(r.y), c);
             acc.x = fmaf(r.x, v.x, acc.x);
             acc.y = fmaf(r.x, v.y, acc.y);
             acc.z = fmaf(r.x, v.z, acc.z);
