@@ -148,7 +148,8 @@ __device__ __forceinline__ void macros(const float* g, float& drho, float* u) {
     }
     const float rho = 1.f + drho;
 #pragma unroll
-    for (int d = 0; d < L::D; ++d) u[d] = m[d] / rho;
+    const float rrho = 1.f / rho;
+    for (int d = 0; d < L::D; ++d) u[d] = m[d] * rrho;
 }
 
 // centred equilibrium feq - w of detail/equilibrium_distribution.cuh:41-64:
@@ -165,7 +166,13 @@ __device__ __forceinline__ float feq_c(int a, float drho, const float* u) {
         uc += (float)T::cz(a) * u[2];
     }
     const float w = T::w(a);
-    return w * drho + w * (1.f + drho) * (uc / cs2 + (uc * uc) / (2.f * cs4) - uu);
+    // 1 / cs^2 and 1 / (2 cs^4) are compile-time constants: multiplications
+    // instead of 2 x 27 IEEE divisions per feq evaluation (rounding differs
+    // from dividing by at most an ulp of each term)
+    constexpr float r_cs2 = (float)(1.0 / ((double)0.57735026918962576451f * 0.57735026918962576451f));
+    constexpr float r_2cs4 = 0.5f * r_cs2 * r_cs2;
+    (void)cs4;
+    return w * drho + w * (1.f + drho) * (uc * r_cs2 + (uc * uc) * r_2cs4 - uu);
 }
 
 // ------------------------------------------------------------- collision
@@ -178,7 +185,7 @@ __device__ __forceinline__ float feq_c(int a, float drho, const float* u) {
 // factor use s (and rho - 1), where the reference's C contributions cancel
 // exactly, all other terms use K.
 __device__ __forceinline__ void mom1(int m, float u, float& a, float& x) {
-    a = (m == 0) ? 1.f : (m == 1 ? 0.f : 1.f / 3.f);
+    a = (m == 0) ? 1.f : (m == 1 ? 0.f : 1.f * (1.f / 3.f));
     x = (m == 0) ? 0.f : (m == 1 ? -u : u * u);
 }
 
@@ -271,19 +278,19 @@ __device__ void collide_d3q27(const float* g, float drho, const float* u, const 
     float k[27];
     k[0] = k[1] = k[2] = k[3] = 0.f;
     float om = S.om_ab;
-    k[4] = om * (-Kxy / 12.f);
-    k[5] = om * (-Kxz / 12.f);
-    k[6] = om * (-Kyz / 12.f);
-    k[7] = om * (-(sxx - syy) / 12.f);
-    k[8] = om * (-(sxx + syy - 2.f * szz) / 36.f);
-    k[9] = om * (-(sxx + syy + szz - drho) / 18.f);
+    k[4] = om * (-Kxy * (1.f / 12.f));
+    k[5] = om * (-Kxz * (1.f / 12.f));
+    k[6] = om * (-Kyz * (1.f / 12.f));
+    k[7] = om * (-(sxx - syy) * (1.f / 12.f));
+    k[8] = om * (-(sxx + syy - 2.f * szz) * (1.f / 36.f));
+    k[9] = om * (-(sxx + syy + szz - drho) * (1.f / 18.f));
     om = S.om_fix[0];
     k[10] = om * (-(6.f * Kxy * v1 + 3.f * Kxyy + 6.f * Kxz * v2 + 3.f * Kxzz + 3.f * Kyy * v0 + 3.f * Kzz * v0 -
-                    2.f * rho * v0) / 72.f);
+                    2.f * rho * v0) * (1.f / 72.f));
     k[11] = om * (-(3.f * Kxx * v1 + 3.f * Kxxy + 6.f * Kxy * v0 + 6.f * Kyz * v2 + 3.f * Kyzz + 3.f * Kzz * v1 -
-                    2.f * rho * v1) / 72.f);
+                    2.f * rho * v1) * (1.f / 72.f));
     k[12] = om * (-(3.f * Kxx * v2 + 3.f * Kxxz + 6.f * Kxz * v0 + 3.f * Kyy * v2 + 3.f * Kyyz + 6.f * Kyz * v1 -
-                    2.f * rho * v2) / 72.f);
+                    2.f * rho * v2) * (1.f / 72.f));
     om = S.om_fix[1];
     k[13] = om * (-(2.f * Kxy * v1 + Kxyy - 2.f * Kxz * v2 - Kxzz + Kyy * v0 - Kzz * v0) / 8.f);
     k[14] = om * (-(Kxx * v1 + Kxxy + 2.f * Kxy * v0 - 2.f * Kyz * v2 - Kyzz - Kzz * v1) / 8.f);
@@ -296,22 +303,22 @@ __device__ void collide_d3q27(const float* g, float drho, const float* u, const 
                     12.f * Kxz * v0 * v2 + 6.f * Kxzz * v0 + 3.f * Kyy * v0sq + 3.f * Kyy * v2sq - 4.f * syy +
                     6.f * Kyyz * v2 + 3.f * syyzz + 12.f * Kyz * v1 * v2 + 6.f * Kyzz * v1 + 3.f * Kzz * v0sq +
                     3.f * Kzz * v1sq - 4.f * szz - 2.f * rho * v0sq - 2.f * rho * v1sq - 2.f * rho * v2sq +
-                    3.f * drho) / 36.f);
+                    3.f * drho) * (1.f / 36.f));
     om = S.om_fix[4];
     k[18] = om * (-(3.f * Kxx * v1sq + 3.f * Kxx * v2sq - 4.f * sxx + 6.f * Kxxy * v1 + 3.f * sxxyy +
                     6.f * Kxxz * v2 + 3.f * sxxzz + 12.f * Kxy * v0 * v1 + 6.f * Kxyy * v0 +
                     12.f * Kxz * v0 * v2 + 6.f * Kxzz * v0 + 3.f * Kyy * v0sq - 6.f * Kyy * v2sq + 2.f * syy -
                     12.f * Kyyz * v2 - 6.f * syyzz - 24.f * Kyz * v1 * v2 - 12.f * Kyzz * v1 + 3.f * Kzz * v0sq -
-                    6.f * Kzz * v1sq + 2.f * szz - 2.f * rho * v0sq + rho * v1sq + rho * v2sq) / 72.f);
+                    6.f * Kzz * v1sq + 2.f * szz - 2.f * rho * v0sq + rho * v1sq + rho * v2sq) * (1.f / 72.f));
     k[19] = om * (-(3.f * Kxx * v1sq - 3.f * Kxx * v2sq + 6.f * Kxxy * v1 + 3.f * sxxyy - 6.f * Kxxz * v2 -
                     3.f * sxxzz + 12.f * Kxy * v0 * v1 + 6.f * Kxyy * v0 - 12.f * Kxz * v0 * v2 -
                     6.f * Kxzz * v0 + 3.f * Kyy * v0sq - 2.f * syy - 3.f * Kzz * v0sq + 2.f * szz - rho * v1sq +
-                    rho * v2sq) / 24.f);
+                    rho * v2sq) * (1.f / 24.f));
     om = S.om_fix[4];
     k[20] = om * (-(3.f * Kxx * v1 * v2 + 3.f * Kxxy * v2 + 3.f * Kxxyz + 3.f * Kxxz * v1 + 6.f * Kxy * v0 * v2 +
-                    6.f * Kxyz * v0 + 6.f * Kxz * v0 * v1 + 3.f * Kyz * v0sq - 2.f * Kyz - rho * v1 * v2) / 24.f);
+                    6.f * Kxyz * v0 + 6.f * Kxz * v0 * v1 + 3.f * Kyz * v0sq - 2.f * Kyz - rho * v1 * v2) * (1.f / 24.f));
     k[21] = om * (-(6.f * Kxy * v1 * v2 + 3.f * Kxyy * v2 + 3.f * Kxyyz + 6.f * Kxyz * v1 + 3.f * Kxz * v1sq -
-                    2.f * Kxz + 3.f * Kyy * v0 * v2 + 3.f * Kyyz * v0 + 6.f * Kyz * v0 * v1 - rho * v0 * v2) / 24.f);
+                    2.f * Kxz + 3.f * Kyy * v0 * v2 + 3.f * Kyyz * v0 + 6.f * Kyz * v0 * v1 - rho * v0 * v2) * (1.f / 24.f));
     k[22] = om * (-(3.f * Kxy * v2sq - 2.f * Kxy + 6.f * Kxyz * v2 + 3.f * Kxyzz + 6.f * Kxz * v1 * v2 +
                     3.f * Kxzz * v1 + 6.f * Kyz * v0 * v2 + 3.f * Kyzz * v0 + 3.f * Kzz * v0 * v1 - rho * v0 * v1) /
                   24.f);
@@ -321,18 +328,18 @@ __device__ void collide_d3q27(const float* g, float drho, const float* u, const 
                     4.f * Kxz * v2 + 3.f * Kxzz * v1sq - 2.f * Kxzz + 3.f * Kyy * v0 * v2sq - 2.f * Kyy * v0 +
                     6.f * K[0][2][1] * v0 * v2 + 3.f * Kyyzz * v0 + 12.f * Kyz * v0 * v1 * v2 +
                     6.f * Kyzz * v0 * v1 + 3.f * Kzz * v0 * v1sq - 2.f * Kzz * v0 - rho * v0 * v1sq -
-                    rho * v0 * v2sq + rho * v0) / 24.f);
+                    rho * v0 * v2sq + rho * v0) * (1.f / 24.f));
     k[24] = om * (-(3.f * Kxx * v1 * v2sq - 2.f * Kxx * v1 + 3.f * Kxxy * v2sq - 2.f * Kxxy + 6.f * Kxxyz * v2 +
                     3.f * Kxxyzz + 6.f * Kxxz * v1 * v2 + 3.f * Kxxzz * v1 + 6.f * Kxy * v0 * v2sq -
                     4.f * Kxy * v0 + 12.f * Kxyz * v0 * v2 + 6.f * Kxyzz * v0 + 12.f * Kxz * v0 * v1 * v2 +
                     6.f * Kxzz * v0 * v1 + 6.f * Kyz * v0sq * v2 - 4.f * Kyz * v2 + 3.f * Kyzz * v0sq -
                     2.f * Kyzz + 3.f * Kzz * v0sq * v1 - 2.f * Kzz * v1 - rho * v0sq * v1 - rho * v1 * v2sq +
-                    rho * v1) / 24.f);
+                    rho * v1) * (1.f / 24.f));
     k[25] = om * (-(3.f * Kxx * v1sq * v2 - 2.f * Kxx * v2 + 6.f * Kxxy * v1 * v2 + 3.f * Kxxyy * v2 +
                     3.f * Kxxyyz + 6.f * Kxxyz * v1 + 3.f * Kxxz * v1sq - 2.f * Kxxz + 12.f * Kxy * v0 * v1 * v2 +
                     6.f * Kxyy * v0 * v2 + 6.f * Kxyyz * v0 + 12.f * Kxyz * v0 * v1 + 6.f * Kxz * v0 * v1sq -
                     4.f * Kxz * v0 + 3.f * Kyy * v0sq * v2 - 2.f * Kyy * v2 + 3.f * Kyyz * v0sq - 2.f * Kyyz +
-                    6.f * Kyz * v0sq * v1 - 4.f * Kyz * v1 - rho * v0sq * v2 - rho * v1sq * v2 + rho * v2) / 24.f);
+                    6.f * Kyz * v0sq * v1 - 4.f * Kyz * v1 - rho * v0sq * v2 - rho * v1sq * v2 + rho * v2) * (1.f / 24.f));
     k[26] = om * (-(27.f * Kxx * v1sq * v2sq - 18.f * Kxx * v1sq - 18.f * Kxx * v2sq + 12.f * sxx +
                     54.f * Kxxy * v1 * v2sq - 36.f * Kxxy * v1 + 27.f * Kxxyy * v2sq - 18.f * sxxyy +
                     54.f * Kxxyyz * v2 + 27.f * sxxyyzz + 108.f * Kxxyz * v1 * v2 + 54.f * Kxxyzz * v1 +
@@ -346,7 +353,7 @@ __device__ void collide_d3q27(const float* g, float drho, const float* u, const 
                     54.f * Kyzz * v0sq * v1 - 36.f * Kyzz * v1 + 27.f * Kzz * v0sq * v1sq - 18.f * Kzz * v0sq -
                     18.f * Kzz * v1sq + 12.f * szz - 9.f * rho * v0sq * v1sq - 9.f * rho * v0sq * v2sq +
                     9.f * rho * v0sq - 9.f * rho * v1sq * v2sq + 9.f * rho * v1sq + 9.f * rho * v2sq -
-                    7.f * drho) / 216.f);
+                    7.f * drho) * (1.f / 216.f));
     // df = K k dt (detail/simulation_engine.cuh:518-527)
 #pragma unroll
     for (int l = 0; l < 27; ++l) {
@@ -369,29 +376,29 @@ __device__ void collide_d2q9(const float* g, float drho, const float* u, const S
     float k[9];
     k[0] = k[1] = k[2] = 0.f;
     k[3] = idt * (rho * (u0 * u0 + u1 * u1) - g[E] - g[N] - g[Sd] - g[W] -
-                  2.f * (g[SE] + g[SW] + g[NE] + g[NW] - drho / 3.f)) / 12.f;
+                  2.f * (g[SE] + g[SW] + g[NE] + g[NW] - drho * (1.f / 3.f))) * (1.f / 12.f);
     k[4] = om * (g[N] + g[Sd] - g[E] - g[W] + rho * (u0 * u0 - u1 * u1)) / 4.f;
     k[5] = om * (g[NE] + g[SW] - g[NW] - g[SE] + rho * (u0 * u1)) / 4.f;
     {
         float t1 = (g[SE] + g[SW] - g[NE] - g[NW] - 2.f * u0 * u0 * u1 * rho +
-                    u1 * (1.f / 3.f + (drho - g[N] - g[Sd] - g[R]))) / 4.f;
+                    u1 * (1.f * (1.f / 3.f) + (drho - g[N] - g[Sd] - g[R]))) / 4.f;
         float t2 = u0 / 2.f * (g[NE] - g[NW] - g[SE] + g[SW]);
         float t3 = -u1 / 2.f * (-3.f * k[3] - k[4]) - 2.f * u0 * k[5];
         k[6] = -idt * (t1 + t2) + t3;
     }
     {
         float t1 = (g[SW] + g[NW] - g[SE] - g[NE] - 2.f * u0 * u1 * u1 * rho +
-                    u0 * (1.f / 3.f + (drho - g[W] - g[E] - g[R]))) / 4.f;
+                    u0 * (1.f * (1.f / 3.f) + (drho - g[W] - g[E] - g[R]))) / 4.f;
         float t2 = u1 / 2.f * (g[NE] + g[SW] - g[SE] - g[NW]);
         float t3 = -u0 / 2.f * (-3.f * k[3] + k[4]) - 2.f * u1 * k[5];
         k[7] = -idt * (t1 + t2) + t3;
     }
     {
-        float t1 = drho / 9.f - g[NE] - g[NW] - g[SE] - g[SW];
+        float t1 = drho * (1.f / 9.f) - g[NE] - g[NW] - g[SE] - g[SW];
         float t2 = 2.f * (u0 * (g[NE] - g[NW] + g[SE] - g[SW]) + u1 * (g[NE] + g[NW] - g[SE] - g[SW]));
         float t3 = 4.f * u0 * u1 * (g[NW] - g[NE] + g[SE] - g[SW]);
-        float t4 = -u0 * u0 * (1.f / 3.f + (g[N] + g[NE] + g[NW] + g[Sd] + g[SE] + g[SW]));
-        float t5 = u1 * u1 * (3.f * u0 * u0 * rho - (1.f / 3.f + (g[E] + g[NE] + g[NW] + g[SE] + g[SW] + g[W])));
+        float t4 = -u0 * u0 * (1.f * (1.f / 3.f) + (g[N] + g[NE] + g[NW] + g[Sd] + g[SE] + g[SW]));
+        float t5 = u1 * u1 * (3.f * u0 * u0 * rho - (1.f * (1.f / 3.f) + (g[E] + g[NE] + g[NW] + g[SE] + g[SW] + g[W])));
         float t6 = -2.f * k[3] - 2.f * u0 * k[7] - 2.f * u1 * k[6] + 4.f * u0 * u1 * k[5] -
                    (3.f / 2.f * k[3] - k[4] / 2.f) * (u0 * u0 + u1 * u1);
         k[8] = idt * (1.f / 4.f * (t1 + t2 + t3 + t4 + t5)) + t6;
@@ -460,6 +467,17 @@ __global__ void __launch_bounds__(kBlock, 4) k_macro_pml(const WorkItem* __restr
     float* Q1cur = par ? S.Q1b : S.Q1a;
     const float* Q1prev = par ? S.Q1a : S.Q1b;
     const int nn = (int)(it.end - it.begin);
+    const int64_t i = (int64_t)it.begin + threadIdx.x;
+    const bool active = (int)threadIdx.x < nn;
+    const bool layer = active && i >= S.nb && i < S.nb + S.nl;
+    // node i carries NAGA's PML field of layer node i + pml_shift
+    const int64_t jf = i + S.pml_shift;
+    const bool field = active && jf >= S.nb && jf < S.nb + S.nl;
+    // per-node inputs issued before the row staging so their latency overlaps it
+    const float4 mp = active ? S.M[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float sg = layer ? __ldg(S.sigma + (i - S.nb)) : 0.f;
+    const float sf = field ? __ldg(S.sigma + (jf - S.nb)) : 0.f;
+    const bool src = active && i < S.nbl && S.is_src[i];
     {
         const float4* g4 = reinterpret_cast<const float4*>(S.G + (int64_t)it.begin * QP);
         const float4* q4 = reinterpret_cast<const float4*>(Q1prev + (int64_t)it.begin * QP);
@@ -469,9 +487,6 @@ __global__ void __launch_bounds__(kBlock, 4) k_macro_pml(const WorkItem* __restr
         }
     }
     __syncthreads();
-    const int64_t i = (int64_t)it.begin + threadIdx.x;
-    const bool active = (int)threadIdx.x < nn;
-    const bool layer = active && i >= S.nb && i < S.nb + S.nl;
     float* myG = reinterpret_cast<float*>(rowG) + threadIdx.x * QP;
     float* myQ = reinterpret_cast<float*>(rowQ) + threadIdx.x * QP;
     if (active) {
@@ -480,20 +495,13 @@ __global__ void __launch_bounds__(kBlock, 4) k_macro_pml(const WorkItem* __restr
         for (int a = 0; a < Q; ++a) g[a] = myG[L::pos(a)];
         float drho, u[3] = {0.f, 0.f, 0.f};
         macros<L>(g, drho, u);
-        const float4 mp = S.M[i];
         const float up[3] = {mp.y, mp.z, mp.w};
         S.M[i] = make_float4(drho, u[0], u[1], L::D == 3 ? u[2] : 0.f);
-        const float sg = layer ? __ldg(S.sigma + (i - S.nb)) : 0.f;
-        // node i carries NAGA's PML field of layer node i + pml_shift
-        const int64_t jf = i + S.pml_shift;
-        const bool field = jf >= S.nb && jf < S.nb + S.nl;
-        const float sf = field ? __ldg(S.sigma + (jf - S.nb)) : 0.f;
         float dcol[Q];
         collide<L>(g, drho, u, S, dcol);
         float q1[QP], out[QP], phi[QP];
 #pragma unroll
         for (int t = 0; t < QP; ++t) q1[t] = out[t] = phi[t] = 0.f;
-        const bool src = i < S.nbl && S.is_src[i];
 #pragma unroll
         for (int a = 0; a < Q; ++a) {
             const int t = L::pos(a);
