@@ -97,10 +97,12 @@ def kernel_bytes(dim, N, nb, nl, nbd, k, kb):
         "pml_gather": nbl * (st + 2 * row + 32) + nl * row,
         "edge_collide": nbd * (2 * row + 8 * kb),
         "filter": N * 2 * row + nbl * 8 * k,
-        "rk_stage1": nbl * (st + 3 * row),
-        "rk_stage2": nbl * (st + 5 * row),
-        "rk_stage3": nbl * (st + 5 * row),
-        "rk_stage4": nbl * (st + 4 * row),
+        # Horner RK4: stencil, the stage rows gathered (counted once), the
+        # node's own start row in, the stage row out
+        "rk_stage1": nbl * (st + 2 * row),
+        "rk_stage2": nbl * (st + 3 * row),
+        "rk_stage3": nbl * (st + 3 * row),
+        "rk_stage4": nbl * (st + 3 * row),
         "edge_interp": nbd * (8 * kb + row),
     }
 

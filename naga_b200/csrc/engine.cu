@@ -209,10 +209,10 @@ void set_parameters(naga_scene* s) {
         D.om_ab = 1.f / (3.f * nu_lat + .5f * dt_lat);
         for (int t = 0; t < 6; ++t) D.om_fix[t] = 0.f;
     }
-    D.a_half = dt_lat * 0.5f;
-    D.a_full = dt_lat * 1.f;
-    D.b1 = (float)(1. / 6.);
-    D.b2 = (float)(2. / 6.);
+    D.rk_a[0] = dt_lat * 0.25f;
+    D.rk_a[1] = dt_lat * (float)(1.0 / 3.0);
+    D.rk_a[2] = dt_lat * 0.5f;
+    D.rk_a[3] = dt_lat;
     D.half_dt = dt_lat / 2.f;
 }
 
@@ -251,19 +251,18 @@ int scene_setup(naga_scene* s) {
     V.sigma = sig;
 
     // state buffers
-    float* bufs[8];
-    for (int b = 0; b < 8; ++b) {
+    float* bufs[7];
+    for (int b = 0; b < 7; ++b) {
         if ((rc = s->alloc(&bufs[b], N * QP))) return rc;
         NAGA_CUDA_TRY(cudaMemsetAsync(bufs[b], 0, sizeof(float) * N * QP, st));
     }
     V.G = bufs[0];
     V.G1 = bufs[1];
     V.G2 = bufs[2];
-    V.ACC = bufs[3];
-    V.S1 = bufs[4];
-    V.S1P = bufs[5];
-    V.Q1a = bufs[6];
-    V.Q1b = bufs[7];
+    V.S1 = bufs[3];
+    V.S1P = bufs[4];
+    V.Q1a = bufs[5];
+    V.Q1b = bufs[6];
     float4* M = nullptr;
     if ((rc = s->alloc(&M, N))) return rc;
     NAGA_CUDA_TRY(cudaMemsetAsync(M, 0, sizeof(float4) * N, st));

@@ -2,7 +2,7 @@
 //
 // HBM layout of a scene with N nodes (order: bulk [0, nb), layer
 // [nb, nb + nl), boundary [nbl, nbl + nbd), ghost [.., N)):
-//   populations   G, G1, G2, ACC, S1, S1P: node-major rows of QP floats
+//   populations   G, G1, G2, S1, S1P: node-major rows of QP floats
 //                 (QP = 28 for D3Q27, 12 for D2Q9), centred: g = f - w,
 //                 populations in paired slot order (common.cuh)
 //   Q1a, Q1b      PML trapezoid integrals, rows of QP floats, ping-pong
@@ -44,14 +44,13 @@ struct SceneDev {
     float om_fix[6];  // D3Q27 fixed higher-order rates (1.5, 1.83, 1.4, 1.61, 1.98, 1.74)
     float inv_dt;     // 1 / dt_lat
     float rho0;
-    float a_half, a_full, b1, b2;  // RK4 coefficients dt/2, dt, 1/6, 2/6
+    float rk_a[4];                 // Horner RK4 stage factors dt/4, dt/3, dt/2, dt
     float half_dt;                 // dt_lat / 2 of the PML trapezoid rule
     float _pad1;
     // state
     float* G;
     float* G1;
     float* G2;
-    float* ACC;
     float* S1;
     float* S1P;
     float* Q1a;
