@@ -232,6 +232,16 @@ int naga_scene_read_probes_async(naga_scene* scene, int64_t first,
                                  int64_t count, float* out);
 /* centred populations g = f - w, host [N][Q], and rho - rho0, host [N]   */
 int naga_scene_read_state(naga_scene* scene, float* g, float* drho);
+/* Snapshots (replace NAGA's cereal save/load of its observers and state,
+ * density_observer.cuh:115-133, pml_absorption.inl:902-920): the dynamic
+ * state -- populations, macros, PML integrals, step counters, probe ring --
+ * as one host buffer with a versioned header. Loading it into a scene
+ * created from the same description resumes stepping bit for bit (the
+ * eviction / resume format of a serving loop). Stencil tables are rebuilt
+ * from the description, not stored.                                       */
+int64_t naga_scene_snapshot_bytes(const naga_scene* scene);
+int naga_scene_save(naga_scene* scene, void* buf, int64_t capacity);
+int naga_scene_load(naga_scene* scene, const void* buf, int64_t size);
 int naga_scene_write_state(naga_scene* scene, const float* g);
 /* set-up tables as stored for the step: idx [N][k], W [N][k][dim],
  * filter weights [N][k], boundary idx/weights [n_boundary][k_boundary],

@@ -111,6 +111,9 @@ _SIGS = {
     "naga_server_read_stats": ([C.c_void_p, C.c_void_p], C.c_int),
     "naga_profile_enable": ([C.c_int], C.c_int),
     "naga_tuning_report": ([C.c_char_p, C.c_int64], C.c_int64),
+    "naga_scene_snapshot_bytes": ([C.c_void_p], C.c_int64),
+    "naga_scene_save": ([C.c_void_p, C.c_void_p, C.c_int64], C.c_int),
+    "naga_scene_load": ([C.c_void_p, C.c_void_p, C.c_int64], C.c_int),
     "naga_scene_read_probes_async": ([C.c_void_p, C.c_int64, C.c_int64, C.c_void_p], C.c_int),
     "naga_profile_reset": ([], C.c_int),
     "naga_profile_read": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
@@ -254,6 +257,17 @@ class Scene:
         out = np.zeros((count, self.n_probes), np.float32)
         _check(lib().naga_scene_read_probes(self.h, first, count, _p(out)))
         return out
+
+    def save(self) -> bytes:
+        """Snapshot of the dynamic state (naga_scene_save)."""
+        n = lib().naga_scene_snapshot_bytes(self.h)
+        buf = C.create_string_buffer(int(n))
+        _check(lib().naga_scene_save(self.h, buf, n))
+        return buf.raw
+
+    def load(self, snapshot: bytes) -> None:
+        """Resume from a snapshot of a scene with the same description."""
+        _check(lib().naga_scene_load(self.h, snapshot, len(snapshot)))
 
     def probes_async(self, first: int, count: int, out) -> None:
         """Enqueue the copy of steps [first, first + count) to host address

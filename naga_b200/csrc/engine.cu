@@ -719,6 +719,90 @@ extern "C" int naga_scene_read_probes_async(naga_scene* s, int64_t first, int64_
     return NAGA_OK;
 }
 
+// ------------------------------------------------------------- snapshots
+// Dynamic state of a scene, enough to resume stepping bit for bit in a scene
+// created from the same description: populations, macros, both PML
+// integral buffers, the device step counter (its parity selects the Q1
+// buffer), the host step count and the probe ring. Tables are not included:
+// they are rebuilt from the description.
+namespace {
+struct SnapshotHeader {
+    char magic[8];  // "NAGASNP1"
+    int32_t version, dim, qp, n_probes;
+    int64_t n, probe_cap, steps;
+    uint64_t device_step;
+    int64_t payload;  // bytes after the header
+};
+int64_t snapshot_payload(const naga_scene* s) {
+    const int64_t rows = s->N * s->QP * (int64_t)sizeof(float);
+    return 3 * rows + s->N * (int64_t)sizeof(float4) +
+           (int64_t)s->dev.probe_cap * std::max(1, s->dev.np) * (int64_t)sizeof(float);
+}
+}  // namespace
+
+extern "C" int64_t naga_scene_snapshot_bytes(const naga_scene* s) {
+    return s ? (int64_t)sizeof(SnapshotHeader) + snapshot_payload(s) : -1;
+}
+
+extern "C" int naga_scene_save(naga_scene* s, void* buf, int64_t cap) {
+    if (!s || !buf) return set_error(NAGA_EINVAL, "naga_scene_save: null argument");
+    const int64_t need = naga_scene_snapshot_bytes(s);
+    if (cap < need) return set_error(NAGA_EINVAL, "naga_scene_save: buffer smaller than naga_scene_snapshot_bytes");
+    cudaStream_t st = active_stream(s);
+    NAGA_CUDA_TRY(cudaStreamSynchronize(st));
+    SnapshotHeader h{};
+    std::memcpy(h.magic, "NAGASNP1", 8);
+    h.version = 1;
+    h.dim = s->dim;
+    h.qp = s->QP;
+    h.n_probes = s->dev.np;
+    h.n = s->N;
+    h.probe_cap = s->dev.probe_cap;
+    h.steps = s->steps;
+    h.payload = snapshot_payload(s);
+    NAGA_CUDA_TRY(cudaMemcpyAsync(&h.device_step, s->dev.step, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+    char* p = static_cast<char*>(buf) + sizeof(SnapshotHeader);
+    const size_t rows = sizeof(float) * (size_t)s->N * s->QP;
+    NAGA_CUDA_TRY(cudaMemcpyAsync(p, s->dev.G, rows, cudaMemcpyDeviceToHost, st));
+    NAGA_CUDA_TRY(cudaMemcpyAsync(p + rows, s->dev.Q1a, rows, cudaMemcpyDeviceToHost, st));
+    NAGA_CUDA_TRY(cudaMemcpyAsync(p + 2 * rows, s->dev.Q1b, rows, cudaMemcpyDeviceToHost, st));
+    NAGA_CUDA_TRY(cudaMemcpyAsync(p + 3 * rows, s->dev.M, sizeof(float4) * s->N, cudaMemcpyDeviceToHost, st));
+    NAGA_CUDA_TRY(cudaMemcpyAsync(p + 3 * rows + sizeof(float4) * s->N, s->dev.probe_ring,
+                                  sizeof(float) * (size_t)s->dev.probe_cap * std::max(1, s->dev.np),
+                                  cudaMemcpyDeviceToHost, st));
+    NAGA_CUDA_TRY(cudaStreamSynchronize(st));
+    std::memcpy(buf, &h, sizeof h);
+    return NAGA_OK;
+}
+
+extern "C" int naga_scene_load(naga_scene* s, const void* buf, int64_t size) {
+    if (!s || !buf) return set_error(NAGA_EINVAL, "naga_scene_load: null argument");
+    if (size < (int64_t)sizeof(SnapshotHeader)) return set_error(NAGA_EINVAL, "naga_scene_load: truncated snapshot");
+    SnapshotHeader h;
+    std::memcpy(&h, buf, sizeof h);
+    if (std::memcmp(h.magic, "NAGASNP1", 8) != 0 || h.version != 1)
+        return set_error(NAGA_EINVAL, "naga_scene_load: not a snapshot of this format");
+    if (h.dim != s->dim || h.qp != s->QP || h.n != s->N || h.n_probes != s->dev.np || h.probe_cap != s->dev.probe_cap ||
+        h.payload != snapshot_payload(s))
+        return set_error(NAGA_EINVAL, "naga_scene_load: snapshot is of a scene with another shape");
+    if (size < (int64_t)sizeof h + h.payload) return set_error(NAGA_EINVAL, "naga_scene_load: truncated snapshot");
+    cudaStream_t st = active_stream(s);
+    NAGA_CUDA_TRY(cudaStreamSynchronize(st));
+    const char* p = static_cast<const char*>(buf) + sizeof h;
+    const size_t rows = sizeof(float) * (size_t)s->N * s->QP;
+    NAGA_CUDA_TRY(cudaMemcpyAsync(s->dev.G, p, rows, cudaMemcpyHostToDevice, st));
+    NAGA_CUDA_TRY(cudaMemcpyAsync(s->dev.Q1a, p + rows, rows, cudaMemcpyHostToDevice, st));
+    NAGA_CUDA_TRY(cudaMemcpyAsync(s->dev.Q1b, p + 2 * rows, rows, cudaMemcpyHostToDevice, st));
+    NAGA_CUDA_TRY(cudaMemcpyAsync(s->dev.M, p + 3 * rows, sizeof(float4) * s->N, cudaMemcpyHostToDevice, st));
+    NAGA_CUDA_TRY(cudaMemcpyAsync(s->dev.probe_ring, p + 3 * rows + sizeof(float4) * s->N,
+                                  sizeof(float) * (size_t)s->dev.probe_cap * std::max(1, s->dev.np),
+                                  cudaMemcpyHostToDevice, st));
+    NAGA_CUDA_TRY(cudaMemcpyAsync(s->dev.step, &h.device_step, sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+    NAGA_CUDA_TRY(cudaStreamSynchronize(st));
+    s->steps = h.steps;
+    return NAGA_OK;
+}
+
 extern "C" int naga_scene_read_state(naga_scene* s, float* g, float* drho) {
     if (!s) return set_error(NAGA_EINVAL, "naga_scene_read_state: null scene");
     NAGA_CUDA_TRY(cudaStreamSynchronize(active_stream(s)));

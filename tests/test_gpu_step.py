@@ -178,3 +178,32 @@ def test_async_probe_reads_match_synchronous(naga, oracle):
     s.probes_async(30, 10, wrap.data_ptr())  # ring slots 14, 15, 0, ..., 7
     s.sync()
     assert np.array_equal(wrap.numpy(), ref.probes(30, 10))
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_snapshot_resumes_bit_for_bit(naga, oracle, dim):
+    """Save after 17 steps, keep stepping; a new scene of the same
+    description loaded from the snapshot takes the same next 13 steps bit for
+    bit (state, probe trace, step count), across an odd step count so the
+    PML ping-pong parity is exercised; a snapshot of another shape is
+    rejected."""
+    n_side, layers = (30, 3) if dim == 2 else (14, 3)
+    g = naga.generate_grid(dim, n_side, layers, 2)
+    k = 16 if dim == 2 else 32
+    probes = PROBES2 if dim == 2 else PROBES3
+    a = naga.Scene(g, k=k, shape=1 if dim == 2 else 0, probes=probes, probe_capacity=64)
+    a.set_density(naga.gaussian_pulse(g["points"], [0.5] * dim, 1e-3, 0.08))
+    a.step(17)
+    snap = a.save()
+    a.step(13)
+    b = naga.Scene(g, k=k, shape=1 if dim == 2 else 0, probes=probes, probe_capacity=64)
+    b.load(snap)
+    assert b.step_count == 17
+    b.step(13)
+    assert b.step_count == a.step_count == 30
+    assert np.array_equal(a.state()[0], b.state()[0])
+    assert np.array_equal(a.probes(0, 30), b.probes(0, 30))
+    other = naga.Scene(naga.generate_grid(dim, n_side + 1, layers, 2), k=k, shape=1 if dim == 2 else 0,
+                       probes=probes, probe_capacity=64)
+    with pytest.raises(RuntimeError, match="another shape"):
+        other.load(snap)
