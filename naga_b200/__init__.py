@@ -112,6 +112,7 @@ _SIGS = {
     "naga_profile_enable": ([C.c_int], C.c_int),
     "naga_tuning_report": ([C.c_char_p, C.c_int64], C.c_int64),
     "naga_scene_snapshot_bytes": ([C.c_void_p], C.c_int64),
+    "naga_scene_set_density_source": ([C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64], C.c_int),
     "naga_scene_save": ([C.c_void_p, C.c_void_p, C.c_int64], C.c_int),
     "naga_scene_load": ([C.c_void_p, C.c_void_p, C.c_int64], C.c_int),
     "naga_scene_read_probes_async": ([C.c_void_p, C.c_int64, C.c_int64, C.c_void_p], C.c_int),
@@ -257,6 +258,14 @@ class Scene:
         out = np.zeros((count, self.n_probes), np.float32)
         _check(lib().naga_scene_read_probes(self.h, first, count, _p(out)))
         return out
+
+    def set_density_source(self, nodes, values) -> None:
+        """Density sources: values [n_steps][len(nodes)] (dimensional density,
+        float32 max = no term that step); see naga_scene_set_density_source."""
+        nodes = np.ascontiguousarray(nodes, np.int64)
+        values = np.ascontiguousarray(values, np.float32).reshape(-1, max(len(nodes), 1))
+        _check(lib().naga_scene_set_density_source(self.h, _p(nodes), len(nodes), _p(values),
+                                                   values.shape[0] if len(nodes) else 0))
 
     def save(self) -> bytes:
         """Snapshot of the dynamic state (naga_scene_save)."""

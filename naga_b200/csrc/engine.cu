@@ -96,6 +96,8 @@ struct naga_scene {
     naga_batch* owner = nullptr;                               // user batch, if any
     naga_batch* solo = nullptr;                                // private batch for naga_scene_step
     int64_t steps = 0;                                         // host mirror of the device counter
+    int* src_slot = nullptr;                                   // density sources (see SceneDev)
+    float* src_vals = nullptr;
     std::vector<float> probe_xyz;
 
     template <class T>
@@ -630,6 +632,8 @@ extern "C" int naga_scene_destroy(naga_scene* s) {
     if (s->solo) naga_batch_destroy(s->solo);
     if (s->stream) cudaStreamSynchronize(s->stream);
     for (void* p : s->allocs) cudaFree(p);
+    if (s->src_slot) cudaFree(s->src_slot);
+    if (s->src_vals) cudaFree(s->src_vals);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return NAGA_OK;
@@ -716,6 +720,47 @@ extern "C" int naga_scene_read_probes_async(naga_scene* s, int64_t first, int64_
     if (count > n1)
         NAGA_CUDA_TRY(cudaMemcpyAsync(out + n1 * np, s->dev.probe_ring, sizeof(float) * (count - n1) * np,
                                       cudaMemcpyDeviceToHost, st));
+    return NAGA_OK;
+}
+
+// --------------------------------------------------------- density sources
+extern "C" int naga_scene_set_density_source(naga_scene* s, const int64_t* nodes, int64_t n_nodes,
+                                             const float* values, int64_t n_steps) {
+    if (!s) return set_error(NAGA_EINVAL, "naga_scene_set_density_source: null scene");
+    if (n_nodes < 0 || n_steps < 0 || (n_nodes > 0 && (!nodes || (n_steps > 0 && !values))))
+        return set_error(NAGA_EINVAL, "naga_scene_set_density_source: invalid arguments");
+    std::vector<int> slot;
+    if (n_nodes > 0) {
+        slot.assign((size_t)s->N, -1);
+        for (int64_t t = 0; t < n_nodes; ++t) {
+            if (nodes[t] < 0 || nodes[t] >= s->N)
+                return set_error(NAGA_EINVAL, "naga_scene_set_density_source: node index out of range");
+            if (slot[nodes[t]] >= 0)
+                return set_error(NAGA_EINVAL, "naga_scene_set_density_source: node listed twice");
+            slot[nodes[t]] = (int)t;
+        }
+    }
+    cudaStream_t st = active_stream(s);
+    NAGA_CUDA_TRY(cudaStreamSynchronize(st));
+    if (s->src_slot) cudaFree(s->src_slot);
+    if (s->src_vals) cudaFree(s->src_vals);
+    s->src_slot = nullptr;
+    s->src_vals = nullptr;
+    if (n_nodes > 0 && n_steps > 0) {
+        NAGA_CUDA_TRY(cudaMalloc(&s->src_slot, sizeof(int) * (size_t)s->N));
+        NAGA_CUDA_TRY(cudaMalloc(&s->src_vals, sizeof(float) * (size_t)n_nodes * n_steps));
+        NAGA_CUDA_TRY(cudaMemcpyAsync(s->src_slot, slot.data(), sizeof(int) * slot.size(), cudaMemcpyHostToDevice, st));
+        NAGA_CUDA_TRY(cudaMemcpyAsync(s->src_vals, values, sizeof(float) * (size_t)n_nodes * n_steps,
+                                      cudaMemcpyHostToDevice, st));
+        NAGA_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    s->dev.src_slot = s->src_slot;
+    s->dev.src_vals = s->src_vals;
+    s->dev.src_n = s->src_slot ? n_nodes : 0;
+    s->dev.src_steps = s->src_slot ? n_steps : 0;
+    // the batches hold device copies of the scene description
+    if (s->owner) s->owner->dirty = true;
+    if (s->solo) s->solo->dirty = true;
     return NAGA_OK;
 }
 

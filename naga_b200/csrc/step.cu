@@ -33,6 +33,7 @@
 // touches 4 (8) rows instead of 32, and each thread holds two opposite
 // population pairs of its chunk.
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -463,7 +464,8 @@ __global__ void __launch_bounds__(kBlock, 4) k_macro_pml(const WorkItem* __restr
     __shared__ float4 rowG[kBlock * QP / 4], rowQ[kBlock * QP / 4];
     __shared__ double red[2][2 * QP];
     NAGA_FOR_ITEMS(items, nitems)
-    const int par = (int)(*S.step & 1ull);
+    const unsigned long long step = *S.step;
+    const int par = (int)(step & 1ull);
     float* Q1cur = par ? S.Q1b : S.Q1a;
     const float* Q1prev = par ? S.Q1a : S.Q1b;
     const int nn = (int)(it.end - it.begin);
@@ -495,6 +497,22 @@ __global__ void __launch_bounds__(kBlock, 4) k_macro_pml(const WorkItem* __restr
         for (int a = 0; a < Q; ++a) g[a] = myG[L::pos(a)];
         float drho, u[3] = {0.f, 0.f, 0.f};
         macros<L>(g, drho, u);
+        // density source of this step (after the probes sampled the macros):
+        // f_a += (s / rho0) w_a, and the reference's density statement
+        // rho <- (rho + (rho + s)) / 2 applied once, u unchanged
+        // (detail/simulation_engine.cuh:1057-1107 without its race)
+        if (S.src_slot) {
+            const int sl = S.src_slot[i];
+            if (sl >= 0 && (int64_t)step < S.src_steps) {
+                const float sv = S.src_vals[(int64_t)step * S.src_n + sl];
+                if (sv != FLT_MAX) {
+                    const float ds = sv / S.rho0;
+#pragma unroll
+                    for (int a = 0; a < Q; ++a) g[a] = fmaf(ds, LatticeTables<L>::w(a), g[a]);
+                    drho += 0.5f * ds;
+                }
+            }
+        }
         const float up[3] = {mp.y, mp.z, mp.w};
         S.M[i] = make_float4(drho, u[0], u[1], L::D == 3 ? u[2] : 0.f);
         float dcol[Q];
@@ -579,7 +597,16 @@ __global__ void __launch_bounds__(256) k_scene_tail(const SceneDev* __restrict__
         float v = 0.f;
         for (int s = lane_id(); s < S.kp; s += 32) {
             const uint32_t j = S.pidx[(int64_t)s * S.np + p];
-            v += S.pw[(int64_t)s * S.np + p] * S.M[j].x;
+            float dr = S.M[j].x;
+            // the probes see the density before this step's source term
+            if (S.src_slot) {
+                const int sl = S.src_slot[j];
+                if (sl >= 0 && (int64_t)step < S.src_steps) {
+                    const float sv = S.src_vals[(int64_t)step * S.src_n + sl];
+                    if (sv != FLT_MAX) dr -= 0.5f * (sv / S.rho0);
+                }
+            }
+            v += S.pw[(int64_t)s * S.np + p] * dr;
         }
         v = warp_sum(v);
         if (lane_id() == 0) S.probe_ring[(int64_t)slot * S.np + p] = v * S.rho0;

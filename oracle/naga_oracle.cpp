@@ -708,6 +708,7 @@ struct SceneBase {
     virtual int write_state(const double* g) = 0;
     virtual int tables(uint32_t*, double*, double*, uint32_t*, double*, uint32_t*, double*) const = 0;
     virtual int pml_state(double* q1, double* q2) const = 0;
+    virtual int set_sources(const int64_t* nodes, int64_t n, const float* values, int64_t n_steps) = 0;
 };
 
 // One scene, T = double (the FP64 oracle) or T = float (the reference's
@@ -735,6 +736,11 @@ struct Scene : SceneBase {
     // state (reference layout: population-major f[a][i])
     std::vector<T> f, s1, s2, q1, q2, rho, u, f0, df, kk;
     T time = 0;
+    // density sources: per-step values (dimensional density, FLT_MAX = no
+    // term this step) of a set of nodes; frame = steps since set_density
+    std::vector<int64_t> src_nodes;
+    std::vector<float> src_vals;  // [src_steps][n]
+    int64_t src_steps = 0, frame = 0;
 
     T& F(std::vector<T>& v, int a, int64_t i) { return v[(size_t)a * N + i]; }
 
@@ -861,7 +867,27 @@ struct Scene : SceneBase {
         for (int a = 0; a < Q; ++a)
             for (int64_t i = 0; i < N; ++i) F(f, a, i) = (T)L.w[a] * (T(1) + (T)drho[i]);
         macros();
+        frame = 0;
         return 0;
+    }
+
+    // apply_density_source_termsv5 (detail/simulation_engine.cuh:1057-1107)
+    // with the race over the Q threads of a node (N2) resolved: the
+    // population update f_a += (s / rho0) w_a once per population, and the
+    // density statement rho <- (rho + (rho + s)) / 2 once per node.
+    void apply_sources() {
+        if (src_nodes.empty() || frame >= src_steps) return;
+        const int64_t n = (int64_t)src_nodes.size();
+        for (int64_t t = 0; t < n; ++t) {
+            const float sv = src_vals[(size_t)frame * n + t];
+            if (sv == std::numeric_limits<float>::max()) continue;
+            const int64_t i = src_nodes[t];
+            const T st = (T)sv;
+            const T ds = st / rho0;
+            for (int a = 0; a < Q; ++a) F(f, a, i) += ds * (T)L.w[a];
+            const T imposed = (rho[i] + st) / rho0;
+            rho[i] = (rho[i] + imposed * rho0) / T(2);
+        }
     }
 
     // sum_s sum_d W(d,s,i) field_d(j_s): FP64 sums sequentially; FP32
@@ -1087,10 +1113,12 @@ struct Scene : SceneBase {
             macros();
             if (probes)
                 for (int p = 0; p < np; ++p) probes[(size_t)n * np + p] = probe(p);
+            apply_sources();
             pre_streaming();
             rk4();
             interpolate_boundaries(f);
             time += dt;
+            ++frame;
         }
         return 0;
     }
@@ -1098,11 +1126,13 @@ struct Scene : SceneBase {
     int phase(int ph) override {
         if (ph == 1) {
             macros();
+            apply_sources();
             pre_streaming();
         } else if (ph == 2) {
             rk4();
             interpolate_boundaries(f);
             time += dt;
+            ++frame;
         } else {
             return 1;
         }
@@ -1119,6 +1149,16 @@ struct Scene : SceneBase {
             }
             if (drho) drho[i] = r * (double)rho0 - (double)rho0;
         }
+        return 0;
+    }
+
+    int set_sources(const int64_t* nodes, int64_t n, const float* values, int64_t n_steps) override {
+        if (n < 0 || n_steps < 0 || (n > 0 && (!nodes || (n_steps > 0 && !values)))) return 1;
+        for (int64_t t = 0; t < n; ++t)
+            if (nodes[t] < 0 || nodes[t] >= N) return 1;
+        src_nodes.assign(nodes, nodes + n);
+        src_vals.assign(values, values + (size_t)n * n_steps);
+        src_steps = n_steps;
         return 0;
     }
 
@@ -1178,6 +1218,10 @@ extern "C" int orc_scene_create(const orc_scene_desc* d, orc_scene** out) {
     return 0;
 }
 extern "C" void orc_scene_destroy(orc_scene* s) { delete s; }
+extern "C" int orc_scene_set_sources(orc_scene* s, const int64_t* nodes, int64_t n, const float* values,
+                                     int64_t n_steps) {
+    return s->impl->set_sources(nodes, n, values, n_steps);
+}
 extern "C" int orc_scene_set_density(orc_scene* s, const float* d) { return s->impl->set_density(d); }
 extern "C" int orc_scene_step(orc_scene* s, int n, double* p) { return s->impl->step(n, p); }
 extern "C" int orc_scene_step_phase(orc_scene* s, int ph) { return s->impl->phase(ph); }

@@ -87,6 +87,11 @@ int orc_scene_set_density(orc_scene* s, const float* drho);
 /* advance nsteps; probe densities (rho - rho0) sampled at the start of
  * every step are appended to out_probes [nsteps][n_probes] (may be NULL). */
 int orc_scene_step(orc_scene* s, int nsteps, double* out_probes);
+/* density sources (per-step values of a node set, dimensional density,
+ * FLT_MAX = no term that step), applied after the probes of each step as
+ * detail/simulation_engine.cuh:1057-1107 without its race               */
+int orc_scene_set_sources(orc_scene* s, const int64_t* nodes, int64_t n,
+                          const float* values, int64_t n_steps);
 /* centred populations g = f - w, [N][Q] double, and rho - rho0 [N].      */
 int orc_scene_read_state(const orc_scene* s, double* g, double* drho);
 /* replace the populations (centred, [N][Q]) and recompute macros.        */

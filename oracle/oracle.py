@@ -63,6 +63,7 @@ def lib(path: str | None = None):
     L.orc_scene_write_state.argtypes = [vp, vp]
     L.orc_scene_tables.argtypes = [vp] * 8
     L.orc_scene_pml_state.argtypes = [vp, vp, vp]
+    L.orc_scene_set_sources.argtypes = [vp, vp, i64, vp, i64]
     L.orc_lattice.argtypes = [i32, vp, vp, vp, vp, vp]
     L.orc_collision.argtypes = [i32, vp, dbl, vp, dbl, dbl, vp]
     if path is None:
@@ -205,6 +206,13 @@ class Scene:
     def write_state(self, g):
         g = np.ascontiguousarray(g, np.float64)
         assert lib().orc_scene_write_state(self.h, _p(g)) == 0
+
+    def set_sources(self, nodes, values):
+        """Density sources: values [n_steps][len(nodes)] (dimensional
+        density, float32 max = no term that step)."""
+        nodes = np.ascontiguousarray(nodes, np.int64)
+        values = np.ascontiguousarray(values, np.float32).reshape(-1, len(nodes))
+        assert lib().orc_scene_set_sources(self.h, _p(nodes), len(nodes), _p(values), values.shape[0]) == 0
 
     def pml_state(self):
         q1 = np.zeros((self.N, self.Q)); q2 = np.zeros((self.N, self.Q))

@@ -206,3 +206,24 @@ def test_oracle_phases_equal_full_step(naga, oracle):
         b.phase(1)
         b.phase(2)
     assert np.array_equal(a.state()[0], b.state()[0])
+
+
+def test_oracle_density_sources(naga, oracle):
+    """Sources of only the sentinel (float32 max) change nothing, bit for bit;
+    a positive source raises the density at its node (the source pass of
+    simulation_engine.cuh:1057-1107, applied once per node)."""
+    g = naga.generate_grid(2, 24, 3, 0)
+    mk = lambda: oracle.Scene(2, g["points"], g["n_bulk"], g["n_layer"], g["n_boundary"], g["normals"],
+                              g["sigma"], g["h"], k=16, shape=1, probes=np.array([[0.5, 0.5]], np.float32))
+    drho = naga.gaussian_pulse(g["points"], [0.5, 0.5], 1e-3, 0.08)
+    a, b, c = mk(), mk(), mk()
+    for s in (a, b, c):
+        s.set_density(drho)
+    centre = int(np.argmin(((g["points"] - 0.5) ** 2).sum(1)))
+    b.set_sources([centre], np.full((5, 1), np.finfo(np.float32).max, np.float32))
+    c.set_sources([centre], np.full((5, 1), 1e-3, np.float32))
+    a.step(5)
+    b.step(5)
+    c.step(5)
+    assert np.array_equal(a.state()[0], b.state()[0])
+    assert c.state()[1][centre] > a.state()[1][centre]
