@@ -24,6 +24,7 @@
 #include <naga_b200.h>
 
 #include <algorithm>
+#include <limits>
 #include <array>
 #include <cstdint>
 #include <memory>
@@ -168,6 +169,22 @@ class density_observer : public simulation_observer<Lattice> {
     std::vector<value_type> density_values_, time_values_;
 };
 
+// A density source (density_source.cuh:41-82): before each step the engine
+// fills `source_terms` [N] with the sentinel std::numeric_limits<float>::
+// max() and calls every registered source, which writes the dimensional
+// density terms of its nodes for that step's time. NAGA's callback also
+// receives the device state (state_variables); here the state stays on the
+// GPU, so sources depend on the domain, the parameters and time.
+template <class Lattice>
+class density_source {
+  public:
+    using value_type = typename lattice_traits<Lattice>::value_type;
+    virtual void add_density_source(const simulation_nodes<value_type>& domain,
+                                    const problem_parameters<value_type>& params, const value_type& time,
+                                    std::vector<value_type>& source_terms) = 0;
+    virtual ~density_source() = default;
+};
+
 // Options of the B200 engine that NAGA fixes at compile time.
 struct engine_options {
     int k = 0;                 // stencil size; 0 = 32 (NAGA's num_interp_support)
@@ -233,6 +250,7 @@ class simulation_engine {
     void step_forward() {
         impl_->ensure();
         const int64_t t = naga_scene_step_count(impl_->scene);
+        if (!impl_->sources.empty()) impl_->upload_sources(t);
         detail::check(naga_scene_step(impl_->scene, 1), "step_forward");
         if (!impl_->observers.empty()) {
             std::vector<float> pr(impl_->observers.size());
@@ -253,6 +271,21 @@ class simulation_engine {
     value_type speed_of_sound() const { return impl_->params.speed_of_sound; }
     const simulation_domain_t& domain() const { return impl_->domain; }
     const problem_parameters_t& problem_parameters() const { return impl_->params; }
+
+    // simulation_engine::register_density_source (simulation_engine.cuh:80-82)
+    void register_density_source(density_source<Lattice>& src) {
+        auto& v = impl_->sources;
+        if (std::find(v.begin(), v.end(), &src) != v.end())
+            throw std::runtime_error("Density source already registered with an engine.");
+        v.push_back(&src);
+    }
+    void unregister_density_source(density_source<Lattice>& src) {
+        auto& v = impl_->sources;
+        v.erase(std::remove(v.begin(), v.end(), &src), v.end());
+        if (v.empty() && impl_->scene)
+            detail::check(naga_scene_set_density_source(impl_->scene, nullptr, 0, nullptr, 0, 0),
+                          "unregister_density_source");
+    }
 
     void attach_observer(simulation_observer<Lattice>& o) {
         impl_->observers.push_back(&o);
@@ -298,8 +331,31 @@ class simulation_engine {
         simulation_domain_t domain{};
         std::vector<float> drho;
         std::vector<simulation_observer<Lattice>*> observers;
+        std::vector<density_source<Lattice>*> sources;
+        std::vector<value_type> terms;  // per-step source terms [N]
+        std::vector<int64_t> src_nodes;
+        std::vector<float> src_row;
         naga_scene* scene = nullptr;
         value_type time = 0;
+
+        // the registered sources' terms for step t (time `time`) as one row
+        void upload_sources(int64_t t) {
+            const size_t N = domain.num_bulk_points + domain.num_layer_points + domain.num_boundary_points +
+                             domain.num_ghost_nodes;
+            const value_type none = std::numeric_limits<float>::max();
+            terms.assign(N, none);
+            for (auto* src : sources) src->add_density_source(domain, params, time, terms);
+            src_nodes.clear();
+            src_row.clear();
+            for (size_t i = 0; i < N; ++i)
+                if (terms[i] != none) {
+                    src_nodes.push_back((int64_t)i);
+                    src_row.push_back((float)terms[i]);
+                }
+            detail::check(naga_scene_set_density_source(scene, src_nodes.data(), (int64_t)src_nodes.size(),
+                                                        src_row.data(), t, src_nodes.empty() ? 0 : 1),
+                          "step_forward: density sources");
+        }
 
         void invalidate() {
             if (scene) naga_scene_destroy(scene);

@@ -236,16 +236,16 @@ int naga_scene_read_state(naga_scene* scene, float* g, float* drho);
  * simulation_engine.cuh:80-82, and density_source::add_density_source,
  * density_source.cuh:41-82): values [n_steps][n_nodes] of the listed nodes
  * (dimensional density; FLT_MAX = no term that step, NAGA's sentinel), kept
- * on the device; step t (counted from the last set_density) applies row t
- * after the probes sample the macros: f_a += (s / rho0) w_a, rho <- rho +
- * s / 2 once per node (NAGA's pass does these from racing threads,
- * detail/simulation_engine.cuh:1057-1107). Steps beyond n_steps have no
- * source. Replaces any earlier sources; n_nodes = 0 removes them. NAGA's
- * callback interface is host-polymorphic; a time series of values is its
- * device-side form for sources that depend on time only.                  */
+ * on the device; step first_step + r (steps counted from the last
+ * set_density) applies row r after the probes sample the macros:
+ * f_a += (s / rho0) w_a, rho <- rho + s / 2 once per node (NAGA's pass does
+ * these from racing threads, detail/simulation_engine.cuh:1057-1107). Other
+ * steps have no source. Replaces any earlier sources (the device node map
+ * is reused when the node list is unchanged, so a caller may upload one row
+ * per step cheaply); n_nodes = 0 removes them.                             */
 int naga_scene_set_density_source(naga_scene* scene, const int64_t* nodes,
                                   int64_t n_nodes, const float* values,
-                                  int64_t n_steps);
+                                  int64_t first_step, int64_t n_steps);
 /* Snapshots (replace NAGA's cereal save/load of its observers and state,
  * density_observer.cuh:115-133, pml_absorption.inl:902-920): the dynamic
  * state -- populations, macros, PML integrals, step counters, probe ring --

@@ -112,7 +112,8 @@ _SIGS = {
     "naga_profile_enable": ([C.c_int], C.c_int),
     "naga_tuning_report": ([C.c_char_p, C.c_int64], C.c_int64),
     "naga_scene_snapshot_bytes": ([C.c_void_p], C.c_int64),
-    "naga_scene_set_density_source": ([C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64], C.c_int),
+    "naga_scene_set_density_source": ([C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int64],
+                                      C.c_int),
     "naga_scene_save": ([C.c_void_p, C.c_void_p, C.c_int64], C.c_int),
     "naga_scene_load": ([C.c_void_p, C.c_void_p, C.c_int64], C.c_int),
     "naga_scene_read_probes_async": ([C.c_void_p, C.c_int64, C.c_int64, C.c_void_p], C.c_int),
@@ -259,12 +260,13 @@ class Scene:
         _check(lib().naga_scene_read_probes(self.h, first, count, _p(out)))
         return out
 
-    def set_density_source(self, nodes, values) -> None:
+    def set_density_source(self, nodes, values, first_step: int = 0) -> None:
         """Density sources: values [n_steps][len(nodes)] (dimensional density,
-        float32 max = no term that step); see naga_scene_set_density_source."""
+        float32 max = no term that step) for steps first_step, first_step + 1,
+        ...; see naga_scene_set_density_source."""
         nodes = np.ascontiguousarray(nodes, np.int64)
         values = np.ascontiguousarray(values, np.float32).reshape(-1, max(len(nodes), 1))
-        _check(lib().naga_scene_set_density_source(self.h, _p(nodes), len(nodes), _p(values),
+        _check(lib().naga_scene_set_density_source(self.h, _p(nodes), len(nodes), _p(values), first_step,
                                                    values.shape[0] if len(nodes) else 0))
 
     def save(self) -> bytes:

@@ -98,6 +98,8 @@ struct naga_scene {
     int64_t steps = 0;                                         // host mirror of the device counter
     int* src_slot = nullptr;                                   // density sources (see SceneDev)
     float* src_vals = nullptr;
+    int64_t src_vals_cap = 0;
+    std::vector<int64_t> src_nodes;
     std::vector<float> probe_xyz;
 
     template <class T>
@@ -725,42 +727,59 @@ extern "C" int naga_scene_read_probes_async(naga_scene* s, int64_t first, int64_
 
 // --------------------------------------------------------- density sources
 extern "C" int naga_scene_set_density_source(naga_scene* s, const int64_t* nodes, int64_t n_nodes,
-                                             const float* values, int64_t n_steps) {
+                                             const float* values, int64_t first_step, int64_t n_steps) {
     if (!s) return set_error(NAGA_EINVAL, "naga_scene_set_density_source: null scene");
-    if (n_nodes < 0 || n_steps < 0 || (n_nodes > 0 && (!nodes || (n_steps > 0 && !values))))
+    if (n_nodes < 0 || n_steps < 0 || first_step < 0 || (n_nodes > 0 && (!nodes || (n_steps > 0 && !values))))
         return set_error(NAGA_EINVAL, "naga_scene_set_density_source: invalid arguments");
-    std::vector<int> slot;
-    if (n_nodes > 0) {
-        slot.assign((size_t)s->N, -1);
-        for (int64_t t = 0; t < n_nodes; ++t) {
-            if (nodes[t] < 0 || nodes[t] >= s->N)
-                return set_error(NAGA_EINVAL, "naga_scene_set_density_source: node index out of range");
-            if (slot[nodes[t]] >= 0)
-                return set_error(NAGA_EINVAL, "naga_scene_set_density_source: node listed twice");
-            slot[nodes[t]] = (int)t;
-        }
-    }
     cudaStream_t st = active_stream(s);
     NAGA_CUDA_TRY(cudaStreamSynchronize(st));
-    if (s->src_slot) cudaFree(s->src_slot);
-    if (s->src_vals) cudaFree(s->src_vals);
-    s->src_slot = nullptr;
-    s->src_vals = nullptr;
-    if (n_nodes > 0 && n_steps > 0) {
-        NAGA_CUDA_TRY(cudaMalloc(&s->src_slot, sizeof(int) * (size_t)s->N));
-        NAGA_CUDA_TRY(cudaMalloc(&s->src_vals, sizeof(float) * (size_t)n_nodes * n_steps));
-        NAGA_CUDA_TRY(cudaMemcpyAsync(s->src_slot, slot.data(), sizeof(int) * slot.size(), cudaMemcpyHostToDevice, st));
-        NAGA_CUDA_TRY(cudaMemcpyAsync(s->src_vals, values, sizeof(float) * (size_t)n_nodes * n_steps,
-                                      cudaMemcpyHostToDevice, st));
+    if (n_nodes == 0 || n_steps == 0) {
+        if (s->src_slot) cudaFree(s->src_slot);
+        if (s->src_vals) cudaFree(s->src_vals);
+        s->src_slot = nullptr;
+        s->src_vals = nullptr;
+        s->src_nodes.clear();
+        s->src_vals_cap = 0;
+    } else {
+        const bool same_nodes = s->src_slot && (int64_t)s->src_nodes.size() == n_nodes &&
+                                std::equal(nodes, nodes + n_nodes, s->src_nodes.begin());
+        if (!same_nodes) {
+            std::vector<int> slot((size_t)s->N, -1);
+            for (int64_t t = 0; t < n_nodes; ++t) {
+                if (nodes[t] < 0 || nodes[t] >= s->N)
+                    return set_error(NAGA_EINVAL, "naga_scene_set_density_source: node index out of range");
+                if (slot[nodes[t]] >= 0)
+                    return set_error(NAGA_EINVAL, "naga_scene_set_density_source: node listed twice");
+                slot[nodes[t]] = (int)t;
+            }
+            if (!s->src_slot) NAGA_CUDA_TRY(cudaMalloc(&s->src_slot, sizeof(int) * (size_t)s->N));
+            NAGA_CUDA_TRY(cudaMemcpyAsync(s->src_slot, slot.data(), sizeof(int) * slot.size(), cudaMemcpyHostToDevice, st));
+            s->src_nodes.assign(nodes, nodes + n_nodes);
+        }
+        const int64_t nv = n_nodes * n_steps;
+        if (nv > s->src_vals_cap) {
+            if (s->src_vals) cudaFree(s->src_vals);
+            s->src_vals = nullptr;
+            NAGA_CUDA_TRY(cudaMalloc(&s->src_vals, sizeof(float) * (size_t)nv));
+            s->src_vals_cap = nv;
+        }
+        NAGA_CUDA_TRY(cudaMemcpyAsync(s->src_vals, values, sizeof(float) * (size_t)nv, cudaMemcpyHostToDevice, st));
         NAGA_CUDA_TRY(cudaStreamSynchronize(st));
     }
+    const bool on = s->src_slot != nullptr;
+    const bool relink = s->dev.src_slot != s->src_slot || s->dev.src_vals != s->src_vals ||
+                        s->dev.src_n != (on ? n_nodes : 0) || s->dev.src_first != (on ? first_step : 0) ||
+                        s->dev.src_steps != (on ? n_steps : 0);
     s->dev.src_slot = s->src_slot;
     s->dev.src_vals = s->src_vals;
-    s->dev.src_n = s->src_slot ? n_nodes : 0;
-    s->dev.src_steps = s->src_slot ? n_steps : 0;
+    s->dev.src_n = on ? n_nodes : 0;
+    s->dev.src_first = on ? first_step : 0;
+    s->dev.src_steps = on ? n_steps : 0;
     // the batches hold device copies of the scene description
-    if (s->owner) s->owner->dirty = true;
-    if (s->solo) s->solo->dirty = true;
+    if (relink) {
+        if (s->owner) s->owner->dirty = true;
+        if (s->solo) s->solo->dirty = true;
+    }
     return NAGA_OK;
 }
 

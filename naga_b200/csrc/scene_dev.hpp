@@ -69,11 +69,12 @@ struct SceneDev {
     const uint8_t* is_src;
     // outputs / bookkeeping
     // density sources: src_slot[i] = column of node i in src_vals (-1:
-    // none); src_vals [src_steps][src_n], FLT_MAX = no term that step.
+    // none); src_vals [src_steps][src_n], row r for step src_first + r,
+    // FLT_MAX = no term that step.
     // Null src_slot: the scene has no sources.
     const int* src_slot;
     const float* src_vals;
-    int64_t src_n, src_steps;
+    int64_t src_n, src_first, src_steps;  // rows apply to steps [src_first, src_first + src_steps)
     float* probe_ring;
     double* partials;  // [n_all_items][2 QP], slot order
     float* means;      // [2 QP], slot order

@@ -503,8 +503,9 @@ __global__ void __launch_bounds__(kBlock, 4) k_macro_pml(const WorkItem* __restr
         // (detail/simulation_engine.cuh:1057-1107 without its race)
         if (S.src_slot) {
             const int sl = S.src_slot[i];
-            if (sl >= 0 && (int64_t)step < S.src_steps) {
-                const float sv = S.src_vals[(int64_t)step * S.src_n + sl];
+            const int64_t row = (int64_t)step - S.src_first;
+            if (sl >= 0 && row >= 0 && row < S.src_steps) {
+                const float sv = S.src_vals[row * S.src_n + sl];
                 if (sv != FLT_MAX) {
                     const float ds = sv / S.rho0;
 #pragma unroll
@@ -601,8 +602,9 @@ __global__ void __launch_bounds__(256) k_scene_tail(const SceneDev* __restrict__
             // the probes see the density before this step's source term
             if (S.src_slot) {
                 const int sl = S.src_slot[j];
-                if (sl >= 0 && (int64_t)step < S.src_steps) {
-                    const float sv = S.src_vals[(int64_t)step * S.src_n + sl];
+                const int64_t row = (int64_t)step - S.src_first;
+                if (sl >= 0 && row >= 0 && row < S.src_steps) {
+                    const float sv = S.src_vals[row * S.src_n + sl];
                     if (sv != FLT_MAX) dr -= 0.5f * (sv / S.rho0);
                 }
             }
