@@ -18,6 +18,7 @@
 #include "scene_dev.hpp"
 
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 namespace naga {
@@ -273,6 +274,41 @@ __device__ __forceinline__ void kernel_and_weight(double delta, const double* xy
     }
 }
 
+// The quadrature of the stencil build depends on the node only through
+// delta: xy = delta u_q, and the product a_d(xy) w_q scales exactly as
+// 1 / delta (3-D: a ~ delta^2 / delta^6, w ~ delta^3; 2-D: a ~ delta^2 /
+// delta^5, w ~ delta^2). One launch tabulates u_q and K_qd = a_d w_q at
+// delta = 1 with the functions above; the per-node loop scales them.
+struct QuadTable {
+    double u[64][3];
+    double K[64][3];
+    double ksum[3];  // sum_q K_qd
+};
+__device__ QuadTable g_quad[2];  // D2Q9, D3Q27 (filled once per device)
+
+template <int D>
+__global__ void quad_table_kernel() {
+    QuadTable& g_q = g_quad[D - 2];
+    constexpr int nq = D == 2 ? 16 : 64;
+    const int q = threadIdx.x;
+    if (q < nq) {
+        double u[D], a[D], wq;
+        unit_quad<D>(q, u);
+        kernel_and_weight<D>(1.0, u, q, a, wq);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            g_q.u[q][d] = d < D ? u[d] : 0.0;
+            g_q.K[q][d] = d < D ? a[d] * wq : 0.0;
+        }
+    }
+    __syncthreads();
+    if (q < 3) {
+        double sum = 0;
+        for (int t = 0; t < nq; ++t) sum += g_q.K[t][q];  // fixed order
+        g_q.ksum[q] = sum;
+    }
+}
+
 // nearest-neighbour distance |x_i - x_{idx[i][1]}| in FP64
 template <int D>
 __global__ void nn_kernel(const float* __restrict__ pts, const uint32_t* __restrict__ idx, int k, int64_t n,
@@ -343,27 +379,27 @@ __global__ void divergence_build_kernel(const float* __restrict__ pts, int64_t n
         const double delta = 0.05 * sqrt(__shfl_sync(kFull, r2own[0], 1));
         __syncwarp();
         build_G0<D>(s.xs, k, shape, s.G);
-        // right-hand sides b_d = sum_q alpha_d(q) w_q G_x(q), rows lane / lane+32
+        // right-hand sides b_d = sum_q alpha_d(q) w_q G_x(q), rows lane / lane+32,
+        // from the delta = 1 table: x_q = delta u_q / h, alpha_d w_q = K_qd / delta
+        const QuadTable& tq = g_quad[D - 2];
         double b0[D], b1[D], cself[D];
+        const double rdel = 1.0 / delta, us = delta / sp;
 #pragma unroll
-        for (int d = 0; d < D; ++d) b0[d] = b1[d] = cself[d] = 0;
+        for (int d = 0; d < D; ++d) {
+            b0[d] = b1[d] = 0;
+            cself[d] = tq.ksum[d] * rdel;
+        }
         for (int q = 0; q < nq; ++q) {
-            double u[D], xy[D], a[D], xq[D], wq;
-            unit_quad<D>(q, u);
+            double xq[D];
 #pragma unroll
-            for (int d = 0; d < D; ++d) {
-                xy[d] = delta * u[d];
-                xq[d] = xy[d] / sp;
-            }
-            kernel_and_weight<D>(delta, xy, q, a, wq);
+            for (int d = 0; d < D; ++d) xq[d] = us * tq.u[q][d];
             const double g0 = lane < nsys ? gx_row<D>(s.xs, k, shape, xq, lane) : 0.0;
             const double g1 = lane + 32 < nsys ? gx_row<D>(s.xs, k, shape, xq, lane + 32) : 0.0;
 #pragma unroll
             for (int d = 0; d < D; ++d) {
-                const double aw = a[d] * wq;
+                const double aw = tq.K[q][d] * rdel;
                 b0[d] += aw * g0;
                 b1[d] += aw * g1;
-                cself[d] += aw;
             }
         }
         const int info = factor(s, nsys, precision);
@@ -477,6 +513,23 @@ int divergence_build_device(const float* pts, int64_t n, int dim, int k, int sha
     if (dim != 2 && dim != 3) return set_error(NAGA_EINVAL, "divergence build: dim must be 2 or 3");
     if (k < dim + 2 || nsys > 64) return set_error(NAGA_EINVAL, "divergence build: need dim + 2 <= k <= 60");
     if (n < k) return set_error(NAGA_EINVAL, "divergence build: fewer points than k");
+    {
+        // the quadrature table of this lattice, once per device
+        static std::mutex mu;
+        static bool filled[64][2] = {};
+        int dev = 0;
+        NAGA_CUDA_TRY(cudaGetDevice(&dev));
+        std::lock_guard<std::mutex> lk(mu);
+        if (dev >= 0 && dev < 64 && !filled[dev][dim - 2]) {
+            if (dim == 2)
+                quad_table_kernel<2><<<1, 64, 0, st>>>();
+            else
+                quad_table_kernel<3><<<1, 64, 0, st>>>();
+            NAGA_CUDA_TRY(cudaGetLastError());
+            NAGA_CUDA_TRY(cudaStreamSynchronize(st));
+            filled[dev][dim - 2] = true;
+        }
+    }
     float* d2 = nullptr;
     double* nn = nullptr;
     double* sp = nullptr;
