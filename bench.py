@@ -267,25 +267,47 @@ def serving_block(naga, torch, args, rank, world, dist):
         arrivals.append((t, max(16, int(round(n ** (1 / 3)))), len(arrivals)))
     router = replicas.Router(world)
     owner = [router.place(n_side ** 3, 2000) for (_, n_side, _) in arrivals]
+    mine = [a for a, o in zip(arrivals, owner) if o == rank]
     server = naga.Server(3, memory_budget=150 * 10 ** 9, steps_per_tick=20)
     probes = np.array(PROBES3, np.float32)
-    nxt, submitted = 0, 0
+    # the clients: a producer thread builds each request's point cloud and
+    # pulse in arrival order (the generator releases the GIL), the loop
+    # submits what has arrived and ticks
+    import queue
+
+    ready: queue.Queue = queue.Queue()
+    stop = threading.Event()
+
+    def produce():
+        for at, n_side, seed in mine:
+            if stop.is_set():
+                return
+            g = naga.generate_grid(3, n_side, max(2, n_side // 8), 1000 + seed)
+            ready.put((at, g, naga.gaussian_pulse(g["points"], [0.5] * 3, 1e-3, 0.05)))
+
+    producer = threading.Thread(target=produce, daemon=True)
+    submitted, pending = 0, None
     torch.cuda.synchronize()
     t0 = time.perf_counter()
+    producer.start()
     while True:
         el = time.perf_counter() - t0
         if el >= T:
             break
-        while nxt < len(arrivals) and arrivals[nxt][0] <= el:
-            at, n_side, seed = arrivals[nxt]
-            if owner[nxt] == rank:
-                g = naga.generate_grid(3, n_side, max(2, n_side // 8), 1000 + seed)
-                drho = naga.gaussian_pulse(g["points"], [0.5] * 3, 1e-3, 0.05)
-                server.submit(g, drho, 2000, k=32, shape=0, weight_precision=1, probes=probes,
-                              probe_capacity=2048)
-                submitted += 1
-            nxt += 1
+        while True:
+            if pending is None:
+                try:
+                    pending = ready.get_nowait()
+                except queue.Empty:
+                    break
+            if pending[0] > el:
+                break
+            _, g, drho = pending
+            server.submit(g, drho, 2000, k=32, shape=0, weight_precision=1, probes=probes, probe_capacity=2048)
+            submitted += 1
+            pending = None
         server.tick()
+    stop.set()
     torch.cuda.synchronize()
     st = server.stats()
     server.close()
