@@ -307,8 +307,14 @@ int scene_setup(naga_scene* s) {
     if ((rc = s->alloc(&pv, 2 * std::max<int64_t>(s->nbl, 1)))) return rc;
     NAGA_CUDA_TRY(cudaMemsetAsync(pv, 0, sizeof(float4) * 2 * std::max<int64_t>(s->nbl, 1), st));
     if (s->nl > 0 && (rc = pml_vectors_device(D, W, V.sigma, s->nb, s->nl, s->nbl, N, k, pv, st))) return rc;
+    float4* stp = nullptr;
+    if (s->nl > 0) {
+        if ((rc = s->alloc(&stp, (int64_t)k * s->nbl))) return rc;
+        if ((rc = pml_table_device(D, W, s->nb, s->nl, s->nbl, N, k, stp, st))) return rc;
+    }
     V.PHI = phi;
     V.PV = pv;
+    V.stP = stp;
 
     // boundary interpolation: kNN among bulk + layer, RPIM at the boundary
     // node with the nodal spacing (detail/simulation_engine.cuh:223-258)

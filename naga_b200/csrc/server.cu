@@ -75,6 +75,7 @@ extern "C" int64_t naga_scene_estimate_bytes(const naga_scene_desc* d) {
     b += ((N + 127) / 128) * 2 * QP * 8 + (int64_t)std::max(1, d->probe_capacity) * std::max(1, d->n_probes) * 4;
     // PML field rows of the layer and the per-node mean vectors
     b += d->n_layer * QP * 4 + (d->n_bulk + d->n_layer + 1) * 32;
+    if (d->n_layer > 0) b += (d->n_bulk + d->n_layer) * (int64_t)d->k * 16;  // PML gather records
     // set-up scratch: kNN sort + distances, nearest-neighbour means
     b += N * (16 + 12 + (int64_t)d->k * 4 + 8);
     return b;

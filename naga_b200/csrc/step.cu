@@ -766,6 +766,12 @@ struct StencilSrc {  // divergence stencil (Wx, Wy, Wz | filter weight, index)
         return {sc.stW + (int64_t)w.begin * k, (uint32_t)((w.end - w.begin) * k * sizeof(float4))};
     }
 };
+struct PmlSrc {  // PML gather records (see pml_table_kernel)
+    __device__ TileSrc operator()(const SceneDev& sc, const WorkItem& w) const {
+        const int k = sc.k;
+        return {sc.stP + (int64_t)w.begin * k, (uint32_t)((w.end - w.begin) * k * sizeof(float4))};
+    }
+};
 struct FilterSrc {  // D3Q27 filter records of the item's bulk/layer nodes
     __device__ TileSrc operator()(const SceneDev& sc, const WorkItem& w) const {
         const int k = sc.k;
@@ -805,17 +811,20 @@ __global__ void __launch_bounds__(kBlockMT) k_pml_gather(const WorkItem* __restr
     const int c = threadIdx.x % G::TPN, ns = threadIdx.x / G::TPN;
     float d0[3], d1[3];
     pair_dirs<L>(c < G::NCH ? c : 0, d0, d1);
-    NAGA_PIPE_BEGIN(float4, (tile_cap<G::NPB, K>()), StencilSrc{})
+    NAGA_PIPE_BEGIN(float4, (tile_cap<G::NPB, K>()), PmlSrc{})
     const int k = K > 0 ? K : S.k;
     const int nn = (int)(it.end - it.begin);
     const int64_t i = (int64_t)it.begin + ns;
     if (ns < nn && c < G::NCH) {
         float4 dv = make_float4(0.f, 0.f, 0.f, 0.f);
+        // the node's layer supports lead its records (in stencil order) and
+        // their count rides in V1.w: no per-support layer test
+        const float4 v1 = __ldg(S.PV + 2 * i), v2 = __ldg(S.PV + 2 * i + 1);
+        const int kn = min((int)__float_as_uint(v1.w), k);
 #pragma unroll 8
-        for (int s = 0; s < k; ++s) {
+        for (int s = 0; s < kn; ++s) {
             const float4 rec = tile[s * nn + ns];
-            const int64_t jl = (int64_t)__float_as_uint(rec.w) - S.nb;
-            if (jl < 0 || jl >= S.nl) continue;
+            const uint32_t jl = __float_as_uint(rec.w);
             const float wz = L::D == 3 ? rec.z : 0.f;
             const float4 v = ld4g<L>(S.PHI, jl, c);
             const float p0 = d0[0] * rec.x + d0[1] * rec.y + d0[2] * wz;
@@ -827,7 +836,6 @@ __global__ void __launch_bounds__(kBlockMT) k_pml_gather(const WorkItem* __restr
         }
         const float4 m1 = *reinterpret_cast<const float4*>(S.means + 4 * c);
         const float4 m2 = *reinterpret_cast<const float4*>(S.means + QP + 4 * c);
-        const float4 v1 = __ldg(S.PV + 2 * i), v2 = __ldg(S.PV + 2 * i + 1);
         const float e1 = d0[0] * v1.x + d0[1] * v1.y + d0[2] * v1.z;
         const float e2 = d0[0] * v2.x + d0[1] * v2.y + d0[2] * v2.z;
         const float f1 = d1[0] * v1.x + d1[1] * v1.y + d1[2] * v1.z;
@@ -1056,6 +1064,7 @@ __global__ void pml_vectors_kernel(const float4* __restrict__ stW, const float* 
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nbl) return;
     float4 v1 = make_float4(0.f, 0.f, 0.f, 0.f), v2 = v1;
+    uint32_t cnt = 0;
     for (int s = 0; s < k; ++s) {
         const float4 r = stW[pass_record(i, s, k, nbl, n, npb)];
         const int64_t jl = (int64_t)__float_as_uint(r.w) - nb;
@@ -1069,11 +1078,44 @@ __global__ void pml_vectors_kernel(const float4* __restrict__ stW, const float* 
             v1.z = fmaf(r.z, sg, v1.z);
             v2.z = fmaf(r.z, sg2, v2.z);
         }
+        ++cnt;
     }
+    v1.w = __uint_as_float(cnt);  // count of layer supports (pml_table_kernel puts them first)
     PV[2 * i] = v1;
     PV[2 * i + 1] = v2;
 }
 }  // namespace
+
+namespace {
+// PML gather records in the stencil's pass order: the node's supports in
+// the layer first, in stencil order, as (Wx, Wy, Wz or 0, PHI row j - nb);
+// then zero-weight records on the last such row (never read by the gather,
+// whose trip count is the node's layer-support count, but valid rows)
+__global__ void pml_table_kernel(const float4* __restrict__ stW, int64_t nb, int64_t nl, int64_t nbl, int64_t n,
+                                 int k, int npb, int dim, float4* __restrict__ stP) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nbl || nl <= 0) return;
+    int o = 0;
+    uint32_t last = 0;
+    for (int s = 0; s < k; ++s) {
+        const float4 r = stW[pass_record(i, s, k, nbl, n, npb)];
+        const int64_t jl = (int64_t)__float_as_uint(r.w) - nb;
+        if (jl < 0 || jl >= nl) continue;
+        last = (uint32_t)jl;
+        stP[pass_record(i, o++, k, nbl, n, npb)] = make_float4(r.x, r.y, dim == 3 ? r.z : 0.f, __uint_as_float(last));
+    }
+    for (; o < k; ++o) stP[pass_record(i, o, k, nbl, n, npb)] = make_float4(0.f, 0.f, 0.f, __uint_as_float(last));
+}
+}  // namespace
+
+int pml_table_device(int dim, const float4* stW, int64_t nb, int64_t nl, int64_t nbl, int64_t n, int k, float4* stP,
+                     cudaStream_t st) {
+    if (nbl <= 0 || nl <= 0) return NAGA_OK;
+    pml_table_kernel<<<(unsigned)((nbl + 255) / 256), 256, 0, st>>>(stW, nb, nl, nbl, n, k, nodes_per_pass(dim), dim,
+                                                                    stP);
+    NAGA_CUDA_TRY(cudaGetLastError());
+    return NAGA_OK;
+}
 
 int pml_vectors_device(int dim, const float4* stW, const float* sigma, int64_t nb, int64_t nl, int64_t nbl, int64_t n,
                        int k, float4* PV, cudaStream_t st) {
