@@ -303,7 +303,7 @@ def serving_block(naga, torch, args, rank, world, dist):
             if pending[0] > el:
                 break
             _, g, drho = pending
-            server.submit(g, drho, 2000, k=32, shape=0, weight_precision=1, probes=probes, probe_capacity=2048)
+            server.submit(g, drho, 2000, k=32, shape=0, probes=probes, probe_capacity=2048)
             submitted += 1
             pending = None
         server.tick()
@@ -319,7 +319,8 @@ def serving_block(naga, torch, args, rank, world, dist):
             "p50_step_ms": replicas.max_over_ranks(st["p50_step_ms"], dist, "cuda"),
             "p99_step_ms": replicas.max_over_ranks(st["p99_step_ms"], dist, "cuda"),
             "ticks_rank0": st["ticks"], "done": st["done"], "active_at_end": st["active"],
-            "queued_at_end": st["queued"], "failed": st["failed"], "peak_bytes_rank0": st["peak_bytes"]}
+            "queued_at_end": st["queued"], "failed": st["failed"], "peak_bytes_rank0": st["peak_bytes"],
+            "host_ms_rank0": {k: round(st[k + "_ms"], 1) for k in ("prepare", "admit", "wait", "retire")}}
 
 
 def setup_block(naga, torch, args):

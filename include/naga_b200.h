@@ -319,6 +319,10 @@ typedef struct naga_server_stats {
     int64_t bytes_in_use, peak_bytes;
     int64_t done, failed;
     int active, queued;
+    /* host wall time spent in each phase of naga_server_tick, summed:
+     * preparing the batch (membership changes, graph capture), admitting
+     * (scene set-up), waiting for the batch, retiring and growing it      */
+    double prepare_ms, admit_ms, wait_ms, retire_ms;
 } naga_server_stats;
 
 /* estimated device bytes of a scene (resident state plus set-up scratch)  */

@@ -366,7 +366,9 @@ class ServerStats(C.Structure):
     _fields_ = [("ticks", C.c_int64), ("steps", C.c_int64), ("node_updates", C.c_int64),
                 ("busy_ms", C.c_double), ("p50_step_ms", C.c_double), ("p99_step_ms", C.c_double),
                 ("bytes_in_use", C.c_int64), ("peak_bytes", C.c_int64), ("done", C.c_int64),
-                ("failed", C.c_int64), ("active", C.c_int), ("queued", C.c_int)]
+                ("failed", C.c_int64), ("active", C.c_int), ("queued", C.c_int),
+                ("prepare_ms", C.c_double), ("admit_ms", C.c_double), ("wait_ms", C.c_double),
+                ("retire_ms", C.c_double)]
 
 
 def scene_desc(grid: dict, *, k: int, k_boundary=None, k_probe=None, shape=1, pml_indexing=0,

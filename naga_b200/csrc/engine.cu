@@ -13,6 +13,7 @@
 #include <cstring>
 #include <memory>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 namespace naga {
@@ -93,6 +94,8 @@ struct naga_scene {
     std::vector<void*> allocs;
     int64_t bytes = 0;
     std::vector<WorkItem> items_all, items_all_mt, items_fluid, items_edge, items_pml;  // scene slot 0
+    WorkItem* d_lists = nullptr;  // the five lists above back to back on the device (batch rebuilds copy them)
+    int64_t n_list[5] = {};
     naga_batch* owner = nullptr;                               // user batch, if any
     naga_batch* solo = nullptr;                                // private batch for naga_scene_step
     int64_t steps = 0;                                         // host mirror of the device counter
@@ -118,6 +121,13 @@ struct naga_scene {
     }
 };
 
+// one scene's item list copied into a batch list, with the scene slot set
+struct ListCopy {
+    const WorkItem* src;
+    int64_t dst;
+    uint32_t n, scene;
+};
+
 struct naga_batch {
     int dim = 0;
     bool is_solo = false;
@@ -130,22 +140,46 @@ struct naga_batch {
     int k = 0, kb = 0;  // common stencil sizes of the members (0 if they differ)
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    // grow-only device tables (a membership change rewrites them in place on
+    // the batch stream; they are reallocated only when they must grow)
+    WorkItem* d_items = nullptr;  // the five item lists back to back
+    int64_t items_cap = 0;
+    int scenes_cap = 0;
+    ListCopy* d_copies = nullptr;
+    int copies_cap = 0;
+    void* h_stage = nullptr;  // page-locked staging of the scene and copy tables
+    size_t stage_cap = 0;
 
-    void free_tables() {
+    void free_graph() {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         exec = nullptr;
         graph = nullptr;
+    }
+    void free_tables() {
+        free_graph();
         if (d_scenes) cudaFree(d_scenes);
-        if (d_all) cudaFree(d_all);
-        if (d_fluid) cudaFree(d_fluid);
-        if (d_edge) cudaFree(d_edge);
-        if (d_pml) cudaFree(d_pml);
-        if (d_all_mt) cudaFree(d_all_mt);
+        if (d_items) cudaFree(d_items);
+        if (d_copies) cudaFree(d_copies);
+        if (h_stage) cudaFreeHost(h_stage);
         d_scenes = nullptr;
+        d_items = nullptr;
+        d_copies = nullptr;
+        h_stage = nullptr;
         d_all = d_all_mt = d_fluid = d_edge = d_pml = nullptr;
+        items_cap = stage_cap = 0;
+        scenes_cap = copies_cap = 0;
     }
 };
+
+__global__ void concat_items_kernel(const ListCopy* __restrict__ copies, WorkItem* __restrict__ dst) {
+    const ListCopy c = copies[blockIdx.y];
+    for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < c.n; w += gridDim.x * blockDim.x) {
+        WorkItem it = c.src[w];
+        it.scene = c.scene;
+        dst[c.dst + w] = it;
+    }
+}
 
 // flag[w] = 1 when a node of item w has a stencil support in the layer
 // [nb, nb + nl) (idx: node-major [n][k] kNN indices)
@@ -443,6 +477,20 @@ int scene_setup(naga_scene* s) {
             if (flag[w]) s->items_pml.push_back(s->items_fluid[w]);
     }
     V.n_all_items = (int)s->items_all.size();
+    {
+        const std::vector<WorkItem>* lists[5] = {&s->items_all, &s->items_all_mt, &s->items_fluid, &s->items_edge,
+                                                 &s->items_pml};
+        std::vector<WorkItem> packed;
+        for (int l = 0; l < 5; ++l) {
+            s->n_list[l] = (int64_t)lists[l]->size();
+            packed.insert(packed.end(), lists[l]->begin(), lists[l]->end());
+        }
+        if ((rc = s->alloc(&s->d_lists, (int64_t)packed.size()))) return rc;
+        if (!packed.empty())
+            NAGA_CUDA_TRY(cudaMemcpyAsync(s->d_lists, packed.data(), sizeof(WorkItem) * packed.size(),
+                                          cudaMemcpyHostToDevice, st));
+        NAGA_CUDA_TRY(cudaStreamSynchronize(st));
+    }
     double* partials = nullptr;
     if ((rc = s->alloc(&partials, (int64_t)V.n_all_items * 2 * QP))) return rc;
     NAGA_CUDA_TRY(cudaMemsetAsync(partials, 0, sizeof(double) * V.n_all_items * 2 * QP, st));
@@ -460,58 +508,85 @@ int scene_setup(naga_scene* s) {
 }
 
 int batch_rebuild(naga_batch* b) {
-    b->free_tables();
-    std::vector<SceneDev> sd;
-    std::vector<WorkItem> all, all_mt, fluid, edge, pml;
-    b->k = b->members.empty() ? 0 : b->members[0]->desc.k;
-    b->kb = b->members.empty() ? 0 : b->members[0]->desc.k_boundary;
-    for (size_t t = 0; t < b->members.size(); ++t) {
-        naga_scene* s = b->members[t];
+    b->free_graph();
+    const int ns = (int)b->members.size();
+    b->k = ns == 0 ? 0 : b->members[0]->desc.k;
+    b->kb = ns == 0 ? 0 : b->members[0]->desc.k_boundary;
+    int64_t n[5] = {}, base[6] = {};
+    for (naga_scene* s : b->members) {
         if (s->desc.k != b->k) b->k = 0;
         if (s->desc.k_boundary != b->kb) b->kb = 0;
-        for (auto it : s->items_all_mt) {
-            it.scene = (uint32_t)t;
-            all_mt.push_back(it);
-        }
-        sd.push_back(s->dev);
-        for (auto it : s->items_pml) {
-            it.scene = (uint32_t)t;
-            pml.push_back(it);
-        }
-        for (auto it : s->items_all) {
-            it.scene = (uint32_t)t;
-            all.push_back(it);
-        }
-        for (auto it : s->items_fluid) {
-            it.scene = (uint32_t)t;
-            fluid.push_back(it);
-        }
-        for (auto it : s->items_edge) {
-            it.scene = (uint32_t)t;
-            edge.push_back(it);
-        }
+        for (int l = 0; l < 5; ++l) n[l] += s->n_list[l];
     }
-    b->n_all = (int)all.size();
-    b->n_all_mt = (int)all_mt.size();
-    b->n_fluid = (int)fluid.size();
-    b->n_edge = (int)edge.size();
-    b->n_pml = (int)pml.size();
-    auto up = [&](auto** dst, const auto& v) -> int {
-        using T = typename std::remove_reference<decltype(v)>::type::value_type;
-        size_t bytes = sizeof(T) * std::max<size_t>(v.size(), 1);
-        NAGA_CUDA_TRY(cudaMalloc((void**)dst, bytes));
-        if (!v.empty())
-            NAGA_CUDA_TRY(cudaMemcpyAsync(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, b->stream));
-        NAGA_CUDA_TRY(cudaStreamSynchronize(b->stream));
+    for (int l = 0; l < 5; ++l) base[l + 1] = base[l] + n[l];
+    for (int l = 0; l < 5; ++l)
+        if (n[l] > 0x7fffffff) return set_error(NAGA_EINVAL, "batch: more than 2^31 - 1 work items in one list");
+    // grow the device tables (cudaFree waits for the device, so only here)
+    auto grow = [&](auto** p, auto& cap, int64_t need) -> int {
+        if (need <= (int64_t)cap && *p) return NAGA_OK;
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+        const int64_t c = std::max<int64_t>(need + need / 4, 16);
+        using T = typename std::remove_pointer<typename std::remove_reference<decltype(*p)>::type>::type;
+        cudaError_t e = cudaMalloc((void**)p, sizeof(T) * (size_t)c);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            cap = 0;
+            return set_error(e == cudaErrorMemoryAllocation ? NAGA_ENOMEM : NAGA_ECUDA,
+                             std::string("batch tables: ") + cudaGetErrorString(e));
+        }
+        cap = (std::remove_reference_t<decltype(cap)>)c;
         return NAGA_OK;
     };
+    std::vector<ListCopy> copies;
+    int64_t dst[5];
+    for (int l = 0; l < 5; ++l) dst[l] = base[l];
+    for (int t = 0; t < ns; ++t) {
+        naga_scene* s = b->members[t];
+        int64_t at = 0;
+        for (int l = 0; l < 5; ++l) {
+            if (s->n_list[l] > 0) copies.push_back({s->d_lists + at, dst[l], (uint32_t)s->n_list[l], (uint32_t)t});
+            at += s->n_list[l];
+            dst[l] += s->n_list[l];
+        }
+    }
     int rc;
-    if ((rc = up(&b->d_scenes, sd))) return rc;
-    if ((rc = up(&b->d_all, all))) return rc;
-    if ((rc = up(&b->d_all_mt, all_mt))) return rc;
-    if ((rc = up(&b->d_fluid, fluid))) return rc;
-    if ((rc = up(&b->d_edge, edge))) return rc;
-    if ((rc = up(&b->d_pml, pml))) return rc;
+    if ((rc = grow(&b->d_items, b->items_cap, std::max<int64_t>(base[5], 1)))) return rc;
+    if ((rc = grow(&b->d_scenes, b->scenes_cap, std::max(ns, 1)))) return rc;
+    if ((rc = grow(&b->d_copies, b->copies_cap, std::max<int64_t>((int64_t)copies.size(), 1)))) return rc;
+    const size_t sb = sizeof(SceneDev) * ns, cb = sizeof(ListCopy) * copies.size();
+    if (sb + cb > b->stage_cap) {
+        if (b->h_stage) cudaFreeHost(b->h_stage);
+        b->h_stage = nullptr;
+        b->stage_cap = 0;
+        NAGA_CUDA_TRY(cudaMallocHost(&b->h_stage, (sb + cb) * 5 / 4 + 256));
+        b->stage_cap = (sb + cb) * 5 / 4 + 256;
+    }
+    char* stage = (char*)b->h_stage;
+    for (int t = 0; t < ns; ++t) std::memcpy(stage + sizeof(SceneDev) * t, &b->members[t]->dev, sizeof(SceneDev));
+    if (cb) std::memcpy(stage + sb, copies.data(), cb);
+    if (sb) NAGA_CUDA_TRY(cudaMemcpyAsync(b->d_scenes, stage, sb, cudaMemcpyHostToDevice, b->stream));
+    if (cb) NAGA_CUDA_TRY(cudaMemcpyAsync(b->d_copies, stage + sb, cb, cudaMemcpyHostToDevice, b->stream));
+    uint32_t most = 1;
+    for (const ListCopy& c : copies) most = std::max(most, c.n);
+    const unsigned gx = (unsigned)std::min<uint32_t>((most + 255) / 256, 256);
+    for (size_t c0 = 0; c0 < copies.size(); c0 += 65535) {
+        const unsigned gy = (unsigned)std::min<size_t>(copies.size() - c0, 65535);
+        concat_items_kernel<<<dim3(gx, gy), 256, 0, b->stream>>>(b->d_copies + c0, b->d_items);
+        NAGA_CUDA_TRY(cudaGetLastError());
+    }
+    // the staging buffer is reused by the next rebuild
+    NAGA_CUDA_TRY(cudaStreamSynchronize(b->stream));
+    b->d_all = b->d_items + base[0];
+    b->d_all_mt = b->d_items + base[1];
+    b->d_fluid = b->d_items + base[2];
+    b->d_edge = b->d_items + base[3];
+    b->d_pml = b->d_items + base[4];
+    b->n_all = (int)n[0];
+    b->n_all_mt = (int)n[1];
+    b->n_fluid = (int)n[2];
+    b->n_edge = (int)n[3];
+    b->n_pml = (int)n[4];
     b->dirty = false;
     return NAGA_OK;
 }

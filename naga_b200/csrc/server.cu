@@ -58,6 +58,7 @@ struct naga_server {
     int64_t ticks = 0, steps = 0, node_updates = 0;
     double busy_ms = 0;
     double last_tick_ms = 0;     // device time of the previous tick's steps
+    double prepare_ms = 0, admit_ms = 0, wait_ms = 0, retire_ms = 0;  // host wall time per tick phase
     std::vector<float> step_ms;  // per-step latency samples
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int64_t done = 0, failed = 0;
@@ -178,10 +179,16 @@ extern "C" int naga_server_tick(naga_server* s, int* n_active, int* n_queued) {
     const bool stepping = !s->active.empty();
     cudaStream_t bst = (cudaStream_t)naga_batch_stream(s->batch);
     int rc;
+    using clock = std::chrono::steady_clock;
+    auto since = [](clock::time_point t0) {
+        return std::chrono::duration<double, std::milli>(clock::now() - t0).count();
+    };
     if (stepping) {
         // membership changes (rebuild, first-time shape tuning, graph
         // capture) happen here, outside the timed window of the steps
+        const auto t_prep = clock::now();
         if ((rc = naga_batch_prepare(s->batch))) return rc;
+        s->prepare_ms += since(t_prep);
         NAGA_CUDA_TRY(cudaEventRecord(s->ev0, bst));
         if ((rc = naga_batch_step(s->batch, spt))) return rc;
         NAGA_CUDA_TRY(cudaEventRecord(s->ev1, bst));
@@ -192,14 +199,10 @@ extern "C" int naga_server_tick(naga_server* s, int* n_active, int* n_queued) {
     // previous tick's steps the rest waits, so a burst of arrivals does not
     // stall the running scenes (at least one request is admitted per tick).
     std::vector<int64_t> admitted;
-    const auto t_admit = std::chrono::steady_clock::now();
+    const auto t_admit = clock::now();
     const double admit_budget_ms = std::max(5.0, s->last_tick_ms);
     while (!s->queue.empty()) {
-        if (!admitted.empty() && stepping) {
-            const double spent =
-                std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_admit).count();
-            if (spent > admit_budget_ms) break;
-        }
+        if (!admitted.empty() && stepping && since(t_admit) > admit_budget_ms) break;
         Request& r = *s->reqs[s->queue.front()];
         const int slots_used = (int)(s->active.size() + admitted.size());
         if (s->cfg.max_active > 0 && slots_used >= s->cfg.max_active) break;
@@ -226,9 +229,12 @@ extern "C" int naga_server_tick(naga_server* s, int* n_active, int* n_queued) {
         r.state = 1;
         admitted.push_back(r.id);
     }
+    s->admit_ms += since(t_admit);
     // 3. retire finished requests, then grow the batch
     if (stepping) {
+        const auto t_wait = clock::now();
         NAGA_CUDA_TRY(cudaEventSynchronize(s->ev1));
+        s->wait_ms += since(t_wait);
         float ms = 0;
         NAGA_CUDA_TRY(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
         s->busy_ms += ms;
@@ -238,6 +244,7 @@ extern "C" int naga_server_tick(naga_server* s, int* n_active, int* n_queued) {
         s->steps += spt;
         for (int64_t id : s->active) s->node_updates += s->reqs[id]->nodes * spt;
     }
+    const auto t_retire = clock::now();
     std::vector<int64_t> still;
     for (int64_t id : s->active) {
         Request& r = *s->reqs[id];
@@ -264,6 +271,7 @@ extern "C" int naga_server_tick(naga_server* s, int* n_active, int* n_queued) {
         if ((rc = naga_batch_add(s->batch, s->reqs[id]->scene))) return rc;
         s->active.push_back(id);
     }
+    s->retire_ms += since(t_retire);
     if (n_active) *n_active = (int)s->active.size();
     if (n_queued) *n_queued = (int)s->queue.size();
     return NAGA_OK;
@@ -305,6 +313,10 @@ extern "C" int naga_server_read_stats(naga_server* s, naga_server_stats* out) {
     st.queued = (int)s->queue.size();
     st.done = s->done;
     st.failed = s->failed;
+    st.prepare_ms = s->prepare_ms;
+    st.admit_ms = s->admit_ms;
+    st.wait_ms = s->wait_ms;
+    st.retire_ms = s->retire_ms;
     if (!s->step_ms.empty()) {
         std::vector<float> v = s->step_ms;
         auto pct = [&](double p) {

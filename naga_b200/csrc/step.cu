@@ -1363,17 +1363,27 @@ int tune_k(const StepLaunch& P, cudaStream_t st) {
     for (int bps = 0; bps <= maxr; bps = bps == 0 ? 2 : bps + 1) {
         if ((rc = set_blocks_per_sm(k_rk<L, K, 1>, s4, bps))) break;
         const int g = std::min(P.n_fluid, (bps > 0 ? bps : maxr) * sms);
-        for (int r = 0; r < 2; ++r) k_rk<L, K, 1><<<g, kBlockMT, s4, st>>>(P.fluid, P.n_fluid, P.scenes);
-        cudaEventRecord(e0, st);
-        for (int r = 0; r < 5; ++r) k_rk<L, K, 1><<<g, kBlockMT, s4, st>>>(P.fluid, P.n_fluid, P.scenes);
-        cudaEventRecord(e1, st);
-        if (cudaEventSynchronize(e1) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+        // one untimed and one timed launch; launches shorter than ~0.4 ms
+        // are timed again over enough repetitions to span ~2 ms (a large
+        // batch costs two launches per candidate)
+        auto timed = [&](int reps, float* ms) -> bool {
+            cudaEventRecord(e0, st);
+            for (int r = 0; r < reps; ++r) k_rk<L, K, 1><<<g, kBlockMT, s4, st>>>(P.fluid, P.n_fluid, P.scenes);
+            cudaEventRecord(e1, st);
+            if (cudaEventSynchronize(e1) != cudaSuccess || cudaGetLastError() != cudaSuccess) return false;
+            cudaEventElapsedTime(ms, e0, e1);
+            *ms /= reps;
+            return true;
+        };
+        k_rk<L, K, 1><<<g, kBlockMT, s4, st>>>(P.fluid, P.n_fluid, P.scenes);
+        float ms = 0.f;
+        bool ok = timed(1, &ms);
+        if (ok && ms < 0.4f) ok = timed(std::min(8, std::max(2, (int)(2.f / std::max(ms, 1e-3f)))), &ms);
+        if (!ok) {
             rc = set_error(NAGA_ECUDA, "launch-shape tuning: a trial launch failed");
             break;
         }
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, e0, e1);
-        std::snprintf(line, sizeof line, " %d:%.1fus", bps, ms * 1000.f / 5);
+        std::snprintf(line, sizeof line, " %d:%.1fus", bps, ms * 1000.f);
         log += line;
         // a fixed carveout must beat the default by 3% to be kept: it also
         // binds the other gather kernels, whose best split may differ

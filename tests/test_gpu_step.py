@@ -107,6 +107,36 @@ def test_batch_equals_individual_scenes(naga, oracle):
     b.close()
 
 
+def test_batch_membership_changes(naga, oracle):
+    """Scenes leave and join a stepping batch (its item tables are rebuilt
+    in place on the device); every scene's trace still equals the same
+    scene stepped alone for the same number of steps."""
+    gs = [naga.generate_grid(2, n, 3, s) for n, s in ((25, 1), (33, 2), (41, 3), (29, 4))]
+
+    def make(g):
+        s = naga.Scene(g, k=16, probes=PROBES2)
+        s.set_density(naga.gaussian_pulse(g["points"], [0.5, 0.5], 1e-3, 0.07))
+        return s
+
+    members = [make(g) for g in gs]
+    b = naga.Batch(2)
+    for s in members[:3]:
+        b.add(s)
+    b.step(10)
+    b.remove(members[1])
+    b.step(10)
+    b.add(members[3])
+    b.step(10)
+    members[1].step(5)  # stepped alone after leaving
+    steps = [30, 15, 30, 10]
+    for g, m, n in zip(gs, members, steps):
+        solo = make(g)
+        solo.step(n)
+        assert np.array_equal(solo.probes(0, n), m.probes(0, n))
+        assert np.array_equal(solo.state()[0], m.state()[0])
+    b.close()
+
+
 def test_step_is_deterministic(naga, oracle):
     a, _, g = pair(naga, oracle, 3, 14, 3)
     b = naga.Scene(g, k=32, shape=0, probes=PROBES3)
