@@ -1176,12 +1176,13 @@ int allow_smem(Kern kern, size_t bytes) {
 }
 
 // resident blocks per SM of a kernel at its launch shape (occupancy
-// calculator, cached per kernel)
+// calculator). The answer depends on the shared-memory carveout set on the
+// kernel, so it is cached per kernel, shared memory and applied shape bps
 template <class Kern>
-int resident_blocks(Kern kern, int block, size_t smem) {
+int resident_blocks(Kern kern, int block, size_t smem, int bps) {
     static std::mutex mu;
-    static std::map<std::pair<const void*, size_t>, int> cache;
-    const auto key = std::make_pair(reinterpret_cast<const void*>(kern), smem);
+    static std::map<std::tuple<const void*, size_t, int>, int> cache;
+    const auto key = std::make_tuple(reinterpret_cast<const void*>(kern), smem, bps);
     std::lock_guard<std::mutex> lk(mu);
     auto f = cache.find(key);
     if (f != cache.end()) return f->second;
@@ -1292,7 +1293,7 @@ int enqueue_step_k(const StepLaunch& P, cudaStream_t st) {
     const int bps = tuned_bps(shape_key(L::D, K, KB, P.n_fluid));
     if ((rc = apply_shape<L, K, KB>(bps))) return rc;
     auto pgrid = [&](auto kern, size_t smem, int n) {
-        int r = resident_blocks(kern, kBlockMT, smem);
+        int r = resident_blocks(kern, kBlockMT, smem, bps);
         if (bps > 0 && bps < r) r = bps;
         const int g = r * sms;
         return n < g ? n : g;
