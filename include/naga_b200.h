@@ -275,6 +275,10 @@ int naga_scene_size(const naga_scene* scene, int64_t* n_nodes, int* q);
 typedef struct naga_batch naga_batch;
 
 int naga_batch_create(int dim, naga_batch** out);
+/* priority 1 creates the batch stream at the device's highest stream
+ * priority, so its steps run ahead of work queued on other streams (scene
+ * set-up); 0 is naga_batch_create                                         */
+int naga_batch_create_with_priority(int dim, int priority, naga_batch** out);
 int naga_batch_destroy(naga_batch* batch);
 /* membership changes take effect at the next naga_batch_step             */
 int naga_batch_add(naga_batch* batch, naga_scene* scene);
@@ -308,7 +312,10 @@ typedef struct naga_server_config {
     int dim;               /* lattice of every request                       */
     int steps_per_tick;    /* steps per tick (>= 1)                          */
     int max_active;        /* scene slots, 0 = limited by memory only        */
-    int _reserved;
+    int step_priority;     /* 0: the batch's steps and admissions' set-up
+                              share the device (more admissions); 1: steps
+                              first (naga_batch_create_with_priority): lower
+                              step latency, slower admission                */
     int64_t memory_budget; /* device bytes the active scenes may hold        */
 } naga_server_config;
 

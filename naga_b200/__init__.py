@@ -93,6 +93,7 @@ _SIGS = {
     "naga_scene_device_bytes": ([C.c_void_p], C.c_int64),
     "naga_scene_size": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "naga_batch_create": ([C.c_int, C.c_void_p], C.c_int),
+    "naga_batch_create_with_priority": ([C.c_int, C.c_int, C.c_void_p], C.c_int),
     "naga_batch_destroy": ([C.c_void_p], C.c_int),
     "naga_batch_add": ([C.c_void_p, C.c_void_p], C.c_int),
     "naga_batch_remove": ([C.c_void_p, C.c_void_p], C.c_int),
@@ -317,10 +318,10 @@ class Scene:
 class Batch:
     """Many scenes of one lattice, stepped together (one launch per kernel)."""
 
-    def __init__(self, dim: int):
+    def __init__(self, dim: int, priority: int = 0):
         self.h = C.c_void_p()
         self.scenes: list[Scene] = []
-        _check(lib().naga_batch_create(dim, C.byref(self.h)))
+        _check(lib().naga_batch_create_with_priority(dim, priority, C.byref(self.h)))
 
     def add(self, s: Scene):
         _check(lib().naga_batch_add(self.h, s.h))
@@ -359,7 +360,7 @@ class Batch:
 # ---------------------------------------------------------------- serving
 class ServerConfig(C.Structure):
     _fields_ = [("dim", C.c_int), ("steps_per_tick", C.c_int), ("max_active", C.c_int),
-                ("_reserved", C.c_int), ("memory_budget", C.c_int64)]
+                ("step_priority", C.c_int), ("memory_budget", C.c_int64)]
 
 
 class ServerStats(C.Structure):
@@ -401,9 +402,10 @@ class Server:
 
     QUEUED, ACTIVE, DONE, FAILED = 0, 1, 2, 3
 
-    def __init__(self, dim: int, memory_budget: int, steps_per_tick: int = 50, max_active: int = 0):
+    def __init__(self, dim: int, memory_budget: int, steps_per_tick: int = 50, max_active: int = 0,
+                 step_priority: int = 0):
         self.h = C.c_void_p()
-        cfg = ServerConfig(dim, steps_per_tick, max_active, 0, memory_budget)
+        cfg = ServerConfig(dim, steps_per_tick, max_active, step_priority, memory_budget)
         _check(lib().naga_server_create(C.byref(cfg), C.byref(self.h)))
         self.n_probes = {}
 

@@ -1049,13 +1049,16 @@ extern "C" int naga_scene_size(const naga_scene* s, int64_t* n, int* q) {
 }
 
 // --------------------------------------------------------------- batches
-extern "C" int naga_batch_create(int dim, naga_batch** out) {
-    if (!out || (dim != 2 && dim != 3)) return set_error(NAGA_EINVAL, "naga_batch_create: bad argument");
+extern "C" int naga_batch_create_with_priority(int dim, int priority, naga_batch** out) {
+    if (!out || (dim != 2 && dim != 3) || (priority != 0 && priority != 1))
+        return set_error(NAGA_EINVAL, "naga_batch_create: bad argument");
     int rc;
     if ((rc = check_device())) return rc;
     auto b = new naga_batch();
     b->dim = dim;
-    cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &hi);
+    cudaError_t e = cudaStreamCreateWithPriority(&b->stream, cudaStreamNonBlocking, priority ? hi : lo);
     if (e != cudaSuccess) {
         delete b;
         return set_error(NAGA_ECUDA, std::string("naga_batch_create: ") + cudaGetErrorString(e));
@@ -1063,6 +1066,8 @@ extern "C" int naga_batch_create(int dim, naga_batch** out) {
     *out = b;
     return NAGA_OK;
 }
+
+extern "C" int naga_batch_create(int dim, naga_batch** out) { return naga_batch_create_with_priority(dim, 0, out); }
 
 extern "C" int naga_batch_destroy(naga_batch* b) {
     if (!b) return NAGA_OK;

@@ -84,11 +84,12 @@ extern "C" int64_t naga_scene_estimate_bytes(const naga_scene_desc* d) {
 
 extern "C" int naga_server_create(const naga_server_config* cfg, naga_server** out) {
     if (!cfg || !out) return set_error(NAGA_EINVAL, "naga_server_create: null argument");
-    if ((cfg->dim != 2 && cfg->dim != 3) || cfg->steps_per_tick < 1 || cfg->memory_budget <= 0 || cfg->max_active < 0)
+    if ((cfg->dim != 2 && cfg->dim != 3) || cfg->steps_per_tick < 1 || cfg->memory_budget <= 0 || cfg->max_active < 0 ||
+        (cfg->step_priority != 0 && cfg->step_priority != 1))
         return set_error(NAGA_EINVAL, "naga_server_create: invalid configuration");
     auto s = std::make_unique<naga_server>();
     s->cfg = *cfg;
-    int rc = naga_batch_create(cfg->dim, &s->batch);
+    int rc = naga_batch_create_with_priority(cfg->dim, cfg->step_priority, &s->batch);
     if (rc) return rc;
     NAGA_CUDA_TRY(cudaEventCreate(&s->ev0));
     NAGA_CUDA_TRY(cudaEventCreate(&s->ev1));

@@ -34,7 +34,8 @@ def test_results_alone_equal_results_in_the_mix(naga):
         alone.append(srv.result(rid))
         srv.close()
     # mixed: staggered arrivals, two slots, so requests join a running batch
-    srv = naga.Server(2, memory_budget=1 << 30, steps_per_tick=10, max_active=2)
+    # (steps ahead of set-up on the device: same results)
+    srv = naga.Server(2, memory_budget=1 << 30, steps_per_tick=10, max_active=2, step_priority=1)
     ids = [srv.submit(reqs[0][0], reqs[0][1], steps[0], k=16, probes=PROBES2)]
     srv.tick()
     srv.tick()

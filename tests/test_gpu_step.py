@@ -87,7 +87,8 @@ def test_config1_probe_trace_500_steps(naga, oracle):
     assert rel_err(gpu.probes(0, 500), po) <= 1e-5
 
 
-def test_batch_equals_individual_scenes(naga, oracle):
+@pytest.mark.parametrize("priority", [0, 1])
+def test_batch_equals_individual_scenes(naga, oracle, priority):
     gs = [naga.generate_grid(2, n, 3, s) for n, s in ((25, 1), (33, 2), (41, 3))]
     solo, members = [], []
     for g in gs:
@@ -95,7 +96,7 @@ def test_batch_equals_individual_scenes(naga, oracle):
             s = naga.Scene(g, k=16, probes=PROBES2)
             s.set_density(naga.gaussian_pulse(g["points"], [0.5, 0.5], 1e-3, 0.08))
             lst.append(s)
-    b = naga.Batch(2)
+    b = naga.Batch(2, priority=priority)
     for s in members:
         b.add(s)
     b.step(25)
