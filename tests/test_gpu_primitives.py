@@ -161,3 +161,61 @@ def test_divergence_stencil_matches_oracle(naga, oracle, dim, shape):
     err = np.abs(_np(W) - oW).max() / np.abs(oW).max()
     assert err < 1e-9
     assert np.abs(_np(delta) - od).max() / od.max() < 1e-14
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_knn_edge_sizes(naga, oracle, dim):
+    """No queries; a source cloud smaller than k (the slots past the n
+    sources hold index 0xffffffff and d2 = +inf, as the oracle; NAGA warns
+    and leaves them unset, nearest_neighbors.cuh:421-425); one source."""
+    import torch
+
+    rng = np.random.default_rng(dim)
+    pts = rng.random((500, dim)).astype(np.float32)
+    idx, d2 = naga.knn(_t(pts), torch.empty((0, dim), device="cuda"), 16)
+    assert tuple(idx.shape) == (0, 16) and tuple(d2.shape) == (0, 16)
+    for n, k in ((5, 16), (1, 4), (16, 16)):
+        src, qry = pts[:n], rng.random((40, dim)).astype(np.float32)
+        idx, d2 = naga.knn(_t(src), _t(qry), k)
+        oi, od = oracle.knn(src, qry, k)
+        assert np.array_equal(_np(idx).view(np.uint32), oi)
+        assert np.array_equal(_np(d2), od)
+        assert (oi[:, n:] == 0xFFFFFFFF).all() and np.isinf(od[:, n:]).all()
+
+
+def test_knn_clouds_ragged(naga, oracle):
+    """Clouds back to back with an empty cloud and clouds smaller than k
+    between full ones: each equals its own search."""
+    rng = np.random.default_rng(11)
+    sizes = [300, 0, 7, 1, 900, 0, 40]
+    clouds = [rng.random((n, 3)).astype(np.float32) for n in sizes]
+    off = np.concatenate([[0], np.cumsum(sizes)])
+    idx, d2 = naga.knn_clouds(_t(np.concatenate(clouds)), off, 32)
+    idx, d2 = _np(idx), _np(d2)
+    for c, pts in enumerate(clouds):
+        if len(pts) == 0:
+            continue
+        oi, od = oracle.knn(pts, pts, 32)
+        assert np.array_equal(idx[off[c]:off[c + 1]].view(np.uint32), oi)
+        assert np.array_equal(d2[off[c]:off[c + 1]], od)
+
+
+def test_inverse_singular_and_empty(naga, oracle):
+    """A matrix with an exactly zero column reports the LAPACK info (the
+    1-based column of the zero pivot) like the oracle; its neighbours in
+    the batch are unaffected; an empty batch is a no-op."""
+    import torch
+
+    rng = np.random.default_rng(3)
+    n = 9
+    A = rng.standard_normal((6, n, n)) + 3 * np.eye(n)
+    A[2, 4, :] = 0.0  # column 5 of matrix 2 (element (i, j) at A[b, j, i])
+    out, info = naga.batched_inverse_f64(_t(A))
+    ref, rinfo = oracle.batched_inverse(A)
+    info = _np(info)
+    assert info[2] == rinfo[2] and info[2] > 0
+    ok = [b for b in range(6) if b != 2]
+    assert (info[ok] == 0).all()
+    assert np.abs(_np(out)[ok] - ref[ok]).max() / np.abs(ref[ok]).max() < 1e-12
+    out0, info0 = naga.batched_inverse_f64(torch.empty((0, n, n), dtype=torch.float64, device="cuda"))
+    assert tuple(out0.shape) == (0, n, n) and tuple(info0.shape) == (0,)

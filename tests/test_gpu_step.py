@@ -266,3 +266,45 @@ def test_density_source_matches_oracle(naga, oracle, dim, n_side, layers, steps)
     gpu.step(5)
     plain.step(5)
     assert np.array_equal(gpu.state()[0], plain.state()[0])
+
+
+def test_batch_of_mixed_stencil_sizes(naga, oracle):
+    """Members with different k take the generic (not fully unrolled)
+    kernels; each still equals the same scene stepped alone."""
+    gs = [naga.generate_grid(2, n, 3, s) for n, s in ((28, 5), (35, 6))]
+    ks = (12, 16)
+
+    def make(g, k):
+        s = naga.Scene(g, k=k, k_boundary=k, probes=PROBES2)
+        s.set_density(naga.gaussian_pulse(g["points"], [0.5, 0.5], 1e-3, 0.07))
+        return s
+
+    members = [make(g, k) for g, k in zip(gs, ks)]
+    b = naga.Batch(2)
+    for s in members:
+        b.add(s)
+    b.step(20)
+    for g, k, m in zip(gs, ks, members):
+        solo = make(g, k)
+        solo.step(20)
+        assert np.array_equal(solo.probes(0, 20), m.probes(0, 20))
+        assert np.array_equal(solo.state()[0], m.state()[0])
+    b.close()
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_scene_without_layer_or_probes_matches_oracle(naga, oracle, dim):
+    """No PML layer (the PML kernels have no work) and no probes."""
+    g = naga.generate_grid(dim, 30 if dim == 2 else 14, 0, 9)
+    assert g["n_layer"] == 0
+    k = 16 if dim == 2 else 32
+    shape = 1 if dim == 2 else 0
+    gpu = naga.Scene(g, k=k, shape=shape)
+    orc = oracle.Scene(dim, g["points"], g["n_bulk"], 0, g["n_boundary"], g["normals"], g["sigma"], g["h"],
+                       k=k, shape=shape)
+    drho = naga.gaussian_pulse(g["points"], [0.5] * dim, 1e-3, 0.1)
+    gpu.set_density(drho)
+    orc.set_density(drho)
+    gpu.step(4)
+    orc.step(4)
+    assert rel_err(gpu.state()[0], orc.state()[0]) < 1e-5
