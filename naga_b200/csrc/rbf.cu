@@ -346,6 +346,112 @@ __global__ void batch_mean_kernel(const double* __restrict__ nn, int64_t n, int6
 
 namespace {
 
+// Per-node pieces shared by the two build kernels. One warp per node i:
+// the support coordinates, shifted to x_i and divided by the spacing, go to
+// xs (shared); lane t keeps support index t (and t + 32) and its squared
+// distance; delta is the interaction radius 0.05 |x_i - x_nn|
+// (operators.cuh:84-117).
+template <int D>
+struct NodeStencil {
+    uint32_t jl[2];
+    double r2own[2];
+    double delta, sp;
+};
+template <int D>
+__device__ __forceinline__ NodeStencil<D> load_node(const float* __restrict__ pts, const uint32_t* __restrict__ idx,
+                                                    int k, int64_t i, double sp, double* xs) {
+    const int lane = lane_id();
+    NodeStencil<D> ns;
+    ns.sp = sp;
+    double xi[D];
+#pragma unroll
+    for (int d = 0; d < D; ++d) xi[d] = (double)pts[i * D + d];
+    ns.jl[0] = ns.jl[1] = 0;
+    ns.r2own[0] = ns.r2own[1] = 0;
+    for (int t = lane, r = 0; t < k; t += 32, ++r) {
+        const uint32_t j = idx[i * k + t];
+        ns.jl[r] = j;
+        double rr = 0;
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            const double xj = (double)pts[(int64_t)j * D + d];
+            xs[t * D + d] = (xj - xi[d]) / sp;
+            rr += (xj - xi[d]) * (xj - xi[d]);
+        }
+        ns.r2own[r] = rr;
+    }
+    ns.delta = 0.05 * sqrt(__shfl_sync(kFull, ns.r2own[0], 1));
+    __syncwarp();
+    return ns;
+}
+
+// right-hand sides b_d = sum_q alpha_d(q) w_q G_x(q), rows lane / lane + 32,
+// from the delta = 1 table: x_q = delta u_q / h, alpha_d w_q = K_qd / delta;
+// cself_d = sum_q alpha_d w_q (the [s = 0] term of the weight)
+template <int D>
+__device__ __forceinline__ void quad_rhs(const double* xs, int k, int nsys, int shape, const NodeStencil<D>& ns,
+                                         double* b0, double* b1, double* cself) {
+    constexpr int nq = D == 2 ? 16 : 64;
+    const int lane = lane_id();
+    const QuadTable& tq = g_quad[D - 2];
+    const double rdel = 1.0 / ns.delta, us = ns.delta / ns.sp;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        b0[d] = b1[d] = 0;
+        cself[d] = tq.ksum[d] * rdel;
+    }
+#pragma unroll 4
+    for (int q = 0; q < nq; ++q) {
+        double xq[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) xq[d] = us * tq.u[q][d];
+        const double g0 = lane < nsys ? gx_row<D>(xs, k, shape, xq, lane) : 0.0;
+        const double g1 = lane + 32 < nsys ? gx_row<D>(xs, k, shape, xq, lane + 32) : 0.0;
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            const double aw = tq.K[q][d] * rdel;
+            b0[d] += aw * g0;
+            b1[d] += aw * g1;
+        }
+    }
+}
+
+// filter weights and the stencil records of node i (weights W0: support
+// lane, W1: support lane + 32)
+template <int D>
+__device__ __forceinline__ void write_node(const StencilOut& out, int64_t i, int k, const NodeStencil<D>& ns,
+                                           const double* W0, const double* W1) {
+    const int lane = lane_id();
+    // selective-filter weights: normalised Gaussian of the distance
+    // (detail/simulation_engine.cuh:1233-1323), computed once
+    double fw0 = 0, fw1 = 0;
+    if (out.Ff || (D == 2 && out.Wf)) {
+        const double inv2s2 = 0.5 / (out.filter_sigma * out.filter_sigma);
+        fw0 = lane < k ? exp(-ns.r2own[0] * inv2s2) : 0.0;
+        fw1 = lane + 32 < k ? exp(-ns.r2own[1] * inv2s2) : 0.0;
+        const double tot = warp_sum(fw0 + fw1);
+        fw0 /= tot;
+        fw1 /= tot;
+    }
+    for (int r = 0; r < 2; ++r) {
+        const int t = lane + 32 * r;
+        if (t >= k) break;
+        const double* Wt = r == 0 ? W0 : W1;
+        if (out.W64)
+#pragma unroll
+            for (int d = 0; d < D; ++d) out.W64[(i * k + t) * D + d] = Wt[d];
+        const int64_t at = out.npb > 0 ? pass_record(i, t, k, out.split, out.n_total, out.npb) : i * k + t;
+        if (out.Wf) {
+            const float fz = D == 3 ? (float)Wt[D - 1] : (float)(r == 0 ? fw0 : fw1);
+            out.Wf[at] = make_float4((float)Wt[0], (float)Wt[1], fz, __uint_as_float(ns.jl[r]));
+        }
+        if (out.Ff) out.Ff[at] = make_float2((float)(r == 0 ? fw0 : fw1), __uint_as_float(ns.jl[r]));
+    }
+    if (out.delta && lane == 0) out.delta[i] = ns.delta;
+}
+
+// Any k and both precisions: G0 column-major, factored by warp_lu, the D
+// right-hand sides solved one after the other.
 template <int D>
 __global__ void divergence_build_kernel(const float* __restrict__ pts, int64_t n, const uint32_t* __restrict__ idx,
                                         int k, const double* __restrict__ spacing, int64_t spacing_batch,
@@ -354,54 +460,12 @@ __global__ void divergence_build_kernel(const float* __restrict__ pts, int64_t n
     extern __shared__ __align__(16) unsigned char smem[];
     const int w = threadIdx.x >> 5, lane = lane_id();
     const int nsys = k + D + 1;
-    const int nq = D == 2 ? 16 : 64;
     WarpSmem s = carve(smem + rbf_smem_per_warp(nsys, k, D, precision) * w, nsys, k, D, precision);
     for (int64_t i = (int64_t)blockIdx.x * wpb + w; i < n; i += (int64_t)gridDim.x * wpb) {
-        double xi[D];
-#pragma unroll
-        for (int d = 0; d < D; ++d) xi[d] = (double)pts[i * D + d];
-        const double sp = spacing[i / spacing_batch];
-        uint32_t jl[2] = {0, 0};
-        double r2own[2] = {0, 0};
-        for (int t = lane, r = 0; t < k; t += 32, ++r) {
-            const uint32_t j = idx[i * k + t];
-            jl[r] = j;
-            double rr = 0;
-#pragma unroll
-            for (int d = 0; d < D; ++d) {
-                const double xj = (double)pts[(int64_t)j * D + d];
-                s.xs[t * D + d] = (xj - xi[d]) / sp;
-                rr += (xj - xi[d]) * (xj - xi[d]);
-            }
-            r2own[r] = rr;
-        }
-        // interaction radius delta_i = 0.05 |x_i - x_nn| (operators.cuh:84-117)
-        const double delta = 0.05 * sqrt(__shfl_sync(kFull, r2own[0], 1));
-        __syncwarp();
+        const NodeStencil<D> ns = load_node<D>(pts, idx, k, i, spacing[i / spacing_batch], s.xs);
         build_G0<D>(s.xs, k, shape, s.G);
-        // right-hand sides b_d = sum_q alpha_d(q) w_q G_x(q), rows lane / lane+32,
-        // from the delta = 1 table: x_q = delta u_q / h, alpha_d w_q = K_qd / delta
-        const QuadTable& tq = g_quad[D - 2];
         double b0[D], b1[D], cself[D];
-        const double rdel = 1.0 / delta, us = delta / sp;
-#pragma unroll
-        for (int d = 0; d < D; ++d) {
-            b0[d] = b1[d] = 0;
-            cself[d] = tq.ksum[d] * rdel;
-        }
-        for (int q = 0; q < nq; ++q) {
-            double xq[D];
-#pragma unroll
-            for (int d = 0; d < D; ++d) xq[d] = us * tq.u[q][d];
-            const double g0 = lane < nsys ? gx_row<D>(s.xs, k, shape, xq, lane) : 0.0;
-            const double g1 = lane + 32 < nsys ? gx_row<D>(s.xs, k, shape, xq, lane + 32) : 0.0;
-#pragma unroll
-            for (int d = 0; d < D; ++d) {
-                const double aw = tq.K[q][d] * rdel;
-                b0[d] += aw * g0;
-                b1[d] += aw * g1;
-            }
-        }
+        quad_rhs<D>(s.xs, k, nsys, shape, ns, b0, b1, cself);
         const int info = factor(s, nsys, precision);
         if (info) atomicOr(status, 2);
         double W0[D], W1[D];
@@ -425,32 +489,239 @@ __global__ void divergence_build_kernel(const float* __restrict__ pts, int64_t n
                 W1[d] = x1;
             }
         }
-        // selective-filter weights: normalised Gaussian of the distance
-        // (detail/simulation_engine.cuh:1233-1323), computed once
-        double fw0 = 0, fw1 = 0;
-        if (out.Ff || (D == 2 && out.Wf)) {
-            const double inv2s2 = 0.5 / (out.filter_sigma * out.filter_sigma);
-            fw0 = lane < k ? exp(-r2own[0] * inv2s2) : 0.0;
-            fw1 = lane + 32 < k ? exp(-r2own[1] * inv2s2) : 0.0;
-            const double tot = warp_sum(fw0 + fw1);
-            fw0 /= tot;
-            fw1 /= tot;
-        }
-        for (int r = 0; r < 2; ++r) {
-            const int t = lane + 32 * r;
-            if (t >= k) break;
-            const double* Wt = r == 0 ? W0 : W1;
-            if (out.W64)
+        write_node<D>(out, i, k, ns, W0, W1);
+        __syncwarp();
+    }
+}
+
+// ---- fixed stencil size, FP64: the augmented system [G0 | b_1 .. b_D] is
+// factored in place, row-major with a padded row stride, so the forward
+// substitution rides along with the elimination and one back substitution
+// serves the D right-hand sides. Pivoting is warp_lu's (first maximal |a|
+// of the column, rows swapped whole), the updates are the same operations
+// in the same order; the back substitution multiplies by the pivot's
+// reciprocal (computed once per column) instead of dividing.
+template <int D, int KC>
+struct AugSize {
+    static constexpr int N = KC + D + 1;              // system size
+    static constexpr int NC = (N + D + 1) / 2 * 2;    // columns with the right-hand sides, even
+    static constexpr int LD = NC % 4 == 2 ? NC : NC + 2;  // row stride: 16-B rows, lanes' rows on distinct banks
+    static constexpr int OFF = N > 32 ? N - 32 : 0;   // lane l owns row OFF + l, lanes < OFF also row l
+    // per-warp block, a multiple of 128 B so every warp's rows stay 16-B aligned
+    static constexpr size_t smem_per_warp = (sizeof(double) * ((size_t)N * LD + (size_t)KC * D + N) + 127) / 128 * 128;
+};
+static_assert(AugSize<3, 32>::LD % 2 == 0 && AugSize<2, 16>::LD % 2 == 0, "16-B aligned rows");
+static_assert(AugSize<3, 32>::smem_per_warp % 16 == 0 && AugSize<2, 16>::smem_per_warp % 16 == 0, "aligned warps");
+
+// G0 row-major with stride LD (G0 is symmetric, so this is also its transpose)
+template <int D, int KC>
+__device__ __forceinline__ void build_G0_rows(const double* xs, int shape, double* A) {
+    using Z = AugSize<D, KC>;
+    if constexpr (KC == 32) {
+        // RBF block by symmetry: lane l evaluates the pairs (l, l + t mod 32),
+        // t = 0..16, and writes both mirror entries (the t = 16 pairs twice,
+        // with the same value)
+        const int l = lane_id();
+        double xl[D];
 #pragma unroll
-                for (int d = 0; d < D; ++d) out.W64[(i * k + t) * D + d] = Wt[d];
-            const int64_t at = out.npb > 0 ? pass_record(i, t, k, out.split, out.n_total, out.npb) : i * k + t;
-            if (out.Wf) {
-                const float fz = D == 3 ? (float)Wt[D - 1] : (float)(r == 0 ? fw0 : fw1);
-                out.Wf[at] = make_float4((float)Wt[0], (float)Wt[1], fz, __uint_as_float(jl[r]));
+        for (int d = 0; d < D; ++d) xl[d] = xs[l * D + d];
+#pragma unroll 4
+        for (int t = 0; t <= 16; ++t) {
+            const int c = (l + t) & 31;
+            double r2 = 0;
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                const double u = xl[d] - xs[c * D + d];
+                r2 += u * u;
             }
-            if (out.Ff) out.Ff[at] = make_float2((float)(r == 0 ? fw0 : fw1), __uint_as_float(jl[r]));
+            const double v = shape_fn(r2, shape);
+            A[l * Z::LD + c] = v;
+            A[c * Z::LD + l] = v;
         }
-        if (out.delta && lane == 0) out.delta[i] = delta;
+        // border [1, x] in row / column l, and the zero corner
+        A[l * Z::LD + KC] = 1.0;
+        A[KC * Z::LD + l] = 1.0;
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            A[l * Z::LD + KC + 1 + d] = xl[d];
+            A[(KC + 1 + d) * Z::LD + l] = xl[d];
+        }
+        if (l < (D + 1) * (D + 1)) A[(KC + l / (D + 1)) * Z::LD + KC + l % (D + 1)] = 0.0;
+        return;
+    }
+#pragma unroll 4
+    for (int e = lane_id(); e < Z::N * Z::N; e += 32) {
+        const int r = e / Z::N, c = e % Z::N;
+        double v;
+        if (r >= KC && c >= KC)
+            v = 0.0;
+        else if (r >= KC)
+            v = (r == KC) ? 1.0 : xs[c * D + (r - KC - 1)];
+        else if (c >= KC)
+            v = (c == KC) ? 1.0 : xs[r * D + (c - KC - 1)];
+        else {
+            double r2 = 0;
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                const double t = xs[r * D + d] - xs[c * D + d];
+                r2 += t * t;
+            }
+            v = shape_fn(r2, shape);
+        }
+        A[r * Z::LD + c] = v;
+    }
+}
+
+// row i -= l_i * row j over columns j+1 .. NC-1, l_i = a_ij / a_jj stored
+template <int NC>
+__device__ __forceinline__ void eliminate_row(double* ri, const double* rj, int j, double inv) {
+    const double l = ri[j] * inv;
+    ri[j] = l;
+    int c = j + 1;
+    if (c & 1) {
+        ri[c] -= l * rj[c];
+        ++c;
+    }
+    for (; c < NC; c += 2) {
+        double2 a = *reinterpret_cast<double2*>(ri + c);
+        const double2 b = *reinterpret_cast<const double2*>(rj + c);
+        a.x -= l * b.x;
+        a.y -= l * b.y;
+        *reinterpret_cast<double2*>(ri + c) = a;
+    }
+}
+
+// In-place LU of the augmented rows; rdiag[j] = 1 / u_jj. Returns 0, or
+// j + 1 for the first column whose pivot is exactly zero (left unreduced).
+template <int D, int KC>
+__device__ int aug_lu(double* A, double* rdiag) {
+    using Z = AugSize<D, KC>;
+    constexpr int N = Z::N, LD = Z::LD, OFF = Z::OFF;
+    const int lane = lane_id();
+    const int p1 = OFF + lane;
+    const bool has1 = p1 < N, has2 = lane < OFF;
+    int info = 0;
+    for (int j = 0; j < N; ++j) {
+        double best = -1.0;
+        int bi = N;
+        if (has2 && lane >= j) {
+            best = fabs(A[lane * LD + j]);
+            bi = lane;
+        }
+        if (has1 && p1 >= j) {
+            const double v = fabs(A[p1 * LD + j]);
+            if (v > best) {
+                best = v;
+                bi = p1;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ov = __shfl_xor_sync(kFull, best, o);
+            const int oi = __shfl_xor_sync(kFull, bi, o);
+            if (ov > best || (ov == best && oi < bi)) {
+                best = ov;
+                bi = oi;
+            }
+        }
+        const int p = bi;
+        if (A[p * LD + j] == 0.0) {
+            if (!info) info = j + 1;
+            if (lane == 0) rdiag[j] = 0.0;
+            __syncwarp();
+            continue;
+        }
+        if (p != j)
+            for (int c = lane; c < Z::NC; c += 32) {
+                const double t = A[j * LD + c];
+                A[j * LD + c] = A[p * LD + c];
+                A[p * LD + c] = t;
+            }
+        __syncwarp();
+        const double inv = 1.0 / A[j * LD + j];
+        if (lane == 0) rdiag[j] = inv;
+        if (has1 && p1 > j) eliminate_row<Z::NC>(A + p1 * LD, A + j * LD, j, inv);
+        if (has2 && lane > j) eliminate_row<Z::NC>(A + lane * LD, A + j * LD, j, inv);
+        __syncwarp();
+    }
+    return info;
+}
+
+template <int D, int KC>
+__global__ void divergence_build_fixed_kernel(const float* __restrict__ pts, int64_t n,
+                                              const uint32_t* __restrict__ idx, const double* __restrict__ spacing,
+                                              int64_t spacing_batch, int shape, StencilOut out,
+                                              int* __restrict__ status, int wpb) {
+    using Z = AugSize<D, KC>;
+    constexpr int N = Z::N, LD = Z::LD, OFF = Z::OFF;
+    static_assert(KC <= 32, "one support per lane");
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int w = threadIdx.x >> 5, lane = lane_id();
+    double* A = reinterpret_cast<double*>(smem + Z::smem_per_warp * w);
+    double* xs = A + N * LD;
+    double* rdiag = xs + KC * D;
+    const int p1 = OFF + lane;
+    const bool has1 = p1 < N, has2 = lane < OFF;
+    for (int64_t i = (int64_t)blockIdx.x * wpb + w; i < n; i += (int64_t)gridDim.x * wpb) {
+        const NodeStencil<D> ns = load_node<D>(pts, idx, KC, i, spacing[i / spacing_batch], xs);
+        build_G0_rows<D, KC>(xs, shape, A);
+        double b0[D], b1[D], cself[D];
+        quad_rhs<D>(xs, KC, N, shape, ns, b0, b1, cself);
+        // right-hand-side columns N .. N+D-1 (original row order), zero padding
+        for (int r = 0; r < 2; ++r) {
+            const int row = lane + 32 * r;
+            if (row < N) {
+#pragma unroll
+                for (int d = 0; d < D; ++d) A[row * LD + N + d] = r == 0 ? b0[d] : b1[d];
+                for (int c = N + D; c < Z::NC; ++c) A[row * LD + c] = 0.0;
+            }
+        }
+        __syncwarp();
+        if (aug_lu<D, KC>(A, rdiag)) atomicOr(status, 2);
+        // back substitution, all right-hand sides at once: y1 holds row
+        // OFF + lane, y2 row lane (lanes < OFF)
+        double y1[D], y2[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            y1[d] = has1 ? A[p1 * LD + N + d] : 0.0;
+            y2[d] = has2 ? A[lane * LD + N + d] : 0.0;
+        }
+        for (int j = N - 1; j >= 0; --j) {
+            const double rj = rdiag[j];
+            double xj[D];
+#pragma unroll
+            for (int d = 0; d < D; ++d)
+                xj[d] = (j >= OFF ? __shfl_sync(kFull, y1[d], j - OFF) : __shfl_sync(kFull, y2[d], j)) * rj;
+            if (has1) {
+                if (p1 == j) {
+#pragma unroll
+                    for (int d = 0; d < D; ++d) y1[d] = xj[d];
+                } else if (p1 < j) {
+                    const double u = A[p1 * LD + j];
+#pragma unroll
+                    for (int d = 0; d < D; ++d) y1[d] -= u * xj[d];
+                }
+            }
+            if (has2) {
+                if (lane == j) {
+#pragma unroll
+                    for (int d = 0; d < D; ++d) y2[d] = xj[d];
+                } else if (lane < j) {
+                    const double u = A[lane * LD + j];
+#pragma unroll
+                    for (int d = 0; d < D; ++d) y2[d] -= u * xj[d];
+                }
+            }
+        }
+        // weight of support t = lane: row t sits in lane t - OFF (or in y2)
+        double W0[D], W1[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            const double v = __shfl_sync(kFull, y1[d], (lane - OFF) & 31);
+            W0[d] = (lane >= OFF ? v : y2[d]) + (lane == 0 ? cself[d] : 0.0);
+            W1[d] = 0.0;
+        }
+        write_node<D>(out, i, KC, ns, W0, W1);
         __syncwarp();
     }
 }
@@ -555,11 +826,25 @@ int divergence_build_device(const float* pts, int64_t n, int dim, int k, int sha
         batch_mean_kernel<<<(unsigned)nb, 256, 0, st>>>(nn, n, batch, sp);
         NAGA_CUDA_TRY(cudaGetLastError());
     }
+    auto fixed = [&](auto kern, size_t per_warp) -> int {
+        const int wpb = warps_per_block_for(per_warp);
+        const size_t smem = per_warp * wpb;
+        const int blocks = (int)std::min<int64_t>((n + wpb - 1) / wpb, (int64_t)sm_count() * 32);
+        NAGA_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<blocks, 32 * wpb, smem, st>>>(pts, n, idx, sp, batch, shape, out, d_status, wpb);
+        return NAGA_OK;
+    };
     const size_t per_warp = rbf_smem_per_warp_h(nsys, k, dim, precision);
     const int wpb = warps_per_block_for(per_warp);
     const size_t smem = per_warp * wpb;
     const int blocks = (int)std::min<int64_t>((n + wpb - 1) / wpb, (int64_t)sm_count() * 32);
-    if (dim == 2) {
+    int lrc = NAGA_OK;
+    // FP64 builds of the benchmark stencil sizes take the fixed-size kernel
+    if (precision == 0 && dim == 3 && k == 32) {
+        lrc = fixed(divergence_build_fixed_kernel<3, 32>, AugSize<3, 32>::smem_per_warp);
+    } else if (precision == 0 && dim == 2 && k == 16) {
+        lrc = fixed(divergence_build_fixed_kernel<2, 16>, AugSize<2, 16>::smem_per_warp);
+    } else if (dim == 2) {
         NAGA_CUDA_TRY(cudaFuncSetAttribute(divergence_build_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         divergence_build_kernel<2><<<blocks, 32 * wpb, smem, st>>>(pts, n, idx, k, sp, batch, shape, precision, out,
                                                                    d_status, wpb);
@@ -568,6 +853,7 @@ int divergence_build_device(const float* pts, int64_t n, int dim, int k, int sha
         divergence_build_kernel<3><<<blocks, 32 * wpb, smem, st>>>(pts, n, idx, k, sp, batch, shape, precision, out,
                                                                    d_status, wpb);
     }
+    if (lrc) return lrc;
     NAGA_CUDA_TRY(cudaGetLastError());
     int h_st[2] = {0, 0};
     NAGA_CUDA_TRY(cudaMemcpyAsync(h_st, d_status, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
