@@ -1133,6 +1133,12 @@ extern "C" int64_t naga_tuning_report(char* buf, int64_t cap) {
     return (int64_t)r.size();
 }
 
+extern "C" int naga_selftest_wait_timeout(double limit_ms) {
+    int rc;
+    if ((rc = check_device())) return rc;
+    return wait_selftest(limit_ms, 0);
+}
+
 // --------------------------------------------------------------- profiling
 extern "C" int naga_profile_enable(int on) {
     std::lock_guard<std::mutex> lk(g_prof.mu);

@@ -308,3 +308,19 @@ def test_scene_without_layer_or_probes_matches_oracle(naga, oracle, dim):
     gpu.step(4)
     orc.step(4)
     assert rel_err(gpu.state()[0], orc.state()[0]) < 1e-5
+
+
+def test_bounded_wait_gives_up_and_context_stays_usable(naga, oracle):
+    """A wait on a barrier that nothing completes gives up after its limit
+    (no hang), the host reads NAGA_ETIMEOUT once (the flag is cleared), and
+    the same context then steps a scene to the oracle's trace."""
+    import time
+
+    t0 = time.perf_counter()
+    assert naga.selftest_wait_timeout(20.0) == naga.NAGA_ETIMEOUT
+    assert time.perf_counter() - t0 < 10.0
+    assert "did not complete in time" in naga.lib().naga_last_error().decode()
+    gpu, orc, _ = pair(naga, oracle, 2, 30, 3, width=0.1)
+    gpu.step(5)
+    po = orc.step(5)
+    assert rel_err(gpu.probes(0, 5), po) <= 1e-5
