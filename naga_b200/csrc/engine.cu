@@ -181,6 +181,20 @@ __global__ void concat_items_kernel(const ListCopy* __restrict__ copies, WorkIte
     }
 }
 
+// boundary interpolation records (weight, source index bits) in pass order
+// from the RPIM support indices / weights [nq][kk], and the flag of every
+// node some boundary node interpolates from (idempotent stores)
+__global__ void boundary_records_kernel(const uint32_t* __restrict__ idx, const double* __restrict__ w, int64_t nq,
+                                        int kk, int npb, float2* __restrict__ rec, uint8_t* __restrict__ is_src) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nq * kk) return;
+    const int64_t q = e / kk;
+    const int t = (int)(e - q * kk);
+    const uint32_t j = idx[e];
+    rec[pass_record(q, t, kk, nq, nq, npb)] = make_float2((float)w[e], __uint_as_float(j));
+    is_src[j] = 1;
+}
+
 // flag[w] = 1 when a node of item w has a stencil support in the layer
 // [nb, nb + nl) (idx: node-major [n][k] kNN indices)
 __global__ void layer_touch_kernel(const uint32_t* __restrict__ idx, int k, const WorkItem* __restrict__ items,
@@ -352,7 +366,9 @@ int scene_setup(naga_scene* s) {
 
     // boundary interpolation: kNN among bulk + layer, RPIM at the boundary
     // node with the nodal spacing (detail/simulation_engine.cuh:223-258)
-    std::vector<uint8_t> is_src(N, 0);
+    uint8_t* dsrc = nullptr;
+    if ((rc = s->alloc(&dsrc, N))) return rc;
+    NAGA_CUDA_TRY(cudaMemsetAsync(dsrc, 0, N, st));
     auto rpim = [&](const float* qry_host, int64_t nq, int64_t nsrc, int kk, uint32_t** idx_out, float** w_out,
                     float2** rec_out) -> int {
         uint32_t* didx = nullptr;
@@ -372,6 +388,24 @@ int scene_setup(naga_scene* s) {
         int r = knn_device(pts, nsrc, dq, nq, D, kk, didx, dd2, st);
         if (!r) r = rbf_weights_device(pts, nsrc, D, didx, kk, dqd, nq, 1, d.nodal_spacing, d.shape,
                                        d.weight_precision, dw, st);
+        if (!r && rec_out) {
+            // boundary: records and source flags built on the device
+            r = s->alloc(rec_out, nq * kk);
+            if (!r) {
+                const int64_t ne = nq * kk;
+                boundary_records_kernel<<<(unsigned)((ne + 255) / 256), 256, 0, st>>>(didx, dw, nq, kk, npb, *rec_out,
+                                                                                      dsrc);
+                cudaError_t e = cudaGetLastError();
+                if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+                if (e != cudaSuccess) r = set_error(NAGA_ECUDA, std::string("boundary records: ") + cudaGetErrorString(e));
+            }
+            cudaFreeAsync(didx, st);
+            cudaFreeAsync(dd2, st);
+            cudaFreeAsync(dq, st);
+            cudaFreeAsync(dqd, st);
+            cudaFreeAsync(dw, st);
+            return r;
+        }
         std::vector<uint32_t> hi(nq * kk);
         std::vector<double> hw(nq * kk);
         if (!r) {
@@ -386,7 +420,7 @@ int scene_setup(naga_scene* s) {
         cudaFreeAsync(dqd, st);
         cudaFreeAsync(dw, st);
         if (r) return r;
-        if (idx_out) {
+        {
             // probes: [k][nq] indices and weights
             std::vector<uint32_t> ti(nq * kk);
             std::vector<float> tw(nq * kk);
@@ -399,20 +433,6 @@ int scene_setup(naga_scene* s) {
             if ((r = s->alloc(w_out, nq * kk))) return r;
             NAGA_CUDA_TRY(cudaMemcpyAsync(*idx_out, ti.data(), sizeof(uint32_t) * nq * kk, cudaMemcpyHostToDevice, st));
             NAGA_CUDA_TRY(cudaMemcpyAsync(*w_out, tw.data(), sizeof(float) * nq * kk, cudaMemcpyHostToDevice, st));
-            NAGA_CUDA_TRY(cudaStreamSynchronize(st));
-        } else {
-            // boundary: (weight, index bits) records in pass order
-            std::vector<float2> rec(nq * kk);
-            for (int64_t q = 0; q < nq; ++q)
-                for (int t = 0; t < kk; ++t) {
-                    float2 v;
-                    v.x = (float)hw[q * kk + t];
-                    std::memcpy(&v.y, &hi[q * kk + t], 4);
-                    rec[pass_record(q, t, kk, nq, nq, npb)] = v;
-                    is_src[hi[q * kk + t]] = 1;
-                }
-            if ((r = s->alloc(rec_out, nq * kk))) return r;
-            NAGA_CUDA_TRY(cudaMemcpyAsync(*rec_out, rec.data(), sizeof(float2) * nq * kk, cudaMemcpyHostToDevice, st));
             NAGA_CUDA_TRY(cudaStreamSynchronize(st));
         }
         return NAGA_OK;
@@ -430,10 +450,6 @@ int scene_setup(naga_scene* s) {
     }
     V.pidx = pidx;
     V.pw = pw;
-    uint8_t* dsrc = nullptr;
-    if ((rc = s->alloc(&dsrc, N))) return rc;
-    NAGA_CUDA_TRY(cudaMemcpyAsync(dsrc, is_src.data(), N, cudaMemcpyHostToDevice, st));
-    NAGA_CUDA_TRY(cudaStreamSynchronize(st));
     V.is_src = dsrc;
 
     float* ring = nullptr;
