@@ -376,15 +376,16 @@ int64_t naga_tuning_report(char* buf, int64_t cap);
 
 /* ------------------------------------------------------ failure detection */
 /* Every wait of the step kernels (tile copies into shared memory, on an
- * mbarrier) gives up after 2 s of device time, the kernel returns, and the
- * next naga_scene_sync / naga_batch_sync / step reports NAGA_ETIMEOUT with
- * the context still usable. This call exercises that path on the current
- * device: one wait on a barrier that nothing completes, with a limit of
- * limit_ms (0 < limit_ms <= 1000); it returns NAGA_ETIMEOUT when the wait
- * gave up and the error was reported (and cleared). Run it while no step
- * is in flight: the timeout flag is shared by the device's step kernels.
+ * mbarrier) gives up after a fixed number of polls (about a second on
+ * B200), the kernel returns, and the next naga_scene_sync /
+ * naga_batch_sync / step reports NAGA_ETIMEOUT with the context still
+ * usable. This call exercises that path on the current device: the same
+ * wait, on a barrier that nothing completes, with `polls` polls (0 = the
+ * step kernels' own limit); it returns NAGA_ETIMEOUT when the wait gave up
+ * and the error was reported (and cleared). Run it while no step is in
+ * flight: the timeout flag is shared by the device's step kernels.
  * No NAGA counterpart (NAGA's kernels have no bounded waits).             */
-int naga_selftest_wait_timeout(double limit_ms);
+int naga_selftest_wait_timeout(int polls);
 
 #ifdef __cplusplus
 }

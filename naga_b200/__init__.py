@@ -94,7 +94,7 @@ _SIGS = {
     "naga_scene_size": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "naga_batch_create": ([C.c_int, C.c_void_p], C.c_int),
     "naga_batch_create_with_priority": ([C.c_int, C.c_int, C.c_void_p], C.c_int),
-    "naga_selftest_wait_timeout": ([C.c_double], C.c_int),
+    "naga_selftest_wait_timeout": ([C.c_int], C.c_int),
     "naga_batch_destroy": ([C.c_void_p], C.c_int),
     "naga_batch_add": ([C.c_void_p, C.c_void_p], C.c_int),
     "naga_batch_remove": ([C.c_void_p, C.c_void_p], C.c_int),
@@ -566,11 +566,11 @@ def read_profile() -> dict:
     return {names[i].decode(): (int(launches[i]), float(ms[i])) for i in range(n.value)}
 
 
-def selftest_wait_timeout(limit_ms: float = 20.0) -> int:
-    """Runs one bounded device wait that nothing completes (the failure path
-    of the step kernels' tile pipeline); returns the status, NAGA_ETIMEOUT
+def selftest_wait_timeout(polls: int = 0) -> int:
+    """Runs the step kernels' bounded device wait on a barrier that nothing
+    completes (0 polls = their own limit); returns the status, NAGA_ETIMEOUT
     when the wait gave up and was reported."""
-    return int(lib().naga_selftest_wait_timeout(float(limit_ms)))
+    return int(lib().naga_selftest_wait_timeout(int(polls)))
 
 
 def tuning_report() -> str:

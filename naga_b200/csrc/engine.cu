@@ -1149,10 +1149,10 @@ extern "C" int64_t naga_tuning_report(char* buf, int64_t cap) {
     return (int64_t)r.size();
 }
 
-extern "C" int naga_selftest_wait_timeout(double limit_ms) {
+extern "C" int naga_selftest_wait_timeout(int polls) {
     int rc;
     if ((rc = check_device())) return rc;
-    return wait_selftest(limit_ms, 0);
+    return wait_selftest(polls, 0);
 }
 
 // --------------------------------------------------------------- profiling

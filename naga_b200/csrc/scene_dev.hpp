@@ -143,7 +143,7 @@ int kernel_count();
 int tile_timeout_check(cudaStream_t st);
 // a bounded wait that nothing completes, then tile_timeout_check (expects
 // NAGA_ETIMEOUT): the failure path of the step kernels' tile pipeline
-int wait_selftest(double limit_ms, cudaStream_t st);
+int wait_selftest(int polls, cudaStream_t st);
 // G rows of the rest state plus a density perturbation (device drho [n],
 // or null for the rest state)
 int density_rows_device(int dim, const float* drho, int64_t n, float* G, cudaStream_t st);
