@@ -336,7 +336,8 @@ int scene_setup(naga_scene* s) {
     out.Wf = W;
     V.stW = W;
     V.stF = nullptr;
-    if (D == 3) {
+    {
+        // (weight, index) records of the selective filter, pass order
         float2* F = nullptr;
         if ((rc = s->alloc(&F, (int64_t)k * N))) return rc;
         NAGA_CUDA_TRY(cudaMemsetAsync(F, 0, sizeof(float2) * k * N, st));
@@ -1002,7 +1003,7 @@ extern "C" int naga_scene_read_tables(naga_scene* s, uint32_t* idx, float* W, fl
     const int k = s->desc.k, D = s->dim, npb = nodes_per_pass(D);
     const int64_t N = s->N;
     // the device tables are in pass order; the outputs are node-major
-    if (idx || W || (fw && D == 2)) {
+    if (idx || W) {
         std::vector<float4> wv((size_t)k * N);
         NAGA_CUDA_TRY(cudaMemcpy(wv.data(), s->dev.stW, sizeof(float4) * wv.size(), cudaMemcpyDeviceToHost));
         for (int64_t i = 0; i < N; ++i)
@@ -1015,10 +1016,9 @@ extern "C" int naga_scene_read_tables(naga_scene* s, uint32_t* idx, float* W, fl
                     if (D == 3) W[e * D + 2] = r.z;
                 }
                 if (idx) std::memcpy(&idx[e], &r.w, 4);
-                if (fw && D == 2) fw[e] = r.z;
             }
     }
-    if (fw && D == 3) {
+    if (fw) {
         std::vector<float2> fv((size_t)k * N);
         NAGA_CUDA_TRY(cudaMemcpy(fv.data(), s->dev.stF, sizeof(float2) * fv.size(), cudaMemcpyDeviceToHost));
         for (int64_t i = 0; i < N; ++i)

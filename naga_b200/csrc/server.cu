@@ -70,7 +70,7 @@ extern "C" int64_t naga_scene_estimate_bytes(const naga_scene_desc* d) {
     if (!d || (d->dim != 2 && d->dim != 3)) return -1;
     const int64_t N = d->n_bulk + d->n_layer + d->n_boundary + d->n_ghost;
     const int64_t QP = d->dim == 2 ? D2Q9::QP : D3Q27::QP;
-    const int64_t rec = d->dim == 3 ? 16 : 12;
+    const int64_t rec = 16;  // float4 stencil records (plus 8-B filter records below)
     int64_t b = N * (7 * QP * 4 + 16 + 1 + (int64_t)d->k * (rec + 8 + 4) + 4 * d->dim);
     b += (int64_t)d->n_boundary * d->k_boundary * 8 + (int64_t)d->n_probes * d->k_probe * 8;
     b += ((N + 127) / 128) * 2 * QP * 8 + (int64_t)std::max(1, d->probe_capacity) * std::max(1, d->n_probes) * 4;

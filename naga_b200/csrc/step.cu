@@ -776,18 +776,11 @@ struct PmlSrc {  // PML gather records (see pml_table_kernel)
         return {sc.stP + (int64_t)w.begin * k, (uint32_t)((w.end - w.begin) * k * sizeof(float4))};
     }
 };
-struct FilterSrc {  // D3Q27 filter records of the item's bulk/layer nodes
+struct FilterSrc {  // filter records of the item's bulk/layer nodes
     __device__ TileSrc operator()(const SceneDev& sc, const WorkItem& w) const {
         const int k = sc.k;
         const int64_t nf = (int64_t)w.begin < sc.nbl ? (int64_t)w.end - w.begin : 0;
         return {sc.stF + (int64_t)w.begin * k, (uint32_t)(nf * k * sizeof(float2))};
-    }
-};
-struct FilterSrc2 {  // D2Q9: the stencil records carry the filter weights
-    __device__ TileSrc operator()(const SceneDev& sc, const WorkItem& w) const {
-        const int k = sc.k;
-        const int64_t nf = (int64_t)w.begin < sc.nbl ? (int64_t)w.end - w.begin : 0;
-        return {sc.stW + (int64_t)w.begin * k, (uint32_t)(nf * k * sizeof(float4))};
     }
 };
 struct EdgeSrc {  // boundary interpolation records
@@ -895,10 +888,9 @@ __global__ void __launch_bounds__(kBlockMT) k_filter(const WorkItem* __restrict_
                                                      const SceneDev* __restrict__ scenes) {
     using G = MT<L>;
     constexpr int QP = L::QP, K_ = K;
-    // D3Q27: (weight, index) filter records; D2Q9: the stencil records,
-    // whose z and w carry the filter weight and the index
-    using T = typename std::conditional<L::D == 3, float2, float4>::type;
-    using Src = typename std::conditional<L::D == 3, FilterSrc, FilterSrc2>::type;
+    // (weight, index) filter records, 8 B each
+    using T = float2;
+    using Src = FilterSrc;
     const int c = threadIdx.x % G::TPN, ns = threadIdx.x / G::TPN;
     float d0[3], d1[3];
     pair_dirs<L>(c < G::NCH ? c : 0, d0, d1);
@@ -913,12 +905,7 @@ __global__ void __launch_bounds__(kBlockMT) k_filter(const WorkItem* __restrict_
             float4 sum = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll 8
             for (int s = 0; s < k; ++s) {
-                const T rt = tile[s * nn + ns];
-                float2 r;
-                if constexpr (L::D == 3)
-                    r = rt;
-                else
-                    r = make_float2(rt.z, rt.w);
+                const float2 r = tile[s * nn + ns];
                 const float4 v = ld4g<L>(S.S1, __float_as_uint(r.y), c);
                 sum.x = fmaf(r.x, v.x - f.x, sum.x);
                 sum.y = fmaf(r.x, v.y - f.y, sum.y);
@@ -1287,7 +1274,7 @@ int apply_shape(int bps) {
     int& applied = AppliedShape<L, K, KB>::bps;
     std::lock_guard<std::mutex> lk(g_shape_mu);
     if (applied == bps) return NAGA_OK;
-    using TF = typename std::conditional<L::D == 3, float2, float4>::type;
+    using TF = float2;  // filter records
     const size_t s4 = tile_bytes<L, K, float4>(), s2 = tile_bytes<L, K, TF>(), sb = tile_bytes<L, KB, float2>();
     int rc;
     if ((rc = set_blocks_per_sm(k_pml_gather<L, K>, s4, bps)) || (rc = set_blocks_per_sm(k_rk<L, K, 1>, s4, bps)) ||
@@ -1303,7 +1290,7 @@ int apply_shape(int bps) {
 template <class L, int K, int KB>
 int enqueue_step_k(const StepLaunch& P, cudaStream_t st) {
     const int cap = sm_count() * 8;
-    using TF = typename std::conditional<L::D == 3, float2, float4>::type;  // filter records
+    using TF = float2;  // filter records
     const size_t s4 = tile_bytes<L, K, float4>(), s2 = tile_bytes<L, K, TF>(), sb = tile_bytes<L, KB, float2>();
     int rc;
     if ((rc = allow_smem(k_pml_gather<L, K>, s4)) || (rc = allow_smem(k_rk<L, K, 1>, s4)) ||
