@@ -455,8 +455,10 @@ __device__ __forceinline__ void load_scene(SceneDev& dst, const SceneDev* src) {
 //   ghost:      S1 = g + collision.
 // The item's rows of G and Q1_prev are staged in shared memory by coalesced
 // loads of the whole block before the (register-heavy) per-node work.
+// D3Q27 runs 4 blocks/SM (its collision needs the registers; tighter bounds
+// spill and were slower); D2Q9 fits 8 (one resident wave of the item grid)
 template <class L>
-__global__ void __launch_bounds__(kBlock, 4) k_macro_pml(const WorkItem* __restrict__ items, int nitems,
+__global__ void __launch_bounds__(kBlock, (L::D == 3 ? 4 : 8)) k_macro_pml(const WorkItem* __restrict__ items, int nitems,
                                                          const SceneDev* __restrict__ scenes) {
     constexpr int Q = L::Q, QP = L::QP;
     // rows of the item's nodes: G and Q1_prev in, then the layer terms
