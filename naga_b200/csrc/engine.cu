@@ -364,6 +364,12 @@ int scene_setup(naga_scene* s) {
     V.PHI = phi;
     V.PV = pv;
     V.stP = stp;
+    float* str = nullptr;
+    if (D == 2) {
+        if ((rc = s->alloc(&str, 3 * (int64_t)k * N))) return rc;
+        if ((rc = compact_records_device(W, (int64_t)k * N, str, st))) return rc;
+    }
+    V.stR = str;
 
     // boundary interpolation: kNN among bulk + layer, RPIM at the boundary
     // node with the nodal spacing (detail/simulation_engine.cuh:223-258)

@@ -60,6 +60,7 @@ struct SceneDev {
     // tables
     const float4* stW;
     const float4* stP;  // PML gather records, pass order (Wx, Wy, Wz or 0, PHI row bits)
+    const float* stR;   // D2Q9: the stencil records compacted to (Wx, Wy, index bits), pass order
     const float4* PV;  // [nbl][2]: (V1, V2) = sum over layer supports of W_s sigma_j, W_s sigma_j^2
     const float2* stF;
     const float* sigma;
@@ -152,6 +153,8 @@ int density_rows_device(int dim, const float* drho, int64_t n, float* G, cudaStr
 int tune_step_shapes(int dim, int k, int kb, const StepLaunch& P, cudaStream_t st);
 // the tuner's measurements, one line per tuned shape
 std::string tuning_report();
+// D2Q9: (Wx, Wy, index) triplets of the pass-ordered stencil records
+int compact_records_device(const float4* stW, int64_t count, float* stR, cudaStream_t st);
 // the PML gather records of a scene (stW in pass order)
 int pml_table_device(int dim, const float4* stW, int64_t nb, int64_t nl, int64_t nbl, int64_t n, int k, float4* stP,
                      cudaStream_t st);

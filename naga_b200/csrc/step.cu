@@ -772,6 +772,12 @@ struct StencilSrc {  // divergence stencil (Wx, Wy, Wz | filter weight, index)
         return {sc.stW + (int64_t)w.begin * k, (uint32_t)((w.end - w.begin) * k * sizeof(float4))};
     }
 };
+struct CompactSrc {  // D2Q9 stencil triplets (Wx, Wy, index)
+    __device__ TileSrc operator()(const SceneDev& sc, const WorkItem& w) const {
+        const int k = sc.k;
+        return {sc.stR + (int64_t)w.begin * k * 3, (uint32_t)((w.end - w.begin) * k * 3 * sizeof(float))};
+    }
+};
 struct PmlSrc {  // PML gather records (see pml_table_kernel)
     __device__ TileSrc operator()(const SceneDev& sc, const WorkItem& w) const {
         const int k = sc.k;
@@ -959,11 +965,16 @@ template <class L, int K, int STAGE>
 __global__ void __launch_bounds__(kBlockMT) k_rk(const WorkItem* __restrict__ items, int nitems,
                                                  const SceneDev* __restrict__ scenes) {
     using G = MT<L>;
-    constexpr int QP = L::QP, K_ = K;
+    // D3Q27 tiles hold (Wx, Wy, Wz, index) records; D2Q9 tiles the
+    // (Wx, Wy, index) triplets, three floats per record
+    constexpr bool D2 = L::D == 2;
+    using T = typename std::conditional<D2, float, float4>::type;
+    constexpr int QP = L::QP, K_ = D2 ? 3 * K : K;
+    using Src = typename std::conditional<D2, CompactSrc, StencilSrc>::type;
     const int c = threadIdx.x % G::TPN, ns = threadIdx.x / G::TPN;
     float d0[3], d1[3];
     pair_dirs<L>(c < G::NCH ? c : 0, d0, d1);
-    NAGA_PIPE_BEGIN(float4, (tile_cap<G::NPB, K>()), StencilSrc{})
+    NAGA_PIPE_BEGIN(T, ((D2 ? 3 : 1) * tile_cap<G::NPB, K>()), Src{})
     const int k = K > 0 ? K : S.k;
     const int nn = (int)(it.end - it.begin);
     const int64_t i = (int64_t)it.begin + ns;
@@ -977,7 +988,13 @@ __global__ void __launch_bounds__(kBlockMT) k_rk(const WorkItem* __restrict__ it
         float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll 16
         for (int s = 0; s < k; ++s) {
-            const float4 rec = tile[s * nn + ns];
+            float4 rec;
+            if constexpr (D2) {
+                const float* t3 = reinterpret_cast<const float*>(tile) + 3 * (s * nn + ns);
+                rec = make_float4(t3[0], t3[1], 0.f, t3[2]);
+            } else {
+                rec = reinterpret_cast<const float4*>(tile)[s * nn + ns];
+            }
             const uint32_t j = __float_as_uint(rec.w);
             const float wz = L::D == 3 ? rec.z : 0.f;
             const float4 v = ld4g<L>(src, j, c);
@@ -1100,6 +1117,24 @@ __global__ void pml_table_kernel(const float4* __restrict__ stW, int64_t nb, int
     for (; o < k; ++o) stP[pass_record(i, o, k, nbl, n, npb)] = make_float4(0.f, 0.f, 0.f, __uint_as_float(last));
 }
 }  // namespace
+
+namespace {
+__global__ void compact_records_kernel(const float4* __restrict__ stW, int64_t count, float* __restrict__ stR) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= count) return;
+    const float4 r = stW[e];
+    stR[3 * e] = r.x;
+    stR[3 * e + 1] = r.y;
+    stR[3 * e + 2] = r.w;
+}
+}  // namespace
+
+int compact_records_device(const float4* stW, int64_t count, float* stR, cudaStream_t st) {
+    if (count <= 0) return NAGA_OK;
+    compact_records_kernel<<<(unsigned)((count + 255) / 256), 256, 0, st>>>(stW, count, stR);
+    NAGA_CUDA_TRY(cudaGetLastError());
+    return NAGA_OK;
+}
 
 int pml_table_device(int dim, const float4* stW, int64_t nb, int64_t nl, int64_t nbl, int64_t n, int k, float4* stP,
                      cudaStream_t st) {
