@@ -195,6 +195,18 @@ __global__ void boundary_records_kernel(const uint32_t* __restrict__ idx, const 
     is_src[j] = 1;
 }
 
+// the largest layer-support count of each PML item's nodes (the count of
+// node i rides in the bits of PV[2 i].w): the item's PML tile only needs
+// that many records per node
+__global__ void pml_item_kmax_kernel(const WorkItem* __restrict__ items, int n, const float4* __restrict__ PV,
+                                     uint32_t* __restrict__ kmax) {
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= n) return;
+    uint32_t m = 0;
+    for (uint32_t i = items[w].begin; i < items[w].end; ++i) m = max(m, __float_as_uint(PV[2 * (int64_t)i].w));
+    kmax[w] = m;
+}
+
 // flag[w] = 1 when a node of item w has a stencil support in the layer
 // [nb, nb + nl) (idx: node-major [n][k] kNN indices)
 __global__ void layer_touch_kernel(const uint32_t* __restrict__ idx, int k, const WorkItem* __restrict__ items,
@@ -498,6 +510,28 @@ int scene_setup(naga_scene* s) {
         if (e != cudaSuccess) return set_error(NAGA_ECUDA, std::string("layer items: ") + cudaGetErrorString(e));
         for (int w = 0; w < nf; ++w)
             if (flag[w]) s->items_pml.push_back(s->items_fluid[w]);
+        // each PML item carries its nodes' largest layer-support count in
+        // `local` (its tile is that many records per node)
+        const int np = (int)s->items_pml.size();
+        if (np > 0) {
+            WorkItem* dpi = nullptr;
+            uint32_t* dk = nullptr;
+            std::vector<uint32_t> km(np, 0);
+            e = cudaMallocAsync(&dpi, sizeof(WorkItem) * np, st);
+            if (e == cudaSuccess) e = cudaMallocAsync(&dk, sizeof(uint32_t) * np, st);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(dpi, s->items_pml.data(), sizeof(WorkItem) * np, cudaMemcpyHostToDevice, st);
+            if (e == cudaSuccess) {
+                pml_item_kmax_kernel<<<(np + 255) / 256, 256, 0, st>>>(dpi, np, pv, dk);
+                e = cudaGetLastError();
+            }
+            if (e == cudaSuccess) e = cudaMemcpyAsync(km.data(), dk, sizeof(uint32_t) * np, cudaMemcpyDeviceToHost, st);
+            if (dpi) cudaFreeAsync(dpi, st);
+            if (dk) cudaFreeAsync(dk, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) return set_error(NAGA_ECUDA, std::string("PML items: ") + cudaGetErrorString(e));
+            for (int w = 0; w < np; ++w) s->items_pml[w].local = std::min<uint32_t>(km[w], (uint32_t)k);
+        }
     }
     V.n_all_items = (int)s->items_all.size();
     {

@@ -778,10 +778,12 @@ struct CompactSrc {  // D2Q9 stencil triplets (Wx, Wy, index)
         return {sc.stR + (int64_t)w.begin * k * 3, (uint32_t)((w.end - w.begin) * k * 3 * sizeof(float))};
     }
 };
-struct PmlSrc {  // PML gather records (see pml_table_kernel)
+struct PmlSrc {  // PML gather records (see pml_table_kernel): the first
+                 // w.local (the item's largest layer-support count) per node
     __device__ TileSrc operator()(const SceneDev& sc, const WorkItem& w) const {
         const int k = sc.k;
-        return {sc.stP + (int64_t)w.begin * k, (uint32_t)((w.end - w.begin) * k * sizeof(float4))};
+        const uint32_t kl = w.local < (uint32_t)k ? w.local : (uint32_t)k;
+        return {sc.stP + (int64_t)w.begin * k, (uint32_t)((w.end - w.begin) * kl * sizeof(float4))};
     }
 };
 struct FilterSrc {  // filter records of the item's bulk/layer nodes
