@@ -203,9 +203,28 @@ typedef struct naga_scene_desc {
     int probe_capacity;    /* probe samples kept on the device (ring)       */
 } naga_scene_desc;
 
-/* builds stencils and weights on the device and sets the rest state */
+/* builds stencils and weights on the device and sets the rest state:
+ * simulation_engine::set_problem_parameters + init_domain
+ * (simulation_engine.cuh:52-74) in one call                              */
 int naga_scene_create(const naga_scene_desc* desc, naga_scene** out);
 int naga_scene_destroy(naga_scene* scene);
+/* simulation_engine::set_problem_parameters (simulation_engine.cuh:52-66)
+ * on an existing scene: nu, rho0, dt, c take effect at the next step (the
+ * lattice-unit rates are recomputed; the stencils do not depend on them) */
+int naga_scene_set_params(naga_scene* scene, double viscosity, double rho0,
+                          double time_step, double speed_of_sound);
+/* simulation_engine::init_domain (simulation_engine.cuh:68-74) on an
+ * existing handle: the scene is rebuilt from desc (new nodes, stencils,
+ * probes; rest state, step 0). The scene must not belong to a user batch.
+ * On error the scene keeps its previous domain.                          */
+int naga_scene_init_domain(naga_scene* scene, const naga_scene_desc* desc);
+/* the initial condition: the same as naga_scene_set_density             */
+int naga_scene_set_initial_condition(naga_scene* scene, const float* drho);
+/* attach_observer of a density probe (density_observer.cuh:47-97) after
+ * creation: its RPIM tables are built, the probe ring gains a column
+ * (earlier samples of the other probes are kept; the new probe reads 0
+ * for steps before it was added); *index receives its probe index.      */
+int naga_scene_add_probe(naga_scene* scene, const float* xyz, int* index);
 /* stream the scene's work is issued on (a cudaStream_t) */
 void* naga_scene_stream(naga_scene* scene);
 /* rest state plus a density perturbation (host [N], units of rho0), u = 0;

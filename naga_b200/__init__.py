@@ -95,6 +95,10 @@ _SIGS = {
     "naga_batch_create": ([C.c_int, C.c_void_p], C.c_int),
     "naga_batch_create_with_priority": ([C.c_int, C.c_int, C.c_void_p], C.c_int),
     "naga_selftest_wait_timeout": ([C.c_int], C.c_int),
+    "naga_scene_set_params": ([C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_double], C.c_int),
+    "naga_scene_init_domain": ([C.c_void_p, C.c_void_p], C.c_int),
+    "naga_scene_set_initial_condition": ([C.c_void_p, C.c_void_p], C.c_int),
+    "naga_scene_add_probe": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "naga_batch_destroy": ([C.c_void_p], C.c_int),
     "naga_batch_add": ([C.c_void_p, C.c_void_p], C.c_int),
     "naga_batch_remove": ([C.c_void_p, C.c_void_p], C.c_int),
@@ -240,6 +244,32 @@ class Scene:
             drho = np.ascontiguousarray(drho, np.float32)
             assert drho.shape == (self.N,)
             _check(lib().naga_scene_set_density(self.h, _p(drho)))
+
+    def set_initial_condition(self, drho=None):
+        """naga_scene_set_initial_condition (the same as set_density)."""
+        drho = None if drho is None else np.ascontiguousarray(drho, np.float32)
+        _check(lib().naga_scene_set_initial_condition(self.h, _p(drho)))
+
+    def set_params(self, viscosity: float, rho0: float, time_step: float, speed_of_sound: float):
+        """simulation_engine::set_problem_parameters on the existing scene."""
+        _check(lib().naga_scene_set_params(self.h, viscosity, rho0, time_step, speed_of_sound))
+
+    def init_domain(self, grid: dict, **kw):
+        """simulation_engine::init_domain on this handle (rebuilt from grid)."""
+        d, keep = scene_desc(grid, **kw)
+        _check(lib().naga_scene_init_domain(self.h, C.byref(d)))
+        self._keep, self.desc = keep, d
+        self.dim, self.Q = grid["dim"], Q_OF[grid["dim"]]
+        self.N = keep[0].shape[0]
+        self.n_probes = d.n_probes
+
+    def add_probe(self, xyz) -> int:
+        """Attach one more density probe; returns its index."""
+        x = np.ascontiguousarray(xyz, np.float32).reshape(self.dim)
+        idx = C.c_int()
+        _check(lib().naga_scene_add_probe(self.h, _p(x), C.byref(idx)))
+        self.n_probes += 1
+        return idx.value
 
     def step(self, n: int = 1):
         _check(lib().naga_scene_step(self.h, n))

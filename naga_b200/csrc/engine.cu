@@ -104,6 +104,7 @@ struct naga_scene {
     int64_t src_vals_cap = 0;
     std::vector<int64_t> src_nodes;
     std::vector<float> probe_xyz;
+    float* d_pts = nullptr;  // node coordinates on the device (probe tables)
 
     template <class T>
     int alloc(T** p, int64_t count) {
@@ -280,6 +281,83 @@ void set_parameters(naga_scene* s) {
     D.half_dt = dt_lat / 2.f;
 }
 
+// RPIM interpolation tables at nq host query points from the first nsrc
+// nodes (kNN + weight solves on the device): the boundary form writes
+// pass-ordered (weight, index) records and flags the sources in dsrc; the
+// probe form writes [kk][nq] index and weight tables
+int rpim_tables(naga_scene* s, const float* pts, const float* qry_host, int64_t nq, int64_t nsrc, int kk,
+                uint32_t** idx_out, float** w_out, float2** rec_out, uint8_t* dsrc) {
+    const naga_scene_desc& d = s->desc;
+    const int D = s->dim;
+    const int npb = nodes_per_pass(D);
+    cudaStream_t st = s->stream;
+    uint32_t* didx = nullptr;
+    float* dd2 = nullptr;
+    float* dq = nullptr;
+    double* dqd = nullptr;
+    double* dw = nullptr;
+    NAGA_CUDA_TRY(cudaMallocAsync(&didx, sizeof(uint32_t) * nq * kk, st));
+    NAGA_CUDA_TRY(cudaMallocAsync(&dd2, sizeof(float) * nq * kk, st));
+    NAGA_CUDA_TRY(cudaMallocAsync(&dq, sizeof(float) * nq * D, st));
+    NAGA_CUDA_TRY(cudaMallocAsync(&dqd, sizeof(double) * nq * D, st));
+    NAGA_CUDA_TRY(cudaMallocAsync(&dw, sizeof(double) * nq * kk, st));
+    std::vector<double> qd(nq * D);
+    for (int64_t t = 0; t < nq * D; ++t) qd[t] = qry_host[t];
+    NAGA_CUDA_TRY(cudaMemcpyAsync(dq, qry_host, sizeof(float) * nq * D, cudaMemcpyHostToDevice, st));
+    NAGA_CUDA_TRY(cudaMemcpyAsync(dqd, qd.data(), sizeof(double) * nq * D, cudaMemcpyHostToDevice, st));
+    int r = knn_device(pts, nsrc, dq, nq, D, kk, didx, dd2, st);
+    if (!r) r = rbf_weights_device(pts, nsrc, D, didx, kk, dqd, nq, 1, d.nodal_spacing, d.shape,
+                                   d.weight_precision, dw, st);
+    if (!r && rec_out) {
+        // boundary: records and source flags built on the device
+        r = s->alloc(rec_out, nq * kk);
+        if (!r) {
+            const int64_t ne = nq * kk;
+            boundary_records_kernel<<<(unsigned)((ne + 255) / 256), 256, 0, st>>>(didx, dw, nq, kk, npb, *rec_out,
+                                                                                  dsrc);
+            cudaError_t e = cudaGetLastError();
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) r = set_error(NAGA_ECUDA, std::string("boundary records: ") + cudaGetErrorString(e));
+        }
+        cudaFreeAsync(didx, st);
+        cudaFreeAsync(dd2, st);
+        cudaFreeAsync(dq, st);
+        cudaFreeAsync(dqd, st);
+        cudaFreeAsync(dw, st);
+        return r;
+    }
+    std::vector<uint32_t> hi(nq * kk);
+    std::vector<double> hw(nq * kk);
+    if (!r) {
+        cudaError_t e1 = cudaMemcpyAsync(hi.data(), didx, sizeof(uint32_t) * nq * kk, cudaMemcpyDeviceToHost, st);
+        cudaError_t e2 = cudaMemcpyAsync(hw.data(), dw, sizeof(double) * nq * kk, cudaMemcpyDeviceToHost, st);
+        cudaError_t e3 = cudaStreamSynchronize(st);
+        if (e1 || e2 || e3) r = set_error(NAGA_ECUDA, "naga_scene_create: copy of interpolation tables failed");
+    }
+    cudaFreeAsync(didx, st);
+    cudaFreeAsync(dd2, st);
+    cudaFreeAsync(dq, st);
+    cudaFreeAsync(dqd, st);
+    cudaFreeAsync(dw, st);
+    if (r) return r;
+    {
+        // probes: [k][nq] indices and weights
+        std::vector<uint32_t> ti(nq * kk);
+        std::vector<float> tw(nq * kk);
+        for (int64_t q = 0; q < nq; ++q)
+            for (int t = 0; t < kk; ++t) {
+                ti[(int64_t)t * nq + q] = hi[q * kk + t];
+                tw[(int64_t)t * nq + q] = (float)hw[q * kk + t];
+            }
+        if ((r = s->alloc(idx_out, nq * kk))) return r;
+        if ((r = s->alloc(w_out, nq * kk))) return r;
+        NAGA_CUDA_TRY(cudaMemcpyAsync(*idx_out, ti.data(), sizeof(uint32_t) * nq * kk, cudaMemcpyHostToDevice, st));
+        NAGA_CUDA_TRY(cudaMemcpyAsync(*w_out, tw.data(), sizeof(float) * nq * kk, cudaMemcpyHostToDevice, st));
+        NAGA_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    return NAGA_OK;
+}
+
 int scene_setup(naga_scene* s) {
     const naga_scene_desc& d = s->desc;
     const int D = s->dim, QP = s->QP;
@@ -303,6 +381,7 @@ int scene_setup(naga_scene* s) {
     float* pts = nullptr;
     int rc;
     if ((rc = s->alloc(&pts, N * D))) return rc;
+    s->d_pts = pts;
     NAGA_CUDA_TRY(cudaMemcpyAsync(pts, d.points, sizeof(float) * N * D, cudaMemcpyHostToDevice, st));
     NAGA_CUDA_TRY(cudaStreamSynchronize(st));
     float* nrm = nullptr;
@@ -390,71 +469,7 @@ int scene_setup(naga_scene* s) {
     NAGA_CUDA_TRY(cudaMemsetAsync(dsrc, 0, N, st));
     auto rpim = [&](const float* qry_host, int64_t nq, int64_t nsrc, int kk, uint32_t** idx_out, float** w_out,
                     float2** rec_out) -> int {
-        uint32_t* didx = nullptr;
-        float* dd2 = nullptr;
-        float* dq = nullptr;
-        double* dqd = nullptr;
-        double* dw = nullptr;
-        NAGA_CUDA_TRY(cudaMallocAsync(&didx, sizeof(uint32_t) * nq * kk, st));
-        NAGA_CUDA_TRY(cudaMallocAsync(&dd2, sizeof(float) * nq * kk, st));
-        NAGA_CUDA_TRY(cudaMallocAsync(&dq, sizeof(float) * nq * D, st));
-        NAGA_CUDA_TRY(cudaMallocAsync(&dqd, sizeof(double) * nq * D, st));
-        NAGA_CUDA_TRY(cudaMallocAsync(&dw, sizeof(double) * nq * kk, st));
-        std::vector<double> qd(nq * D);
-        for (int64_t t = 0; t < nq * D; ++t) qd[t] = qry_host[t];
-        NAGA_CUDA_TRY(cudaMemcpyAsync(dq, qry_host, sizeof(float) * nq * D, cudaMemcpyHostToDevice, st));
-        NAGA_CUDA_TRY(cudaMemcpyAsync(dqd, qd.data(), sizeof(double) * nq * D, cudaMemcpyHostToDevice, st));
-        int r = knn_device(pts, nsrc, dq, nq, D, kk, didx, dd2, st);
-        if (!r) r = rbf_weights_device(pts, nsrc, D, didx, kk, dqd, nq, 1, d.nodal_spacing, d.shape,
-                                       d.weight_precision, dw, st);
-        if (!r && rec_out) {
-            // boundary: records and source flags built on the device
-            r = s->alloc(rec_out, nq * kk);
-            if (!r) {
-                const int64_t ne = nq * kk;
-                boundary_records_kernel<<<(unsigned)((ne + 255) / 256), 256, 0, st>>>(didx, dw, nq, kk, npb, *rec_out,
-                                                                                      dsrc);
-                cudaError_t e = cudaGetLastError();
-                if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-                if (e != cudaSuccess) r = set_error(NAGA_ECUDA, std::string("boundary records: ") + cudaGetErrorString(e));
-            }
-            cudaFreeAsync(didx, st);
-            cudaFreeAsync(dd2, st);
-            cudaFreeAsync(dq, st);
-            cudaFreeAsync(dqd, st);
-            cudaFreeAsync(dw, st);
-            return r;
-        }
-        std::vector<uint32_t> hi(nq * kk);
-        std::vector<double> hw(nq * kk);
-        if (!r) {
-            cudaError_t e1 = cudaMemcpyAsync(hi.data(), didx, sizeof(uint32_t) * nq * kk, cudaMemcpyDeviceToHost, st);
-            cudaError_t e2 = cudaMemcpyAsync(hw.data(), dw, sizeof(double) * nq * kk, cudaMemcpyDeviceToHost, st);
-            cudaError_t e3 = cudaStreamSynchronize(st);
-            if (e1 || e2 || e3) r = set_error(NAGA_ECUDA, "naga_scene_create: copy of interpolation tables failed");
-        }
-        cudaFreeAsync(didx, st);
-        cudaFreeAsync(dd2, st);
-        cudaFreeAsync(dq, st);
-        cudaFreeAsync(dqd, st);
-        cudaFreeAsync(dw, st);
-        if (r) return r;
-        {
-            // probes: [k][nq] indices and weights
-            std::vector<uint32_t> ti(nq * kk);
-            std::vector<float> tw(nq * kk);
-            for (int64_t q = 0; q < nq; ++q)
-                for (int t = 0; t < kk; ++t) {
-                    ti[(int64_t)t * nq + q] = hi[q * kk + t];
-                    tw[(int64_t)t * nq + q] = (float)hw[q * kk + t];
-                }
-            if ((r = s->alloc(idx_out, nq * kk))) return r;
-            if ((r = s->alloc(w_out, nq * kk))) return r;
-            NAGA_CUDA_TRY(cudaMemcpyAsync(*idx_out, ti.data(), sizeof(uint32_t) * nq * kk, cudaMemcpyHostToDevice, st));
-            NAGA_CUDA_TRY(cudaMemcpyAsync(*w_out, tw.data(), sizeof(float) * nq * kk, cudaMemcpyHostToDevice, st));
-            NAGA_CUDA_TRY(cudaStreamSynchronize(st));
-        }
-        return NAGA_OK;
+        return rpim_tables(s, pts, qry_host, nq, nsrc, kk, idx_out, w_out, rec_out, dsrc);
     };
     float2* btab = nullptr;
     if (s->nbd > 0) {
@@ -807,6 +822,91 @@ extern "C" int naga_scene_set_density(naga_scene* s, const float* drho) {
     NAGA_CUDA_TRY(cudaMemsetAsync(V.probe_ring, 0, sizeof(float) * V.probe_cap * std::max(1, V.np), st));
     NAGA_CUDA_TRY(cudaStreamSynchronize(st));
     s->steps = 0;
+    return NAGA_OK;
+}
+
+extern "C" int naga_scene_set_initial_condition(naga_scene* s, const float* drho) {
+    return naga_scene_set_density(s, drho);
+}
+
+extern "C" int naga_scene_set_params(naga_scene* s, double viscosity, double rho0, double time_step,
+                                     double speed_of_sound) {
+    if (!s) return set_error(NAGA_EINVAL, "naga_scene_set_params: null scene");
+    if (!(viscosity >= 0) || !(rho0 > 0) || !(time_step > 0) || !(speed_of_sound > 0))
+        return set_error(NAGA_EINVAL, "naga_scene_set_params: physical parameters must be positive");
+    NAGA_CUDA_TRY(cudaStreamSynchronize(active_stream(s)));
+    s->desc.viscosity = viscosity;
+    s->desc.rho0 = rho0;
+    s->desc.time_step = time_step;
+    s->desc.speed_of_sound = speed_of_sound;
+    set_parameters(s);
+    // the batches holding the scene re-upload its parameters before stepping
+    if (s->owner) s->owner->dirty = true;
+    if (s->solo) s->solo->dirty = true;
+    return NAGA_OK;
+}
+
+extern "C" int naga_scene_init_domain(naga_scene* s, const naga_scene_desc* d) {
+    if (!s || !d) return set_error(NAGA_EINVAL, "naga_scene_init_domain: null argument");
+    if (s->owner) return set_error(NAGA_EINVAL, "naga_scene_init_domain: remove the scene from its batch first");
+    naga_scene* fresh = nullptr;
+    int rc = naga_scene_create(d, &fresh);
+    if (rc) return rc;  // the scene keeps its previous domain
+    NAGA_CUDA_TRY(cudaStreamSynchronize(active_stream(s)));
+    // the handle takes the new scene; the old contents are released
+    std::swap(*s, *fresh);
+    return naga_scene_destroy(fresh);
+}
+
+namespace {
+// frees one of the scene's device allocations now
+void release(naga_scene* s, void* p) {
+    if (!p) return;
+    auto it = std::find(s->allocs.begin(), s->allocs.end(), p);
+    if (it == s->allocs.end()) return;
+    s->allocs.erase(it);
+    cudaFree(p);
+}
+}  // namespace
+
+extern "C" int naga_scene_add_probe(naga_scene* s, const float* xyz, int* index) {
+    if (!s || !xyz) return set_error(NAGA_EINVAL, "naga_scene_add_probe: null argument");
+    if (!s->d_pts) return set_error(NAGA_EINVAL, "naga_scene_add_probe: scene has no domain");
+    cudaStream_t st = active_stream(s);
+    NAGA_CUDA_TRY(cudaStreamSynchronize(st));
+    const int D = s->dim;
+    const int np_old = s->dev.np, np = np_old + 1;
+    s->probe_xyz.insert(s->probe_xyz.end(), xyz, xyz + D);
+    uint32_t* pidx = nullptr;
+    float* pw = nullptr;
+    int rc = rpim_tables(s, s->d_pts, s->probe_xyz.data(), np, s->N, s->desc.k_probe, &pidx, &pw, nullptr, nullptr);
+    float* ring = nullptr;
+    const int64_t cap = s->dev.probe_cap;
+    if (!rc) rc = s->alloc(&ring, cap * np);
+    if (rc) {
+        s->probe_xyz.resize((size_t)np_old * D);
+        release(s, pidx);
+        release(s, pw);
+        return rc;
+    }
+    // the ring gains a column: earlier samples of the old probes are kept,
+    // the new probe's read as zero before it was added
+    NAGA_CUDA_TRY(cudaMemsetAsync(ring, 0, sizeof(float) * cap * np, st));
+    if (np_old > 0)
+        NAGA_CUDA_TRY(cudaMemcpy2DAsync(ring, sizeof(float) * np, s->dev.probe_ring, sizeof(float) * np_old,
+                                        sizeof(float) * np_old, cap, cudaMemcpyDeviceToDevice, st));
+    NAGA_CUDA_TRY(cudaStreamSynchronize(st));
+    release(s, const_cast<uint32_t*>(s->dev.pidx));
+    release(s, const_cast<float*>(s->dev.pw));
+    release(s, s->dev.probe_ring);
+    s->dev.pidx = pidx;
+    s->dev.pw = pw;
+    s->dev.probe_ring = ring;
+    s->dev.np = np;
+    s->desc.n_probes = np;
+    if (s->owner) s->owner->dirty = true;
+    if (s->solo) s->solo->dirty = true;
+    if (index) *index = np - 1;
     return NAGA_OK;
 }
 

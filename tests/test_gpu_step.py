@@ -328,3 +328,67 @@ def test_bounded_wait_gives_up_and_context_stays_usable(naga, oracle):
     gpu.step(5)
     po = orc.step(5)
     assert rel_err(gpu.probes(0, 5), po) <= 1e-5
+
+
+def test_set_params_equals_scene_created_with_them(naga, oracle):
+    """set_problem_parameters on a live scene (naga_scene_set_params, then
+    the initial condition) gives bit for bit the scene created with those
+    parameters."""
+    g = naga.generate_grid(2, 30, 3, 11)
+    drho = naga.gaussian_pulse(g["points"], [0.5, 0.5], 1e-3, 0.08)
+    nu, rho0, dt = 3e-5, 1.2, 0.4 * g["h"]
+    ref = naga.Scene(g, k=16, probes=PROBES2, viscosity=nu, rho0=rho0, time_step=dt)
+    ref.set_density(drho)
+    ref.step(12)
+    s = naga.Scene(g, k=16, probes=PROBES2)
+    s.set_density(drho)
+    s.step(3)
+    s.set_params(nu, rho0, dt, 1.0)
+    s.set_initial_condition(drho)
+    s.step(12)
+    assert np.array_equal(s.probes(0, 12), ref.probes(0, 12))
+    assert np.array_equal(s.state()[0], ref.state()[0])
+
+
+def test_init_domain_rebuilds_the_handle(naga, oracle):
+    """init_domain on a live handle equals a scene created on the new domain
+    (nodes, stencils, probes, step count)."""
+    g1 = naga.generate_grid(2, 26, 3, 12)
+    g2 = naga.generate_grid(2, 33, 4, 13)
+    s = naga.Scene(g1, k=16, probes=PROBES2[:2])
+    s.set_density(naga.gaussian_pulse(g1["points"], [0.5, 0.5], 1e-3, 0.08))
+    s.step(4)
+    drho = naga.gaussian_pulse(g2["points"], [0.45, 0.5], 1e-3, 0.07)
+    s.init_domain(g2, k=16, probes=PROBES2)
+    assert s.step_count == 0 and s.N == len(g2["points"])
+    s.set_density(drho)
+    s.step(10)
+    ref = naga.Scene(g2, k=16, probes=PROBES2)
+    ref.set_density(drho)
+    ref.step(10)
+    assert np.array_equal(s.probes(0, 10), ref.probes(0, 10))
+    assert np.array_equal(s.state()[0], ref.state()[0])
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_add_probe_after_creation(naga, oracle, dim):
+    """A probe attached after some steps samples like the same probe given
+    at creation from then on (zeros before); the other probes keep their
+    history."""
+    g = naga.generate_grid(dim, 30 if dim == 2 else 14, 3, 14)
+    P = PROBES2 if dim == 2 else PROBES3
+    k = 16 if dim == 2 else 32
+    shape = 1 if dim == 2 else 0
+    drho = naga.gaussian_pulse(g["points"], [0.5] * dim, 1e-3, 0.08)
+    ref = naga.Scene(g, k=k, shape=shape, probes=P[:3])
+    ref.set_density(drho)
+    ref.step(10)
+    s = naga.Scene(g, k=k, shape=shape, probes=P[:2])
+    s.set_density(drho)
+    s.step(4)
+    assert s.add_probe(P[2]) == 2
+    s.step(6)
+    got, want = s.probes(0, 10), ref.probes(0, 10)
+    assert np.array_equal(got[:, :2], want[:, :2])
+    assert np.array_equal(got[4:, 2], want[4:, 2])
+    assert (got[:4, 2] == 0).all()
