@@ -218,7 +218,12 @@ class simulation_engine {
         p.lattice_viscosity = fluid_viscosity / ratio;
         const value_type fc = characteristic_frequency == 0 ? value_type(1) / time_step : characteristic_frequency;
         p.lattice_characteristic_frequency = fc * ratio;
-        impl_->invalidate();
+        // a live scene takes the new parameters at its next step (its state
+        // and stencils stay); otherwise they apply when the scene is built
+        if (impl_->scene)
+            detail::check(naga_scene_set_params(impl_->scene, fluid_viscosity, nominal_density, time_step,
+                                                speed_of_sound),
+                          "set_problem_parameters");
     }
 
     void init_domain(const simulation_domain_t& domain) {
@@ -289,7 +294,13 @@ class simulation_engine {
 
     void attach_observer(simulation_observer<Lattice>& o) {
         impl_->observers.push_back(&o);
-        impl_->invalidate();
+        if (impl_->scene) {
+            // a live scene gains a probe; it samples from the next step on
+            const auto l = o.location();
+            std::vector<float> x(l.begin(), l.end());
+            int index = 0;
+            detail::check(naga_scene_add_probe(impl_->scene, x.data(), &index), "attach_observer");
+        }
     }
     void detach_observer(simulation_observer<Lattice>& o) {
         auto& v = impl_->observers;

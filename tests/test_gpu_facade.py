@@ -56,3 +56,10 @@ def test_facade_density_source_matches_python_binding(naga):
     p = s.probes(0, 25)
     assert np.abs(p).max() > 0
     assert np.allclose(rows[:, 2:], p, rtol=0, atol=1e-7 * max(1.0, np.abs(p).max()) + 2e-7)
+
+
+def test_facade_live_observers_and_parameters(naga):
+    """attach_observer and set_problem_parameters on a running facade engine
+    (naga_scene_add_probe / naga_scene_set_params underneath) agree bit for
+    bit with engines that had them from the start."""
+    assert _run_program(naga, "facade_live").strip() == "ok"
