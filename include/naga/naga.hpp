@@ -137,6 +137,52 @@ class jittered_grid_provider : public node_provider<Lattice> {
     naga_grid_spec spec_;
 };
 
+// NAGA's uniform_grid_provider (node_providers/uniform_grid_provider.cuh:
+// 53-161) with its constructor: an axis-aligned box [min, max] at
+// grid_spacing, absorbing layer of the given thickness and peak rate
+// (naga_box_grid_generate). Nodes within each class come in Morton order.
+template <class Lattice>
+class uniform_grid_provider : public node_provider<Lattice> {
+  public:
+    using value_type = typename lattice_traits<Lattice>::value_type;
+    static constexpr unsigned dimensions = Lattice::dimensions;
+    uniform_grid_provider(const point_t<value_type, dimensions>& min, const point_t<value_type, dimensions>& max,
+                          const value_type& grid_spacing, const value_type& absorption_layer_thickness = 0,
+                          const value_type& peak_absorption_rate = 0) {
+        spec_.dim = (int)dimensions;
+        spec_.morton = 1;
+        for (unsigned d = 0; d < 3; ++d) {
+            spec_.min[d] = d < dimensions ? (double)min[d] : 0.0;
+            spec_.max[d] = d < dimensions ? (double)max[d] : 1.0;
+        }
+        spec_.spacing = grid_spacing;
+        spec_.layer_thickness = absorption_layer_thickness;
+        spec_.peak_absorption = peak_absorption_rate;
+    }
+
+    simulation_nodes<value_type> get() const override {
+        int64_t nb, nl, nbd;
+        detail::check(naga_box_grid_counts(&spec_, &nb, &nl, &nbd), "uniform_grid_provider");
+        const int D = spec_.dim;
+        std::vector<float> pts((nb + nl + nbd) * D), nrm(nbd * D), sig(nl);
+        double h = 0;
+        detail::check(naga_box_grid_generate(&spec_, pts.data(), nrm.data(), sig.data(), &h),
+                      "uniform_grid_provider");
+        simulation_nodes<value_type> out;
+        out.points.assign(pts.begin(), pts.end());
+        out.boundary_normals.assign(nrm.begin(), nrm.end());
+        out.layer_absorption.assign(sig.begin(), sig.end());
+        out.num_bulk_points = (size_t)nb;
+        out.num_layer_points = (size_t)nl;
+        out.num_boundary_points = (size_t)nbd;
+        out.nodal_spacing = (value_type)h;
+        return out;
+    }
+
+  private:
+    naga_box_grid_spec spec_{};
+};
+
 template <class Lattice>
 class simulation_observer {
   public:

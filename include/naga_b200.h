@@ -70,6 +70,27 @@ int naga_grid_counts(const naga_grid_spec* spec, int64_t* n_bulk,
  * sigma [n_layer]; any output may be NULL.                                  */
 int naga_grid_generate(const naga_grid_spec* spec, float* points,
                        float* normals, float* sigma, double* nodal_spacing);
+/* NAGA's uniform_grid_provider(min, max, grid_spacing, layer_thickness,
+ * peak_absorption_rate) (node_providers/uniform_grid_provider.cuh:53-161),
+ * on the host in its FP32 arithmetic: an axis-aligned box gridded with
+ * ceil((max - min) / spacing) + 1 nodes per axis, boundary = outer shell
+ * (inward normals), layer = nodes within layer_thickness of the nearest
+ * boundary node, sigma = peak ((L - d) / L)^2; classes [bulk, layer,
+ * boundary], each in Morton order (morton = 1) or grid order (0). Fill the
+ * unused coordinates of min / max for dim = 2 with anything.              */
+typedef struct naga_box_grid_spec {
+    int dim;
+    int morton;
+    double min[3], max[3];
+    double spacing, layer_thickness, peak_absorption;
+} naga_box_grid_spec;
+
+int naga_box_grid_counts(const naga_box_grid_spec* spec, int64_t* n_bulk,
+                         int64_t* n_layer, int64_t* n_boundary);
+/* host outputs as naga_grid_generate; nodal_spacing = spacing            */
+int naga_box_grid_generate(const naga_box_grid_spec* spec, float* points,
+                           float* normals, float* sigma,
+                           double* nodal_spacing);
 /* drho_i = amplitude * exp(-|x_i - center|^2 / (2 width^2)), host arrays    */
 int naga_gaussian_pulse(const float* points, int64_t n, int dim,
                         const double* center, double amplitude, double width,

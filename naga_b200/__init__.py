@@ -60,6 +60,8 @@ _SIGS = {
     "naga_version": ([], C.c_int),
     "naga_grid_counts": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "naga_grid_generate": ([C.c_void_p] * 5, C.c_int),
+    "naga_box_grid_counts": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "naga_box_grid_generate": ([C.c_void_p] * 5, C.c_int),
     "naga_gaussian_pulse": ([C.c_void_p, C.c_int64, C.c_int, C.c_void_p, C.c_double, C.c_double,
                              C.c_void_p], C.c_int),
     "naga_knn": ([C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_void_p,
@@ -177,6 +179,34 @@ def generate_grid(dim: int, n_side: int, n_layers: int, seed: int, jitter: float
     sig = np.zeros(nl.value, np.float32)
     h = C.c_double()
     _check(lib().naga_grid_generate(C.byref(sp), _p(pts), _p(nrm), _p(sig), C.byref(h)))
+    return dict(dim=dim, points=pts, n_bulk=nb.value, n_layer=nl.value, n_boundary=nbd.value,
+                normals=nrm, sigma=sig, h=h.value)
+
+
+class BoxGridSpec(C.Structure):
+    _fields_ = [("dim", C.c_int), ("morton", C.c_int), ("min", C.c_double * 3), ("max", C.c_double * 3),
+                ("spacing", C.c_double), ("layer_thickness", C.c_double), ("peak_absorption", C.c_double)]
+
+
+def box_grid(lo, hi, spacing: float, layer_thickness: float = 0.0, peak_absorption: float = 0.0,
+             morton: bool = True) -> dict:
+    """NAGA's uniform_grid_provider(min, max, grid_spacing, layer_thickness,
+    peak_absorption_rate): see naga_box_grid_generate in include/naga_b200.h."""
+    dim = len(lo)
+    sp = BoxGridSpec()
+    sp.dim, sp.morton = dim, int(bool(morton))
+    for d in range(3):
+        sp.min[d] = float(lo[d]) if d < dim else 0.0
+        sp.max[d] = float(hi[d]) if d < dim else 1.0
+    sp.spacing, sp.layer_thickness, sp.peak_absorption = spacing, layer_thickness, peak_absorption
+    nb, nl, nbd = C.c_int64(), C.c_int64(), C.c_int64()
+    _check(lib().naga_box_grid_counts(C.byref(sp), C.byref(nb), C.byref(nl), C.byref(nbd)))
+    n = nb.value + nl.value + nbd.value
+    pts = np.zeros((n, dim), np.float32)
+    nrm = np.zeros((nbd.value, dim), np.float32)
+    sig = np.zeros(nl.value, np.float32)
+    h = C.c_double()
+    _check(lib().naga_box_grid_generate(C.byref(sp), _p(pts), _p(nrm), _p(sig), C.byref(h)))
     return dict(dim=dim, points=pts, n_bulk=nb.value, n_layer=nl.value, n_boundary=nbd.value,
                 normals=nrm, sigma=sig, h=h.value)
 

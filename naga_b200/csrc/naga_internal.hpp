@@ -24,5 +24,6 @@ struct GridScene {
 };
 
 int build_grid_scene(const naga_grid_spec& spec, GridScene& out);
+int build_box_scene(const naga_box_grid_spec& spec, GridScene& out);
 
 }  // namespace naga

@@ -199,6 +199,139 @@ int build_grid_scene(const naga_grid_spec& sp, GridScene& out) {
     return NAGA_OK;
 }
 
+
+namespace {
+// grid indices of an nx x ny x nz box in increasing Morton order (x lowest)
+void morton_walk_box(int dim, const int64_t* n, int64_t x0, int64_t y0, int64_t z0, int64_t size,
+                     std::vector<int64_t>& out) {
+    if (x0 >= n[0] || y0 >= n[1] || z0 >= n[2]) return;
+    if (size == 1) {
+        out.push_back(x0 + n[0] * (y0 + n[1] * z0));
+        return;
+    }
+    const int64_t hs = size / 2;
+    const int nc = dim == 3 ? 8 : 4;
+    for (int c = 0; c < nc; ++c)
+        morton_walk_box(dim, n, x0 + (c & 1) * hs, y0 + ((c >> 1) & 1) * hs, z0 + ((c >> 2) & 1) * hs, hs, out);
+}
+}  // namespace
+
+// NAGA's uniform_grid_provider (node_providers/uniform_grid_provider.cuh:
+// 53-161) restated on the host, in its FP32 arithmetic: per axis
+// ceil((max - min) / h) + 1 nodes at the spacing that fits the box
+// (ranges/uniform_grid.cuh:58-64, node n at min + (n % size) * spacing, x
+// fastest); the outer shell is the boundary with the normalised outward
+// face normal negated (uniform_grid.cuh:243-293, provider :89-94); a
+// non-boundary node is in the layer when the squared distance to its
+// nearest boundary node -- the projection onto its nearest face -- is
+// <= L^2, with sigma = peak ((L - d) / L)^2 (detail/uniform_grid_provider.
+// inl:111-171). Classes come in NAGA's order [bulk, layer, boundary]; inside
+// each, Morton order (NAGA's is the order of atomic increments, not
+// reproducible) or the grid order.
+int build_box_scene(const naga_box_grid_spec& sp, GridScene& out) {
+    const int dim = sp.dim;
+    if (dim != 2 && dim != 3) return NAGA_EINVAL;
+    const float h = (float)sp.spacing;
+    if (!(h > 0) || !(sp.layer_thickness >= 0)) return NAGA_EINVAL;
+    float mn[3] = {0, 0, 0}, sp_[3] = {1, 1, 1};
+    int64_t n[3] = {1, 1, 1};
+    int64_t total = 1;
+    for (int d = 0; d < dim; ++d) {
+        mn[d] = (float)sp.min[d];
+        const float ext = (float)sp.max[d] - mn[d];
+        if (!(ext > 0)) return NAGA_EINVAL;
+        n[d] = (int64_t)std::ceil(ext / h) + 1;
+        if (n[d] < 3) return NAGA_EINVAL;
+        sp_[d] = ext / (float)(n[d] - 1);
+        total *= n[d];
+    }
+    if (total > (int64_t)UINT32_MAX / 2) return NAGA_EINVAL;
+    float hi[3] = {0, 0, 0};  // coordinate of the high face's nodes
+    for (int d = 0; d < dim; ++d) hi[d] = mn[d] + (float)(n[d] - 1) * sp_[d];
+    const float L = (float)sp.layer_thickness;
+    out.dim = dim;
+    out.h = h;
+
+    std::vector<float> pos((size_t)total * dim);
+    std::vector<char> is_bnd(total, 0);
+    std::vector<float> dist2(total, 0.f);
+    parallel_for(total, [&](int64_t b, int64_t e) {
+        for (int64_t t = b; t < e; ++t) {
+            int64_t r = t;
+            bool bnd = false;
+            float best = 0.f;
+            bool first = true;
+            for (int d = 0; d < dim; ++d) {
+                const int64_t g = r % n[d];
+                r /= n[d];
+                const float x = mn[d] + (float)g * sp_[d];
+                pos[(size_t)t * dim + d] = x;
+                if (g == 0 || g == n[d] - 1) bnd = true;
+                const float lo = (x - mn[d]) * (x - mn[d]), up = (x - hi[d]) * (x - hi[d]);
+                const float m = std::min(lo, up);
+                if (first || m < best) best = m;
+                first = false;
+            }
+            is_bnd[t] = bnd;
+            dist2[t] = best;
+        }
+    });
+
+    std::vector<int64_t> order;
+    order.reserve((size_t)total);
+    if (sp.morton) {
+        int64_t size = 1;
+        while (size < std::max(n[0], std::max(n[1], n[2]))) size *= 2;
+        morton_walk_box(dim, n, 0, 0, 0, size, order);
+    } else {
+        for (int64_t t = 0; t < total; ++t) order.push_back(t);
+    }
+    std::vector<int64_t> bulk, layer, bnd;
+    for (int64_t t : order) {
+        if (is_bnd[t])
+            bnd.push_back(t);
+        else if (L > 0 && dist2[t] <= L * L)
+            layer.push_back(t);
+        else
+            bulk.push_back(t);
+    }
+    out.n_bulk = (int64_t)bulk.size();
+    out.n_layer = (int64_t)layer.size();
+    out.n_boundary = (int64_t)bnd.size();
+    out.points.resize((size_t)total * dim);
+    out.normals.resize((size_t)out.n_boundary * dim);
+    out.sigma.resize((size_t)out.n_layer);
+    out.grid_index.resize((size_t)total);
+    int64_t w = 0;
+    auto emit = [&](int64_t lin) {
+        std::memcpy(&out.points[(size_t)w * dim], &pos[(size_t)lin * dim], sizeof(float) * dim);
+        out.grid_index[w] = lin;
+        ++w;
+    };
+    for (int64_t t : bulk) emit(t);
+    for (size_t q = 0; q < layer.size(); ++q) {
+        const float d = std::sqrt(dist2[layer[q]]);
+        const float r = (L - d) / L;
+        out.sigma[q] = (float)sp.peak_absorption * (r * r);
+        emit(layer[q]);
+    }
+    for (size_t q = 0; q < bnd.size(); ++q) {
+        int64_t r = bnd[q];
+        float nv[3] = {0, 0, 0};
+        for (int d = 0; d < dim; ++d) {
+            const int64_t g = r % n[d];
+            r /= n[d];
+            nv[d] = g == 0 ? -1.f : (g == n[d] - 1 ? 1.f : 0.f);
+        }
+        float nn = 0;
+        for (int d = 0; d < dim; ++d) nn += nv[d] * nv[d];
+        nn = std::sqrt(nn);
+        for (int d = 0; d < dim; ++d) out.normals[q * dim + d] = -(nv[d] / (nn == 0 ? 1.f : nn));
+        emit(bnd[q]);
+    }
+    return NAGA_OK;
+}
+
 }  // namespace naga
 
 using namespace naga;
@@ -272,5 +405,55 @@ extern "C" int naga_gaussian_pulse(const float* points, int64_t n, int dim, cons
         }
         drho[i] = (float)(amplitude * std::exp(-r2 / (2.0 * width * width)));
     }
+    return NAGA_OK;
+}
+
+namespace {
+struct BoxCache {
+    bool valid = false;
+    naga_box_grid_spec spec{};
+    GridScene scene;
+};
+thread_local BoxCache g_box_cache;
+
+int cached_box(const naga_box_grid_spec& spec, const GridScene** out) {
+    BoxCache& c = g_box_cache;
+    if (!c.valid || std::memcmp(&c.spec, &spec, sizeof spec) != 0) {
+        c.valid = false;
+        c.scene = GridScene{};
+        int rc = build_box_scene(spec, c.scene);
+        if (rc) return rc;
+        c.spec = spec;
+        c.valid = true;
+    }
+    *out = &c.scene;
+    return NAGA_OK;
+}
+}  // namespace
+
+extern "C" int naga_box_grid_counts(const naga_box_grid_spec* spec, int64_t* n_bulk, int64_t* n_layer,
+                                    int64_t* n_boundary) {
+    if (!spec) return set_error(NAGA_EINVAL, "naga_box_grid_counts: null spec");
+    naga_box_grid_spec key = *spec;
+    const GridScene* g = nullptr;
+    int rc = cached_box(key, &g);
+    if (rc) return set_error(rc, "naga_box_grid_counts: invalid box grid spec");
+    if (n_bulk) *n_bulk = g->n_bulk;
+    if (n_layer) *n_layer = g->n_layer;
+    if (n_boundary) *n_boundary = g->n_boundary;
+    return NAGA_OK;
+}
+
+extern "C" int naga_box_grid_generate(const naga_box_grid_spec* spec, float* points, float* normals, float* sigma,
+                                      double* nodal_spacing) {
+    if (!spec) return set_error(NAGA_EINVAL, "naga_box_grid_generate: null spec");
+    naga_box_grid_spec key = *spec;
+    const GridScene* g = nullptr;
+    int rc = cached_box(key, &g);
+    if (rc) return set_error(rc, "naga_box_grid_generate: invalid box grid spec");
+    if (points) std::memcpy(points, g->points.data(), g->points.size() * sizeof(float));
+    if (normals) std::memcpy(normals, g->normals.data(), g->normals.size() * sizeof(float));
+    if (sigma) std::memcpy(sigma, g->sigma.data(), g->sigma.size() * sizeof(float));
+    if (nodal_spacing) *nodal_spacing = g->h;
     return NAGA_OK;
 }

@@ -392,3 +392,19 @@ def test_add_probe_after_creation(naga, oracle, dim):
     assert np.array_equal(got[:, :2], want[:, :2])
     assert np.array_equal(got[4:, 2], want[4:, 2])
     assert (got[:4, 2] == 0).all()
+
+
+def test_box_grid_scene_matches_oracle(naga, oracle):
+    """A scene on NAGA's uniform_grid_provider box (non-square, offset,
+    absorbing layer) steps to the FP64 oracle's probe trace."""
+    g = naga.box_grid([-0.5, 0.0], [0.7, 0.9], 0.03, 0.12, 0.1)
+    probes = np.array([[-0.2, 0.45], [0.3, 0.5]], np.float32)
+    gpu = naga.Scene(g, k=16, shape=1, probes=probes)
+    orc = oracle.Scene(2, g["points"], g["n_bulk"], g["n_layer"], g["n_boundary"], g["normals"], g["sigma"],
+                       g["h"], k=16, shape=1, probes=probes)
+    drho = naga.gaussian_pulse(g["points"], [0.1, 0.45], 1e-3, 0.08)
+    gpu.set_density(drho)
+    orc.set_density(drho)
+    gpu.step(60)
+    po = orc.step(60)
+    assert rel_err(gpu.probes(0, 60), po) <= 1e-5
