@@ -1393,7 +1393,7 @@ int enqueue_step_k(const StepLaunch& P, cudaStream_t st) {
 }
 
 // Launch-shape tuner: times RK stage 1 (it reads G and overwrites only the
-// stage scratch G1 and ACC, so it can run between steps) on the batch's own
+// stage scratch G1, so it can run between steps) on the batch's own
 // items for each candidate -- the default carveout (0), then 2 .. max
 // resident blocks per SM -- and keeps the fastest (a fixed carveout only
 // when it beats the default by 3%). NAGA_GATHER_BPS=<n>
