@@ -87,6 +87,20 @@ struct simulation_nodes {
     T nodal_spacing{};
 };
 
+// simulation_engine::solution() (simulation_variables.cuh:52-62) as host
+// copies: f per direction (library population order, naga_lattice), the
+// density rho rho0 and velocity u c / c_s ({dimensions, N}, a node's
+// components adjacent)
+template <class Lattice>
+struct state_variables {
+    using value_type = typename Lattice::value_type;
+    std::array<std::vector<value_type>, Lattice::size> lattice_distributions{};
+    struct {
+        std::vector<value_type> fluid_velocity;
+        std::vector<value_type> fluid_density;
+    } macroscopic_values;
+};
+
 template <class T>
 struct problem_parameters {
     T fluid_viscosity;
@@ -373,6 +387,32 @@ class simulation_engine {
         std::vector<float> g(N * Q);
         detail::check(naga_scene_read_state(impl_->scene, g.data(), nullptr), "populations");
         return g;
+    }
+
+    // simulation_engine::solution() (simulation_engine.cuh:100): the
+    // populations f = w + g per direction and the dimensional macroscopic
+    // values of the last step, copied to the host
+    state_variables<Lattice> solution() {
+        impl_->ensure();
+        int64_t N;
+        int Q;
+        naga_scene_size(impl_->scene, &N, &Q);
+        std::vector<float> g((size_t)N * Q);
+        detail::check(naga_scene_read_state(impl_->scene, g.data(), nullptr), "solution");
+        std::vector<float> w(Q);
+        detail::check(naga_lattice((int)dimensions, nullptr, w.data(), nullptr), "solution");
+        state_variables<Lattice> out;
+        for (int a = 0; a < Q; ++a) {
+            auto& f = out.lattice_distributions[a];
+            f.resize((size_t)N);
+            for (int64_t i = 0; i < N; ++i) f[i] = w[a] + g[(size_t)i * Q + a];
+        }
+        out.macroscopic_values.fluid_density.resize((size_t)N);
+        out.macroscopic_values.fluid_velocity.resize((size_t)N * dimensions);
+        detail::check(naga_scene_read_macros(impl_->scene, out.macroscopic_values.fluid_density.data(),
+                                             out.macroscopic_values.fluid_velocity.data()),
+                      "solution");
+        return out;
     }
 
     naga_scene* handle() {

@@ -275,6 +275,18 @@ int naga_scene_read_probes_async(naga_scene* scene, int64_t first,
                                  int64_t count, float* out);
 /* centred populations g = f - w, host [N][Q], and rho - rho0, host [N]   */
 int naga_scene_read_state(naga_scene* scene, float* g, float* drho);
+/* the lattice in the library's population order (the order of g in
+ * naga_scene_read_state / write_state): Q, weights [Q] and velocities
+ * [Q][dim] (integers); outputs may be NULL. The order and values are NAGA's
+ * (detail/d2q9_lattice.cuh:44-88, detail/d3q27_lattice.cuh:45-123).        */
+int naga_lattice(int dim, int* q, float* weights, int* velocities);
+/* the macroscopic values of simulation_engine::solution()
+ * (simulation_variables.cuh:52-62: fluid_density, fluid_velocity), as NAGA
+ * stores them -- dimensional, rho rho0 and u c / c_s -- and computed where
+ * NAGA computes them, at the start of the last step (after its density
+ * sources; boundary velocities 0, as its bounce-back leaves them). Host
+ * out: density [N], velocity [N][dim]; either may be NULL.               */
+int naga_scene_read_macros(naga_scene* scene, float* density, float* velocity);
 /* Density sources (replace simulation_engine::register_density_source,
  * simulation_engine.cuh:80-82, and density_source::add_density_source,
  * density_source.cuh:41-82): values [n_steps][n_nodes] of the listed nodes

@@ -101,6 +101,8 @@ _SIGS = {
     "naga_scene_init_domain": ([C.c_void_p, C.c_void_p], C.c_int),
     "naga_scene_set_initial_condition": ([C.c_void_p, C.c_void_p], C.c_int),
     "naga_scene_add_probe": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "naga_scene_read_macros": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "naga_lattice": ([C.c_int, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "naga_batch_destroy": ([C.c_void_p], C.c_int),
     "naga_batch_add": ([C.c_void_p, C.c_void_p], C.c_int),
     "naga_batch_remove": ([C.c_void_p, C.c_void_p], C.c_int),
@@ -158,6 +160,17 @@ def _check(rc: int) -> None:
 
 def _p(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def lattice(dim: int):
+    """(weights [Q] float32, velocities [Q, dim] int32) in the library's
+    population order (naga_lattice)."""
+    q = C.c_int()
+    _check(lib().naga_lattice(dim, C.byref(q), None, None))
+    w = np.zeros(q.value, np.float32)
+    c = np.zeros((q.value, dim), np.int32)
+    _check(lib().naga_lattice(dim, C.byref(q), _p(w), _p(c)))
+    return w, c
 
 
 def lattice_weights(dim: int) -> np.ndarray:
@@ -292,6 +305,14 @@ class Scene:
         self.dim, self.Q = grid["dim"], Q_OF[grid["dim"]]
         self.N = keep[0].shape[0]
         self.n_probes = d.n_probes
+
+    def macros(self):
+        """(density [N], velocity [N, dim]) as NAGA's solution() holds them
+        (dimensional; computed at the start of the last step)."""
+        rho = np.zeros(self.N, np.float32)
+        u = np.zeros((self.N, self.dim), np.float32)
+        _check(lib().naga_scene_read_macros(self.h, _p(rho), _p(u)))
+        return rho, u
 
     def add_probe(self, xyz) -> int:
         """Attach one more density probe; returns its index."""

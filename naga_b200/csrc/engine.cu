@@ -1123,6 +1123,50 @@ extern "C" int naga_scene_read_state(naga_scene* s, float* g, float* drho) {
     return NAGA_OK;
 }
 
+extern "C" int naga_lattice(int dim, int* q, float* weights, int* velocities) {
+    if (dim != 2 && dim != 3) return set_error(NAGA_EINVAL, "naga_lattice: dim must be 2 or 3");
+    const int Q = dim == 2 ? D2Q9::Q : D3Q27::Q;
+    if (q) *q = Q;
+    for (int a = 0; a < Q; ++a) {
+        if (weights) weights[a] = dim == 2 ? LatticeTables<D2Q9>::w(a) : LatticeTables<D3Q27>::w(a);
+        if (velocities) {
+            if (dim == 2) {
+                velocities[a * 2] = LatticeTables<D2Q9>::cx(a);
+                velocities[a * 2 + 1] = LatticeTables<D2Q9>::cy(a);
+            } else {
+                velocities[a * 3] = LatticeTables<D3Q27>::cx(a);
+                velocities[a * 3 + 1] = LatticeTables<D3Q27>::cy(a);
+                velocities[a * 3 + 2] = LatticeTables<D3Q27>::cz(a);
+            }
+        }
+    }
+    return NAGA_OK;
+}
+
+extern "C" int naga_scene_read_macros(naga_scene* s, float* density, float* velocity) {
+    if (!s) return set_error(NAGA_EINVAL, "naga_scene_read_macros: null scene");
+    NAGA_CUDA_TRY(cudaStreamSynchronize(active_stream(s)));
+    std::vector<float4> m((size_t)s->N);
+    NAGA_CUDA_TRY(cudaMemcpy(m.data(), s->dev.M, sizeof(float4) * m.size(), cudaMemcpyDeviceToHost));
+    // NAGA stores the macros dimensional: rho rho0 and u c / c_s
+    // (detail/simulation_engine.cuh:53-82)
+    const double rho0 = s->desc.rho0;
+    const double uscale = s->desc.speed_of_sound / (double)lattice_cs_f();
+    const int D = s->dim;
+    for (int64_t i = 0; i < s->N; ++i) {
+        const float4 v = m[(size_t)i];
+        if (density) density[i] = (float)((1.0 + (double)v.x) * rho0);
+        if (velocity) {
+            // the bounce-back of the step resets the boundary nodes' stored
+            // velocity to 0 (detail/simulation_engine.cuh:874-877)
+            const bool wall = i >= s->nbl && i < s->nbl + s->nbd;
+            const float u[3] = {v.y, v.z, v.w};
+            for (int d = 0; d < D; ++d) velocity[i * D + d] = wall ? 0.f : (float)((double)u[d] * uscale);
+        }
+    }
+    return NAGA_OK;
+}
+
 extern "C" int naga_scene_write_state(naga_scene* s, const float* g) {
     if (!s || !g) return set_error(NAGA_EINVAL, "naga_scene_write_state: null argument");
     NAGA_CUDA_TRY(cudaStreamSynchronize(active_stream(s)));

@@ -79,6 +79,18 @@ int main() {
         e4.step_forward();
     }
     if (d3.density_values() != d4.density_values()) return std::puts("parameters differ"), 1;
+
+    // solution(): populations per direction and the dimensional macros
+    const auto sol = e4.solution();
+    const size_t N = nodes.points.size() / 2;
+    if (sol.lattice_distributions[0].size() != N || sol.macroscopic_values.fluid_density.size() != N ||
+        sol.macroscopic_values.fluid_velocity.size() != 2 * N)
+        return std::puts("solution sizes"), 1;
+    double mass = 0;
+    for (const auto& f : sol.lattice_distributions) mass += f[N / 2];
+    if (std::fabs(mass - 1.0) > 1e-2) return std::puts("solution populations"), 1;
+    if (std::fabs(sol.macroscopic_values.fluid_density[N / 2] / 1.1 - 1.0) > 1e-2)
+        return std::puts("solution density"), 1;
     std::puts("ok");
     return 0;
 }

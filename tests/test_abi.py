@@ -104,3 +104,13 @@ def test_cpp_facade_compiles():
     r = subprocess.run([gxx, "-std=c++17", "-fsyntax-only", f"-I{ROOT}/include", "-I/usr/local/cuda/include",
                         src], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_library_lattice_matches_oracle(naga, oracle, dim):
+    """naga_lattice: the population order and weights the library uses (and
+    read_state / write_state expose) are the oracle's, i.e. NAGA's."""
+    w, c = naga.lattice(dim)
+    oc, ow, _, _ = oracle.lattice(dim)
+    assert np.array_equal(c, oc.astype(np.int32))
+    assert np.allclose(w, ow, rtol=0, atol=1e-7)

@@ -408,3 +408,27 @@ def test_box_grid_scene_matches_oracle(naga, oracle):
     gpu.step(60)
     po = orc.step(60)
     assert rel_err(gpu.probes(0, 60), po) <= 1e-5
+
+
+def test_macros_as_naga_solution(naga, oracle):
+    """naga_scene_read_macros: the density and velocity of the last step,
+    dimensional as NAGA stores them (rho rho0, u c / c_s), equal the macros
+    of the state that step started from."""
+    g = naga.generate_grid(2, 30, 3, 15)
+    rho0, c = 1.2, 1.3
+    s = naga.Scene(g, k=16, probes=PROBES2, rho0=rho0, speed_of_sound=c)
+    s.set_density(naga.gaussian_pulse(g["points"], [0.45, 0.5], 1e-3, 0.08))
+    s.step(7)
+    gs, _ = s.state()
+    s.step(1)
+    rho, u = s.macros()
+    w, cv = naga.lattice(2)
+    drho = gs.astype(np.float64).sum(1)
+    ulat = (gs.astype(np.float64) @ cv.astype(np.float64)) / (1.0 + drho)[:, None]
+    nbl = g["n_bulk"] + g["n_layer"]
+    assert np.allclose(rho, (1.0 + drho) * rho0, rtol=0, atol=1e-6)
+    # boundary velocities are 0 after the bounce-back, as in NAGA's solution
+    assert (u[nbl:] == 0).all()
+    want = ulat[:nbl] * c * np.sqrt(3.0)
+    assert np.abs(u[:nbl] - want).max() <= 1e-6 * max(1.0, np.abs(want).max())
+    assert np.abs(u[:nbl]).max() > 0
