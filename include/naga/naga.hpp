@@ -223,6 +223,18 @@ class density_observer : public simulation_observer<Lattice> {
     const std::vector<value_type>& density_values() const { return density_values_; }
     const std::vector<value_type>& time_values() const { return time_values_; }
 
+    // density_observer::save_state / load_state (density_observer.cuh:
+    // 115-133) for a cereal-style archive (ar(values...)); the RPIM tables
+    // of the probe live in the engine's scene (its save_state)
+    template <class Archive>
+    void save_state(Archive& ar) const {
+        ar(loc_, density_values_, time_values_, time_multiplier_);
+    }
+    template <class Archive>
+    void load_state(Archive& ar) {
+        ar(loc_, density_values_, time_values_, time_multiplier_);
+    }
+
   private:
     point_t<value_type, Lattice::dimensions> loc_;
     value_type time_multiplier_;
@@ -387,6 +399,26 @@ class simulation_engine {
         std::vector<float> g(N * Q);
         detail::check(naga_scene_read_state(impl_->scene, g.data(), nullptr), "populations");
         return g;
+    }
+
+    // simulation_engine::save_state / load_state (simulation_engine.cuh:
+    // 108-116) for a cereal-style archive (ar(values...)): the scene's
+    // snapshot (populations, PML history, macros, probe ring, step count;
+    // naga_scene_save) and the engine time. Load into an engine initialised
+    // with the same domain, parameters and observers.
+    template <class Archive>
+    void save_state(Archive& ar) const {
+        impl_->ensure();
+        std::vector<unsigned char> bytes((size_t)naga_scene_snapshot_bytes(impl_->scene));
+        detail::check(naga_scene_save(impl_->scene, bytes.data(), (int64_t)bytes.size()), "save_state");
+        ar(bytes, impl_->time);
+    }
+    template <class Archive>
+    void load_state(Archive& ar) {
+        impl_->ensure();
+        std::vector<unsigned char> bytes;
+        ar(bytes, impl_->time);
+        detail::check(naga_scene_load(impl_->scene, bytes.data(), (int64_t)bytes.size()), "load_state");
     }
 
     // simulation_engine::solution() (simulation_engine.cuh:100): the

@@ -63,3 +63,9 @@ def test_facade_live_observers_and_parameters(naga):
     (naga_scene_add_probe / naga_scene_set_params underneath) agree bit for
     bit with engines that had them from the start."""
     assert _run_program(naga, "facade_live").strip() == "ok"
+
+
+def test_facade_save_and_load_state(naga):
+    """simulation_engine / density_observer save_state and load_state with a
+    cereal-style archive: the restored engine continues bit for bit."""
+    assert _run_program(naga, "facade_state").strip() == "ok"
