@@ -330,10 +330,11 @@ class simulation_engine {
         if (!impl_->sources.empty()) impl_->upload_sources(t);
         detail::check(naga_scene_step(impl_->scene, 1), "step_forward");
         if (!impl_->observers.empty()) {
-            std::vector<float> pr(impl_->observers.size());
+            std::vector<float> pr((size_t)impl_->n_probes);
             detail::check(naga_scene_read_probes(impl_->scene, t, 1, pr.data()), "step_forward");
-            for (size_t o = 0; o < pr.size(); ++o)
-                impl_->observers[o]->update(impl_->time, impl_->params.nominal_density + (value_type)pr[o]);
+            for (size_t o = 0; o < impl_->observers.size(); ++o)
+                impl_->observers[o]->update(impl_->time,
+                                            impl_->params.nominal_density + (value_type)pr[impl_->probe_of[o]]);
         }
         impl_->time += impl_->params.time_step;
     }
@@ -365,19 +366,33 @@ class simulation_engine {
     }
 
     void attach_observer(simulation_observer<Lattice>& o) {
-        impl_->observers.push_back(&o);
         if (impl_->scene) {
             // a live scene gains a probe; it samples from the next step on
             const auto l = o.location();
             std::vector<float> x(l.begin(), l.end());
             int index = 0;
             detail::check(naga_scene_add_probe(impl_->scene, x.data(), &index), "attach_observer");
+            impl_->probe_of.push_back(index);
+            impl_->n_probes = index + 1;
+        } else {
+            impl_->probe_of.push_back((int)impl_->observers.size());
         }
+        impl_->observers.push_back(&o);
     }
+    // the observer stops receiving updates; a live scene keeps its probe
+    // (and its state), as NAGA's detach only drops the observer
     void detach_observer(simulation_observer<Lattice>& o) {
         auto& v = impl_->observers;
-        v.erase(std::remove(v.begin(), v.end(), &o), v.end());
-        impl_->invalidate();
+        for (size_t k = 0; k < v.size();) {
+            if (v[k] == &o) {
+                v.erase(v.begin() + (long)k);
+                impl_->probe_of.erase(impl_->probe_of.begin() + (long)k);
+            } else {
+                ++k;
+            }
+        }
+        if (!impl_->scene)
+            for (size_t k = 0; k < v.size(); ++k) impl_->probe_of[k] = (int)k;
     }
 
     // density perturbation rho - rho0 of every node and the centred
@@ -460,6 +475,8 @@ class simulation_engine {
         simulation_domain_t domain{};
         std::vector<float> drho;
         std::vector<simulation_observer<Lattice>*> observers;
+        std::vector<int> probe_of;  // the scene probe each observer reads
+        int n_probes = 0;           // probes of the live scene
         std::vector<density_source<Lattice>*> sources;
         std::vector<value_type> terms;  // per-step source terms [N]
         std::vector<int64_t> src_nodes;
@@ -489,6 +506,7 @@ class simulation_engine {
         void invalidate() {
             if (scene) naga_scene_destroy(scene);
             scene = nullptr;
+            n_probes = 0;
         }
         void ensure() {
             if (scene) return;
@@ -527,6 +545,9 @@ class simulation_engine {
             d.probes = prb.empty() ? nullptr : prb.data();
             d.probe_capacity = 1024;
             detail::check(naga_scene_create(&d, &scene), "simulation_engine::init_domain");
+            n_probes = (int)observers.size();
+            probe_of.resize(observers.size());
+            for (size_t o = 0; o < observers.size(); ++o) probe_of[o] = (int)o;
             detail::check(naga_scene_set_density(scene, drho.data()), "simulation_engine::reset");
             time = 0;
         }

@@ -80,6 +80,20 @@ int main() {
     }
     if (d3.density_values() != d4.density_values()) return std::puts("parameters differ"), 1;
 
+    // detach on a running engine: the other observers and the state carry on
+    e1.detach_observer(a1);
+    e2.detach_observer(a2);
+    for (int s = 0; s < 3; ++s) {
+        e1.step_forward();
+        e2.step_forward();
+    }
+    if (a1.density_values().size() != 12 || a2.density_values().size() != 12)
+        return std::puts("detached observer still updated"), 1;
+    if (b1.density_values().size() != 15 || b2.density_values().size() != 9 ||
+        !std::equal(b2.density_values().begin(), b2.density_values().end(), b1.density_values().end() - 9))
+        return std::puts("observers after detach differ"), 1;
+    if (e1.populations() != e2.populations()) return std::puts("state after detach differs"), 1;
+
     // solution(): populations per direction and the dimensional macros
     const auto sol = e4.solution();
     const size_t N = nodes.points.size() / 2;
