@@ -1,5 +1,7 @@
-// Batched inverse of small dense matrices: one warp per matrix, the matrix
-// and its factors in shared memory.
+// Batched inverse of small dense matrices, one warp per matrix: FP64
+// Gauss-Jordan in registers for the stencil system sizes (19, 20, 35, 36),
+// FP64 LU in shared memory for any other n <= 64, and FP32 LU with FP64
+// residual refinement.
 //
 // Replaces linalg::batched_matrix_inverse (linalg/batched_matrix_inverse.cuh:
 // 325-397), which hands slices of the batch to cuBLAS getrfBatched +
@@ -37,6 +39,134 @@ __global__ void inverse_f64_kernel(const double* __restrict__ A, double* __restr
         warp_lu_inverse(LU, n, piv, X);
         double* o = Ainv + b * (int64_t)n * n;
         for (int e = lane; e < n * n; e += 32) o[e] = X[(e % n) * n + e / n];
+        if (info && lane == 0) info[b] = inf;
+        __syncwarp();
+    }
+}
+
+// Register-resident Gauss-Jordan inverse for the stencil system sizes
+// (n = k + D + 1: 19 / 20 for k = 16, 35 / 36 for k = 32). Lane l holds rows
+// l and l + 32 in registers. Each elimination step publishes the scaled pivot
+// row in shared memory and every lane updates its rows from it, so the n^3
+// multiply-adds are independent register FMAs rather than a chain of
+// shared-memory read-modify-writes.
+//
+// Pivoting is virtual: every row carries its getrf position (the row order
+// after the swaps so far). The pivot of step k is the first row, in that
+// order, of maximal |a| among positions >= k. That is getrf's choice, so the
+// pivot sequence and info match the LU kernel. With B = P A the matrix in
+// pivot order, the in-place sweep (pivot row scaled by p = 1 / a_kk, a_kk
+// replaced by p; every other row i: a_ij -= a_ik a_kj, a_ik = -a_ik p) leaves
+// row k of B^-1 in the row pivoted at step k. Since A^-1 = B^-1 P, the store
+// un-permutes: A^-1(k, r_m) = B^-1(k, m), with r_m the row pivoted at step m.
+//
+// Register columns rotate by one each step: at step k register j holds column
+// (k + j) mod n, so the pivot column is always register 0 and the new inverse
+// column enters at register n - 1; after n steps the order is the identity
+// again. The step loop therefore indexes no register by k.
+//
+// Measured alternatives, all slower or equal (10^6 systems of 36 x 36 on
+// B200, 18.6 ms for this form): per-row scales instead of rescaling the pivot
+// row (19.6 ms), the next pivot searched while the current step's columns
+// update (19.6-19.9 ms), a vote-and-shuffle fast path for a unique maximum
+// (19.3 ms), the step loop fully unrolled without rotation (25.3 ms at 228
+// registers).
+constexpr int kGjWarps = 2;
+
+template <int N>
+__global__ void __launch_bounds__(32 * kGjWarps, (N > 32 ? 5 : 8))
+    inverse_gj_kernel(const double* __restrict__ A, double* __restrict__ Ainv, int64_t batch,
+                      int* __restrict__ info) {
+    constexpr int S = (N + 31) / 32;
+    constexpr int NP = (N + 1) & ~1;
+    // per warp: the published pivot row (double-buffered by step parity) and
+    // the physical row pivoted at each step
+    __shared__ __align__(16) double prow[kGjWarps][2][NP];
+    __shared__ int rowk[kGjWarps][N];
+    const int w = threadIdx.x >> 5, lane = lane_id();
+    const int64_t nw = (int64_t)gridDim.x * kGjWarps;
+    for (int64_t b = (int64_t)blockIdx.x * kGjWarps + w; b < batch; b += nw) {
+        const double* ai = A + b * (int64_t)(N * N);
+        double a[S][N];
+        int pos[S];
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            const int r = lane + 32 * s;
+            pos[s] = r < N ? r : N;  // N marks a padding row
+#pragma unroll
+            for (int c = 0; c < N; ++c) a[s][c] = r < N ? ai[r + N * c] : 0.0;
+        }
+        int inf = 0;
+#pragma unroll 1
+        for (int k = 0; k < N; ++k) {
+            // pivot: max |a| over positions >= k, ties to the lowest position.
+            // |a| >= 0, so its bits order like unsigned integers.
+            unsigned hi = 0, lo = 0;
+            int bp = N;
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                const unsigned long long v = (unsigned long long)__double_as_longlong(fabs(a[s][0]));
+                const unsigned h = (unsigned)(v >> 32), l = (unsigned)v;
+                const bool better = h > hi || (h == hi && (l > lo || (l == lo && pos[s] < bp)));
+                if (pos[s] >= k && pos[s] < N && better) {
+                    hi = h;
+                    lo = l;
+                    bp = pos[s];
+                }
+            }
+            const unsigned mh = __reduce_max_sync(kFull, hi);
+            const unsigned ml = __reduce_max_sync(kFull, hi == mh ? lo : 0u);
+            const int bpos = __reduce_min_sync(kFull, (hi == mh && lo == ml) ? bp : N);
+            const bool zero = (mh | ml) == 0u;
+            if (zero && !inf) inf = k + 1;
+            bool piv[S];
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                piv[s] = pos[s] == bpos;
+                pos[s] = pos[s] == k ? bpos : (piv[s] ? k : pos[s]);
+            }
+            // the pivot row's owner scales it and publishes it rotated:
+            // pr[m] = a_r(m + 1) p for m < N - 1, pr[N - 1] = p
+            double* pr = prow[w][k & 1];
+#pragma unroll
+            for (int s = 0; s < S; ++s)
+                if (piv[s]) {
+                    rowk[w][k] = lane + 32 * s;
+                    const double p = zero ? 0.0 : 1.0 / a[s][0];
+                    a[s][0] = p;
+#pragma unroll
+                    for (int j = 1; j < N; ++j) a[s][j] *= p;
+#pragma unroll
+                    for (int m = 0; m + 1 < N; m += 2)
+                        *reinterpret_cast<double2*>(pr + m) = make_double2(a[s][m + 1], m + 2 < N ? a[s][m + 2] : p);
+                    if (N & 1) pr[N - 1] = p;
+                }
+            __syncwarp();
+            // every row: a_i(m) = a_i(m + 1) - f_i pr[m] (rotated), the new
+            // column -f_i p; the pivot row (f = 0) only rotates, keeping p
+            double f[S], l[S];
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                f[s] = piv[s] ? 0.0 : a[s][0];
+                l[s] = piv[s] ? a[s][0] : 0.0;
+            }
+#pragma unroll
+            for (int m = 0; m < N; m += 2) {
+                const double2 q = *reinterpret_cast<const double2*>(pr + m);
+#pragma unroll
+                for (int s = 0; s < S; ++s) {
+                    a[s][m] = fma(-f[s], q.x, m + 1 < N ? a[s][m + 1] : l[s]);
+                    if (m + 1 < N) a[s][m + 1] = fma(-f[s], q.y, m + 2 < N ? a[s][m + 2] : l[s]);
+                }
+            }
+        }
+        __syncwarp();
+        double* o = Ainv + b * (int64_t)(N * N);
+#pragma unroll
+        for (int s = 0; s < S; ++s)
+            if (lane + 32 * s < N)
+#pragma unroll
+                for (int j = 0; j < N; ++j) o[pos[s] + N * rowk[w][j]] = a[s][j];
         if (info && lane == 0) info[b] = inf;
         __syncwarp();
     }
@@ -129,6 +259,20 @@ __global__ void inverse_f32r_kernel(const double* __restrict__ A, double* __rest
     }
 }
 
+template <int N>
+int launch_gj(const double* A, double* Ainv, int64_t batch, int* info, cudaStream_t st) {
+    static int per_sm = 0;
+    if (per_sm < 1) {
+        NAGA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, inverse_gj_kernel<N>, 32 * kGjWarps, 0));
+        per_sm = std::max(per_sm, 1);
+    }
+    const int64_t need = (batch + kGjWarps - 1) / kGjWarps;
+    const int blocks = (int)std::min<int64_t>(need, (int64_t)sm_count() * per_sm);
+    inverse_gj_kernel<N><<<blocks, 32 * kGjWarps, 0, st>>>(A, Ainv, batch, info);
+    NAGA_CUDA_TRY(cudaGetLastError());
+    return NAGA_OK;
+}
+
 }  // namespace
 
 int batched_inverse(const double* A, double* Ainv, int n, int64_t batch, int* info, bool refined, int max_iter,
@@ -137,6 +281,13 @@ int batched_inverse(const double* A, double* Ainv, int n, int64_t batch, int* in
     if (batch < 0) return set_error(NAGA_EINVAL, "batched inverse: negative batch");
     if (batch == 0) return NAGA_OK;
     if (!A || !Ainv) return set_error(NAGA_EINVAL, "batched inverse: null pointer");
+    if (!refined) switch (n) {
+            case 19: return launch_gj<19>(A, Ainv, batch, info, st);
+            case 20: return launch_gj<20>(A, Ainv, batch, info, st);
+            case 35: return launch_gj<35>(A, Ainv, batch, info, st);
+            case 36: return launch_gj<36>(A, Ainv, batch, info, st);
+            default: break;
+        }
     const size_t per_warp = (refined ? (size_t)24 : (size_t)16) * n * n + 16 * ((n + 3) / 4);
     const size_t lim = smem_limit();
     int wpb = (int)std::min<size_t>(8, lim / per_warp);

@@ -93,15 +93,25 @@ def _rbf_systems(n_sys, seed=0):
     return G  # symmetric: column-major storage equals row-major
 
 
-@pytest.mark.parametrize("n", [3, 19, 36, 64])
+def _assert_inverse_close(out, ref, A):
+    """A stable inverse is accurate to a small multiple of eps * cond(A)
+    (relative, max-norm). The GPU kernels (LU for most sizes, register
+    Gauss-Jordan for the stencil sizes) and the oracle's LU round
+    differently, so they agree to that bound rather than bit for bit; the
+    largest ratio seen over these batches is about 0.6."""
+    kappa = np.linalg.cond(A)
+    err = np.abs(out - ref).max(axis=(1, 2)) / np.abs(ref).max(axis=(1, 2))
+    assert (err <= 4 * np.finfo(np.float64).eps * kappa).all(), float((err / kappa).max())
+
+
+@pytest.mark.parametrize("n", [3, 19, 20, 35, 36, 64])
 def test_inverse_matches_oracle(naga, oracle, n):
     rng = np.random.default_rng(n)
     A = rng.standard_normal((300, n, n)) + 3 * np.eye(n)
     out, info = naga.batched_inverse_f64(_t(A))
     ref, rinfo = oracle.batched_inverse(A)
     assert (_np(info) == 0).all()
-    err = np.abs(_np(out) - ref).max() / np.abs(ref).max()
-    assert err < 1e-12
+    _assert_inverse_close(_np(out), ref, A)
 
 
 def test_inverse_rbf_systems_f64_and_refined(naga, oracle):
@@ -219,3 +229,23 @@ def test_inverse_singular_and_empty(naga, oracle):
     assert np.abs(_np(out)[ok] - ref[ok]).max() / np.abs(ref[ok]).max() < 1e-12
     out0, info0 = naga.batched_inverse_f64(torch.empty((0, n, n), dtype=torch.float64, device="cuda"))
     assert tuple(out0.shape) == (0, n, n) and tuple(info0.shape) == (0,)
+
+
+@pytest.mark.parametrize("n", [19, 36])
+def test_inverse_register_sizes_singular_and_ties(naga, oracle, n):
+    """The stencil sizes take the register Gauss-Jordan kernel: a zero
+    column reports getrf's info; integer matrices (many equal |a| pivot
+    candidates) and a batch that is not a multiple of the warps per block
+    still match the oracle."""
+    rng = np.random.default_rng(n)
+    A = rng.standard_normal((7, n, n)) + 3 * np.eye(n)
+    A[2, n // 2, :] = 0.0  # column n/2 + 1 of matrix 2
+    A[4] = np.round(2 * A[4])
+    A[5] = rng.integers(-2, 3, (n, n)) + 6 * np.eye(n)
+    out, info = naga.batched_inverse_f64(_t(A))
+    ref, rinfo = oracle.batched_inverse(A)
+    info = _np(info)
+    assert info[2] == rinfo[2] == n // 2 + 1
+    ok = [b for b in range(7) if b != 2]
+    assert (info[ok] == 0).all()
+    _assert_inverse_close(_np(out)[ok], ref[ok], A[ok])
