@@ -103,7 +103,10 @@ int naga_gaussian_pulse(const float* points, int64_t n, int dim,
  * arrays: src [n][dim], qry [nq][dim] float; idx, d2 [nq][k] (ascending).
  * With fewer than k sources the slots past the n found hold index
  * 0xffffffff and d2 = +inf (NAGA prints a warning and leaves them unset,
- * segmentation/nearest_neighbors.cuh:421-425). nq = 0 is a no-op.
+ * segmentation/nearest_neighbors.cuh:421-425). nq = 0 is a no-op. A NaN or
+ * infinite source coordinate returns NAGA_EINVAL before the search runs
+ * (so does every call that builds stencils from points: the divergence
+ * build, scene creation and probes).
  * Replaces nd_cubic_segmentation<T,D>(points, approx_size)
  * (segmentation/nd_cubic_segmentation.cuh:227-303) followed by
  * batched_nearest_neighbors(k, query_map, segmentation)

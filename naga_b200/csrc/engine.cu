@@ -741,6 +741,19 @@ extern "C" int naga_scene_create(const naga_scene_desc* d, naga_scene** out) {
     if (!d->points || (d->n_boundary > 0 && !d->normals) || (d->n_layer > 0 && !d->sigma) ||
         (d->n_probes > 0 && !d->probes) || d->n_probes < 0)
         return set_error(NAGA_EINVAL, "naga_scene_create: missing input array");
+    {
+        // non-finite inputs would reach the kNN as coordinates or as queries
+        auto finite = [](const float* v, int64_t m) {
+            for (int64_t t = 0; t < m; ++t)
+                if (!std::isfinite(v[t])) return false;
+            return true;
+        };
+        if (!finite(d->points, N * d->dim) || (d->n_boundary > 0 && !finite(d->normals, d->n_boundary * d->dim)) ||
+            (d->n_layer > 0 && !finite(d->sigma, d->n_layer)) ||
+            (d->n_probes > 0 && !finite(d->probes, (int64_t)d->n_probes * d->dim)))
+            return set_error(NAGA_EINVAL,
+                             "naga_scene_create: non-finite point coordinates, normals, absorption or probe positions");
+    }
     if (!(d->nodal_spacing > 0) || !(d->time_step > 0) || !(d->speed_of_sound > 0) || !(d->rho0 > 0) ||
         !(d->viscosity >= 0))
         return set_error(NAGA_EINVAL, "naga_scene_create: physical parameters must be positive");
@@ -872,6 +885,8 @@ void release(naga_scene* s, void* p) {
 extern "C" int naga_scene_add_probe(naga_scene* s, const float* xyz, int* index) {
     if (!s || !xyz) return set_error(NAGA_EINVAL, "naga_scene_add_probe: null argument");
     if (!s->d_pts) return set_error(NAGA_EINVAL, "naga_scene_add_probe: scene has no domain");
+    for (int d = 0; d < s->dim; ++d)
+        if (!std::isfinite(xyz[d])) return set_error(NAGA_EINVAL, "naga_scene_add_probe: non-finite probe position");
     cudaStream_t st = active_stream(s);
     NAGA_CUDA_TRY(cudaStreamSynchronize(st));
     const int D = s->dim;

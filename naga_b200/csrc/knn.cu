@@ -356,6 +356,12 @@ int knn_run(const float* src, const int64_t* h_src_off, int nclouds, const float
         for (int d = 0; d < D; ++d) {
             lo[d] = n > 0 ? (double)ord2f(hb[c * 6 + d]) : 0.0;
             hi[d] = n > 0 ? (double)ord2f(hb[c * 6 + 3 + d]) : 1.0;
+            // a NaN or infinite coordinate always lands in a bound (the
+            // ordered-integer min / max puts NaN at one end)
+            if (!std::isfinite(lo[d]) || !std::isfinite(hi[d])) {
+                rc = set_error(NAGA_EINVAL, "naga_knn: non-finite point coordinates in cloud " + std::to_string(c));
+                goto done;
+            }
             if (hi[d] - lo[d] < 1e-6) hi[d] = lo[d] + 1e-6;
             vol *= hi[d] - lo[d];
         }
@@ -544,6 +550,8 @@ int knn_noalloc_run(const float* src, int64_t n, const float* qry, int64_t nq, i
     for (int d = 0; d < D; ++d) {
         lo[d] = n > 0 ? (double)ord2f(hb[d]) : 0.0;
         hi[d] = n > 0 ? (double)ord2f(hb[3 + d]) : 1.0;
+        if (!std::isfinite(lo[d]) || !std::isfinite(hi[d]))
+            return set_error(NAGA_EINVAL, "naga_knn_noalloc: non-finite point coordinates");
         if (hi[d] - lo[d] < 1e-6) hi[d] = lo[d] + 1e-6;
         vol *= hi[d] - lo[d];
     }

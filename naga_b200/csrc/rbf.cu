@@ -350,16 +350,19 @@ namespace {
 // the support coordinates, shifted to x_i and divided by the spacing, go to
 // xs (shared); lane t keeps support index t (and t + 32) and its squared
 // distance; delta is the interaction radius 0.05 |x_i - x_nn|
-// (operators.cuh:84-117).
+// (operators.cuh:84-117). A support index outside [0, n) (a kNN sentinel)
+// is replaced by i and reported in bad (warp-uniform).
 template <int D>
 struct NodeStencil {
     uint32_t jl[2];
     double r2own[2];
     double delta, sp;
+    bool bad;
 };
 template <int D>
-__device__ __forceinline__ NodeStencil<D> load_node(const float* __restrict__ pts, const uint32_t* __restrict__ idx,
-                                                    int k, int64_t i, double sp, double* xs) {
+__device__ __forceinline__ NodeStencil<D> load_node(const float* __restrict__ pts, int64_t n,
+                                                    const uint32_t* __restrict__ idx, int k, int64_t i, double sp,
+                                                    double* xs) {
     const int lane = lane_id();
     NodeStencil<D> ns;
     ns.sp = sp;
@@ -368,8 +371,11 @@ __device__ __forceinline__ NodeStencil<D> load_node(const float* __restrict__ pt
     for (int d = 0; d < D; ++d) xi[d] = (double)pts[i * D + d];
     ns.jl[0] = ns.jl[1] = 0;
     ns.r2own[0] = ns.r2own[1] = 0;
+    bool bad = false;
     for (int t = lane, r = 0; t < k; t += 32, ++r) {
-        const uint32_t j = idx[i * k + t];
+        const uint32_t jr = idx[i * k + t];
+        bad = bad || (int64_t)jr >= n;
+        const uint32_t j = (int64_t)jr < n ? jr : (uint32_t)i;
         ns.jl[r] = j;
         double rr = 0;
 #pragma unroll
@@ -381,6 +387,7 @@ __device__ __forceinline__ NodeStencil<D> load_node(const float* __restrict__ pt
         ns.r2own[r] = rr;
     }
     ns.delta = 0.05 * sqrt(__shfl_sync(kFull, ns.r2own[0], 1));
+    ns.bad = __any_sync(kFull, bad);
     __syncwarp();
     return ns;
 }
@@ -462,7 +469,8 @@ __global__ void divergence_build_kernel(const float* __restrict__ pts, int64_t n
     const int nsys = k + D + 1;
     WarpSmem s = carve(smem + rbf_smem_per_warp(nsys, k, D, precision) * w, nsys, k, D, precision);
     for (int64_t i = (int64_t)blockIdx.x * wpb + w; i < n; i += (int64_t)gridDim.x * wpb) {
-        const NodeStencil<D> ns = load_node<D>(pts, idx, k, i, spacing[i / spacing_batch], s.xs);
+        const NodeStencil<D> ns = load_node<D>(pts, n, idx, k, i, spacing[i / spacing_batch], s.xs);
+        if (ns.bad && lane == 0) atomicOr(status, 1);
         build_G0<D>(s.xs, k, shape, s.G);
         double b0[D], b1[D], cself[D];
         quad_rhs<D>(s.xs, k, nsys, shape, ns, b0, b1, cself);
@@ -602,11 +610,17 @@ __device__ int aug_lu(double* A, double* rdiag) {
     const bool has1 = p1 < N, has2 = lane < OFF;
     int info = 0;
     for (int j = 0; j < N; ++j) {
+        // NaN never becomes a candidate, so the comparisons order totally and
+        // every lane ends with the same pivot; lane 0's is broadcast anyway,
+        // and a column with no candidate (all NaN) pivots on its own row
         double best = -1.0;
         int bi = N;
         if (has2 && lane >= j) {
-            best = fabs(A[lane * LD + j]);
-            bi = lane;
+            const double v = fabs(A[lane * LD + j]);
+            if (v > best) {
+                best = v;
+                bi = lane;
+            }
         }
         if (has1 && p1 >= j) {
             const double v = fabs(A[p1 * LD + j]);
@@ -624,7 +638,8 @@ __device__ int aug_lu(double* A, double* rdiag) {
                 bi = oi;
             }
         }
-        const int p = bi;
+        bi = __shfl_sync(kFull, bi, 0);
+        const int p = bi < N ? bi : j;
         if (A[p * LD + j] == 0.0) {
             if (!info) info = j + 1;
             if (lane == 0) rdiag[j] = 0.0;
@@ -663,7 +678,8 @@ __global__ void divergence_build_fixed_kernel(const float* __restrict__ pts, int
     const int p1 = OFF + lane;
     const bool has1 = p1 < N, has2 = lane < OFF;
     for (int64_t i = (int64_t)blockIdx.x * wpb + w; i < n; i += (int64_t)gridDim.x * wpb) {
-        const NodeStencil<D> ns = load_node<D>(pts, idx, KC, i, spacing[i / spacing_batch], xs);
+        const NodeStencil<D> ns = load_node<D>(pts, n, idx, KC, i, spacing[i / spacing_batch], xs);
+        if (ns.bad && lane == 0) atomicOr(status, 1);
         build_G0_rows<D, KC>(xs, shape, A);
         double b0[D], b1[D], cself[D];
         quad_rhs<D>(xs, KC, N, shape, ns, b0, b1, cself);
@@ -864,6 +880,7 @@ int divergence_build_device(const float* pts, int64_t n, int dim, int k, int sha
     cudaFreeAsync(nn, st);
     cudaFreeAsync(sp, st);
     cudaFreeAsync(d_status, st);
+    if (h_status & 1) return set_error(NAGA_EINVAL, "divergence build: support index out of range");
     if (h_status & 2) return set_error(NAGA_ESINGULAR, "divergence build: singular moment matrix");
     return NAGA_OK;
 }

@@ -36,7 +36,11 @@ __device__ int warp_lu(T* A, int n, int* piv) {
                 bi = oi;
             }
         }
-        const int p = bi;
+        // NaN is never a candidate (v > best fails), so the order is total
+        // and the lanes agree; lane 0's choice is broadcast anyway, and a
+        // column with no candidate (all NaN) pivots on its own row
+        bi = __shfl_sync(kFull, bi, 0);
+        const int p = bi < n ? bi : j;
         if (lane == 0) piv[j] = p;
         const T pv = A[p + n * j];
         if (pv == T(0)) {

@@ -193,6 +193,30 @@ def test_knn_edge_sizes(naga, oracle, dim):
         assert (oi[:, n:] == 0xFFFFFFFF).all() and np.isinf(od[:, n:]).all()
 
 
+def test_nonfinite_coordinates_are_rejected(naga):
+    """NaN or infinite point coordinates are an input error (NAGA_EINVAL)
+    found at the kNN's bounding box, before any search or stencil kernel
+    sees them: plain and batched kNN, the divergence build and scene
+    creation; the context stays usable."""
+    rng = np.random.default_rng(5)
+    pts = rng.random((2000, 3)).astype(np.float32)
+    for bad in (np.nan, np.inf, -np.inf):
+        p = pts.copy()
+        p[123, 1] = bad
+        with pytest.raises(naga.NagaError, match="non-finite"):
+            naga.knn(_t(p), _t(pts[:10]), 8)
+        with pytest.raises(naga.NagaError, match="non-finite"):
+            naga.knn_clouds(_t(np.concatenate([pts[:500], p[:300]])), np.array([0, 500, 800]), 8)
+        with pytest.raises(naga.NagaError, match="non-finite"):
+            naga.divergence_build(_t(p), 32, 0)
+    g = naga.generate_grid(2, 30, 4, 0)
+    g["points"][7, 0] = np.nan
+    with pytest.raises(naga.NagaError, match="non-finite"):
+        naga.Scene(g, k=16)
+    idx, _ = naga.knn(_t(pts), _t(pts[:10]), 8)
+    assert (_np(idx)[:, 0] == np.arange(10)).all()
+
+
 def test_knn_clouds_ragged(naga, oracle):
     """Clouds back to back with an empty cloud and clouds smaller than k
     between full ones: each equals its own search."""
@@ -229,6 +253,25 @@ def test_inverse_singular_and_empty(naga, oracle):
     assert np.abs(_np(out)[ok] - ref[ok]).max() / np.abs(ref[ok]).max() < 1e-12
     out0, info0 = naga.batched_inverse_f64(torch.empty((0, n, n), dtype=torch.float64, device="cuda"))
     assert tuple(out0.shape) == (0, n, n) and tuple(info0.shape) == (0,)
+
+
+@pytest.mark.parametrize("n", [9, 36])
+def test_inverse_nan_matrices_leave_the_batch_intact(naga, oracle, n):
+    """Matrices with NaN entries (all of them, or one) in the middle of a
+    batch: their results are not finite and their neighbours still match
+    the oracle, on the shared-memory LU (n = 9) and the register
+    Gauss-Jordan kernel (n = 36)."""
+    rng = np.random.default_rng(n + 1)
+    A = rng.standard_normal((5, n, n)) + 3 * np.eye(n)
+    A[1] = np.nan
+    A[3, 2, 5] = np.nan
+    out, info = naga.batched_inverse_f64(_t(A))
+    out, info = _np(out), _np(info)
+    ok = [0, 2, 4]
+    ref, _ = oracle.batched_inverse(A[ok])
+    assert (info[ok] == 0).all()
+    _assert_inverse_close(out[ok], ref, A[ok])
+    assert not np.isfinite(out[1]).any() and not np.isfinite(out[3]).all()
 
 
 @pytest.mark.parametrize("n", [19, 36])

@@ -57,3 +57,21 @@ def test_knn_noalloc_rejects_clouds_beyond_its_scratch(naga):
     rc, _, _ = _noalloc(naga, src, qry, 4)
     assert rc == naga.NAGA_EINVAL
     assert b"65536" in naga.lib().naga_last_error()
+
+
+def test_knn_noalloc_rejects_nonfinite_coordinates(naga):
+    """A NaN or infinite source coordinate is an input error found at the
+    bounding box, before the search runs; the next call is unaffected."""
+    rng = np.random.default_rng(12)
+    src = rng.random((3000, 3)).astype(np.float32)
+    qry = rng.random((50, 3)).astype(np.float32)
+    for bad in (np.nan, np.inf, -np.inf):
+        s = src.copy()
+        s[17, 2] = bad
+        rc, _, _ = _noalloc(naga, s, qry, 8)
+        assert rc == naga.NAGA_EINVAL
+        assert b"non-finite" in naga.lib().naga_last_error()
+    rc, idx, d2 = _noalloc(naga, src, qry, 8)
+    assert rc == naga.NAGA_OK
+    ri, rd = _reference(naga, src, qry, 8)
+    assert np.array_equal(idx, ri) and np.array_equal(d2, rd)
