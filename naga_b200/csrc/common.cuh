@@ -27,24 +27,29 @@ int sm_count();
 // d3q27_lattice.cuh:45-98,380-387 and d2q9_lattice.cuh:44-82,142-155). The
 // numeric tables are part of the collision model and are identical to the
 // reference's.
-// Node rows in HBM hold the populations in a "paired" order: after the rest
-// population and one pad, every direction is followed by its opposite, so a
-// float4 chunk holds two opposite pairs (c and -c share |c . W| in the
-// streaming gather, and bounce-back swaps within a chunk). row(slot) is the
+// Node rows in HBM hold the populations in a "paired" order: every
+// direction is followed by its opposite, so a float4 chunk holds two
+// opposite pairs (c and -c share |c . W| in the streaming gather, and
+// bounce-back swaps within a chunk). D3Q27 starts with the rest population
+// and one pad; D2Q9 puts its four pairs in the first two chunks and the rest
+// population (zero streaming rate) with three pads in the third, so its RK
+// stages and PML gather never touch the third chunk. row(slot) is the
 // population stored in a slot (-1: pad), pos(a) the slot of population a.
 struct D2Q9 {
     static constexpr int D = 2, Q = 9, QP = 12;  // QP: padded row (3 x float4)
+    static constexpr int NGATHER = 2;             // chunks with a nonzero streaming rate
     static constexpr __host__ __device__ int row(int slot) {
-        constexpr int t[12] = {0, -1, 1, 5, 2, 6, 3, 7, 4, 8, -1, -1};
+        constexpr int t[12] = {1, 5, 2, 6, 3, 7, 4, 8, 0, -1, -1, -1};
         return t[slot];
     }
     static constexpr __host__ __device__ int pos(int a) {
-        constexpr int t[9] = {0, 2, 4, 6, 8, 3, 5, 7, 9};
+        constexpr int t[9] = {8, 0, 2, 4, 6, 1, 3, 5, 7};
         return t[a];
     }
 };
 struct D3Q27 {
     static constexpr int D = 3, Q = 27, QP = 28;  // QP: padded row (7 x float4)
+    static constexpr int NGATHER = 7;              // chunk 0 holds the rest population and a pair
     static constexpr __host__ __device__ int row(int slot) {
         constexpr int t[28] = {0,  -1, 1,  2,  3,  4,  5,  6,  7,  10, 8,  9,  11, 14,
                                12, 13, 15, 18, 16, 17, 19, 26, 20, 25, 21, 24, 22, 23};

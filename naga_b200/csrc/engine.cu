@@ -1043,8 +1043,11 @@ extern "C" int naga_scene_set_density_source(naga_scene* s, const int64_t* nodes
 // buffer), the host step count and the probe ring. Tables are not included:
 // they are rebuilt from the description.
 namespace {
+constexpr int32_t kSnapshotVersion = 2;
 struct SnapshotHeader {
     char magic[8];  // "NAGASNP1"
+    // 2: D2Q9 rows with the pairs first and the rest population in the
+    // third chunk (1 had the rest population first)
     int32_t version, dim, qp, n_probes;
     int64_t n, probe_cap, steps;
     uint64_t device_step;
@@ -1069,7 +1072,7 @@ extern "C" int naga_scene_save(naga_scene* s, void* buf, int64_t cap) {
     NAGA_CUDA_TRY(cudaStreamSynchronize(st));
     SnapshotHeader h{};
     std::memcpy(h.magic, "NAGASNP1", 8);
-    h.version = 1;
+    h.version = kSnapshotVersion;
     h.dim = s->dim;
     h.qp = s->QP;
     h.n_probes = s->dev.np;
@@ -1097,7 +1100,7 @@ extern "C" int naga_scene_load(naga_scene* s, const void* buf, int64_t size) {
     if (size < (int64_t)sizeof(SnapshotHeader)) return set_error(NAGA_EINVAL, "naga_scene_load: truncated snapshot");
     SnapshotHeader h;
     std::memcpy(&h, buf, sizeof h);
-    if (std::memcmp(h.magic, "NAGASNP1", 8) != 0 || h.version != 1)
+    if (std::memcmp(h.magic, "NAGASNP1", 8) != 0 || h.version != kSnapshotVersion)
         return set_error(NAGA_EINVAL, "naga_scene_load: not a snapshot of this format");
     if (h.dim != s->dim || h.qp != s->QP || h.n != s->N || h.n_probes != s->dev.np || h.probe_cap != s->dev.probe_cap ||
         h.payload != snapshot_payload(s))

@@ -66,12 +66,40 @@ struct MT {
     static constexpr int NPB = kBlockMT / TPN;     // nodes per block pass
 };
 
+// Thread shapes of the pipelined gather kernels: TPN threads per node,
+// thread c owning float4 chunk c, passes of MT<L>::NPB nodes (the tables'
+// pass order), blocks of NPB * TPN threads. D2Q9 runs without an idle lane:
+// its RK stages and PML gather touch only the two pair chunks that carry a
+// direction (L::NGATHER), its filter and boundary kernels the three chunks
+// of the row (256-scene batch: 1725 -> 2053 MNUPS over four threads per
+// node). D3Q27 keeps eight threads for its seven chunks: at seven, nodes
+// straddle warps and every 128-B row is requested by two warps (RK stage
+// 80 -> 107 us, step 458 -> 361 MNUPS).
+template <class L, int TPN_>
+struct Shape {
+    static constexpr int TPN = TPN_;
+    static constexpr int NCH = L::QP / 4;
+    static constexpr int NPB = MT<L>::NPB;
+    static constexpr int BLOCK = NPB * TPN;
+};
+template <class L>
+using MTR = Shape<L, L::D == 3 ? 8 : L::NGATHER>;  // RK stages, PML gather
+template <class L>
+using MTF = Shape<L, L::D == 3 ? 8 : L::QP / 4>;   // filter, boundary kernels
+
+// blocks per SM of the MTF-shaped kernels for the RK stages' tuned bps: the
+// same threads per SM
+template <class L>
+constexpr int other_bps(int bps) {
+    return (bps * MTR<L>::BLOCK + MTF<L>::BLOCK - 1) / MTF<L>::BLOCK;
+}
+
 // direction of the first population of each slot pair of a row
 // ((0, pad) and (pad, pad) pairs have zero direction)
 __constant__ float c_pdir3[14][3] = {{0, 0, 0},  {1, 0, 0},  {0, 1, 0},   {0, 0, 1},  {1, 1, 0},
                                      {-1, 1, 0}, {1, 0, 1},  {-1, 0, 1},  {0, 1, 1},  {0, -1, 1},
                                      {1, 1, 1},  {-1, 1, 1}, {1, -1, 1},  {-1, -1, 1}};
-__constant__ float c_pdir2[6][3] = {{0, 0, 0}, {-1, 1, 0}, {-1, 0, 0}, {-1, -1, 0}, {0, -1, 0}, {0, 0, 0}};
+__constant__ float c_pdir2[6][3] = {{-1, 1, 0}, {-1, 0, 0}, {-1, -1, 0}, {0, -1, 0}, {0, 0, 0}, {0, 0, 0}};
 
 template <class L>
 __device__ __forceinline__ void pair_dirs(int c, float* d0, float* d1) {
@@ -811,9 +839,9 @@ struct EdgeSrc {  // boundary interpolation records
 // over the node's layer supports (set-up). Adds to S1 and, on
 // interpolation sources, S1P.
 template <class L, int K>
-__global__ void __launch_bounds__(kBlockMT) k_pml_gather(const WorkItem* __restrict__ items, int nitems,
-                                                         const SceneDev* __restrict__ scenes) {
-    using G = MT<L>;
+__global__ void __launch_bounds__(MTR<L>::BLOCK) k_pml_gather(const WorkItem* __restrict__ items, int nitems,
+                                                              const SceneDev* __restrict__ scenes) {
+    using G = MTR<L>;  // like the RK stages: only the L::NGATHER chunks carry a term
     constexpr int QP = L::QP, K_ = K;
     const int c = threadIdx.x % G::TPN, ns = threadIdx.x / G::TPN;
     float d0[3], d1[3];
@@ -822,7 +850,8 @@ __global__ void __launch_bounds__(kBlockMT) k_pml_gather(const WorkItem* __restr
     const int k = K > 0 ? K : S.k;
     const int nn = (int)(it.end - it.begin);
     const int64_t i = (int64_t)it.begin + ns;
-    if (ns < nn && c < G::NCH) {
+    // chunks past NGATHER carry no direction (their term is zero)
+    if (ns < nn && c < L::NGATHER) {
         float4 dv = make_float4(0.f, 0.f, 0.f, 0.f);
         // the node's layer supports lead its records (in stencil order) and
         // their count rides in V1.w: no per-support layer test
@@ -900,9 +929,9 @@ __device__ __forceinline__ float4 edge_sum(const float2* tile, int kb, int nn, i
 }
 
 template <class L, int KB>
-__global__ void __launch_bounds__(kBlockMT, 5) k_edge_collide(const WorkItem* __restrict__ items, int nitems,
+__global__ void __launch_bounds__(MTF<L>::BLOCK, 5) k_edge_collide(const WorkItem* __restrict__ items, int nitems,
                                                            const SceneDev* __restrict__ scenes) {
-    using G = MT<L>;
+    using G = MTF<L>;
     constexpr int QP = L::QP, K_ = KB;
     const int c = threadIdx.x % G::TPN, ns = threadIdx.x / G::TPN;
     NAGA_PIPE_BEGIN(float2, (tile_cap<G::NPB, KB>()), EdgeSrc{})
@@ -921,9 +950,9 @@ __global__ void __launch_bounds__(kBlockMT, 5) k_edge_collide(const WorkItem* __
 // 1233-1323); boundary: bounce-back f_a <- f_bb(a) where c_a . n > 0
 // (:789-944), a swap within each opposite pair; ghost: copy
 template <class L, int K>
-__global__ void __launch_bounds__(kBlockMT) k_filter(const WorkItem* __restrict__ items, int nitems,
-                                                     const SceneDev* __restrict__ scenes) {
-    using G = MT<L>;
+__global__ void __launch_bounds__(MTF<L>::BLOCK) k_filter(const WorkItem* __restrict__ items, int nitems,
+                                                          const SceneDev* __restrict__ scenes) {
+    using G = MTF<L>;
     constexpr int QP = L::QP, K_ = K;
     // (weight, index) filter records, 8 B each
     using T = float2;
@@ -991,9 +1020,9 @@ __global__ void __launch_bounds__(kBlockMT) k_filter(const WorkItem* __restrict_
 // their stage values equal the step's start values, which the filter kernel
 // also wrote into the stage buffers G1 and G2.
 template <class L, int K, int STAGE>
-__global__ void __launch_bounds__(kBlockMT) k_rk(const WorkItem* __restrict__ items, int nitems,
-                                                 const SceneDev* __restrict__ scenes) {
-    using G = MT<L>;
+__global__ void __launch_bounds__(MTR<L>::BLOCK) k_rk(const WorkItem* __restrict__ items, int nitems,
+                                                      const SceneDev* __restrict__ scenes) {
+    using G = MTR<L>;
     // D3Q27 tiles hold (Wx, Wy, Wz, index) records; D2Q9 tiles the
     // (Wx, Wy, index) triplets, three floats per record
     constexpr bool D2 = L::D == 2;
@@ -1007,7 +1036,10 @@ __global__ void __launch_bounds__(kBlockMT) k_rk(const WorkItem* __restrict__ it
     const int k = K > 0 ? K : S.k;
     const int nn = (int)(it.end - it.begin);
     const int64_t i = (int64_t)it.begin + ns;
-    if (ns < nn && c < G::NCH) {
+    // chunks past NGATHER (D2Q9's rest population and pads) have zero rate:
+    // their stage values equal g, G keeps them and no gather reads them
+    // from the stage buffers
+    if (ns < nn && c < L::NGATHER) {
         // Horner stages: G1 = g + dt/4 A g, G2 = g + dt/3 A G1, G1 = g + dt/2 A G2,
         // G = g + dt A G1
         const float* src = (STAGE == 1) ? S.G : (STAGE == 2) ? S.G1 : (STAGE == 3) ? S.G2 : S.G1;
@@ -1043,9 +1075,9 @@ __global__ void __launch_bounds__(kBlockMT) k_rk(const WorkItem* __restrict__ it
 
 // boundary: f = interp(f of bulk + layer) (simulation_engine.cuh:1370)
 template <class L, int KB>
-__global__ void __launch_bounds__(kBlockMT, 5) k_edge_interp(const WorkItem* __restrict__ items, int nitems,
+__global__ void __launch_bounds__(MTF<L>::BLOCK, 5) k_edge_interp(const WorkItem* __restrict__ items, int nitems,
                                                           const SceneDev* __restrict__ scenes) {
-    using G = MT<L>;
+    using G = MTF<L>;
     constexpr int QP = L::QP, K_ = KB;
     const int c = threadIdx.x % G::TPN, ns = threadIdx.x / G::TPN;
     NAGA_PIPE_BEGIN(float2, (tile_cap<G::NPB, KB>()), EdgeSrc{})
@@ -1334,11 +1366,12 @@ int apply_shape(int bps) {
     using TF = float2;  // filter records
     const size_t s4 = tile_bytes<L, K, float4>(), s2 = tile_bytes<L, K, TF>(), sb = tile_bytes<L, KB, float2>();
     int rc;
+    const int bo = other_bps<L>(bps);
     if ((rc = set_blocks_per_sm(k_pml_gather<L, K>, s4, bps)) || (rc = set_blocks_per_sm(k_rk<L, K, 1>, s4, bps)) ||
         (rc = set_blocks_per_sm(k_rk<L, K, 2>, s4, bps)) || (rc = set_blocks_per_sm(k_rk<L, K, 3>, s4, bps)) ||
-        (rc = set_blocks_per_sm(k_rk<L, K, 4>, s4, bps)) || (rc = set_blocks_per_sm(k_filter<L, K>, s2, bps)) ||
-        (rc = set_blocks_per_sm(k_edge_collide<L, KB>, sb, bps)) ||
-        (rc = set_blocks_per_sm(k_edge_interp<L, KB>, sb, bps)))
+        (rc = set_blocks_per_sm(k_rk<L, K, 4>, s4, bps)) || (rc = set_blocks_per_sm(k_filter<L, K>, s2, bo)) ||
+        (rc = set_blocks_per_sm(k_edge_collide<L, KB>, sb, bo)) ||
+        (rc = set_blocks_per_sm(k_edge_interp<L, KB>, sb, bo)))
         return rc;
     applied = bps;
     return NAGA_OK;
@@ -1361,12 +1394,17 @@ int enqueue_step_k(const StepLaunch& P, cudaStream_t st) {
     const int sms = sm_count();
     const int bps = tuned_bps(shape_key(L::D, K, KB, P.n_fluid));
     if ((rc = apply_shape<L, K, KB>(bps))) return rc;
-    auto pgrid = [&](auto kern, size_t smem, int n) {
-        int r = resident_blocks(kern, kBlockMT, smem, bps);
-        if (bps > 0 && bps < r) r = bps;
+    const int bo = other_bps<L>(bps);
+    // the RK stages and the PML gather at their block size and bps, the
+    // filter and boundary kernels at theirs and bo
+    auto pgrid_b = [&](auto kern, size_t smem, int n, int block, int b) {
+        int r = resident_blocks(kern, block, smem, b);
+        if (b > 0 && b < r) r = b;
         const int g = r * sms;
         return n < g ? n : g;
     };
+    constexpr int RB = MTR<L>::BLOCK, FB = MTF<L>::BLOCK;
+    auto pgrid = [&](auto kern, size_t smem, int n) { return pgrid_b(kern, smem, n, FB, bo); };
     const bool prof = prof_on();
 #define LAUNCH(id, n, ...)                      \
     if ((n) > 0) {                              \
@@ -1376,17 +1414,17 @@ int enqueue_step_k(const StepLaunch& P, cudaStream_t st) {
     }
     LAUNCH(K_MACRO, P.n_all, (k_macro_pml<L><<<grid(P.n_all), kBlock, 0, st>>>(P.all, P.n_all, P.scenes)));
     LAUNCH(K_TAIL, P.nscenes, (k_scene_tail<L::QP><<<dim3(P.nscenes, 2 * L::QP + 1), 256, 0, st>>>(P.scenes)));
-    LAUNCH(K_PML, P.n_pml, (k_pml_gather<L, K><<<pgrid(k_pml_gather<L, K>, s4, P.n_pml), kBlockMT, s4, st>>>(P.pml, P.n_pml, P.scenes)));
+    LAUNCH(K_PML, P.n_pml, (k_pml_gather<L, K><<<pgrid_b(k_pml_gather<L, K>, s4, P.n_pml, RB, bps), RB, s4, st>>>(P.pml, P.n_pml, P.scenes)));
     LAUNCH(K_EDGE_COLLIDE, P.n_edge,
-           (k_edge_collide<L, KB><<<pgrid(k_edge_collide<L, KB>, sb, P.n_edge), kBlockMT, sb, st>>>(P.edge, P.n_edge, P.scenes)));
+           (k_edge_collide<L, KB><<<pgrid(k_edge_collide<L, KB>, sb, P.n_edge), FB, sb, st>>>(P.edge, P.n_edge, P.scenes)));
     LAUNCH(K_FILTER, P.n_all_mt,
-           (k_filter<L, K><<<pgrid(k_filter<L, K>, s2, P.n_all_mt), kBlockMT, s2, st>>>(P.all_mt, P.n_all_mt, P.scenes)));
-    LAUNCH(K_RK1, P.n_fluid, (k_rk<L, K, 1><<<pgrid(k_rk<L, K, 1>, s4, P.n_fluid), kBlockMT, s4, st>>>(P.fluid, P.n_fluid, P.scenes)));
-    LAUNCH(K_RK2, P.n_fluid, (k_rk<L, K, 2><<<pgrid(k_rk<L, K, 2>, s4, P.n_fluid), kBlockMT, s4, st>>>(P.fluid, P.n_fluid, P.scenes)));
-    LAUNCH(K_RK3, P.n_fluid, (k_rk<L, K, 3><<<pgrid(k_rk<L, K, 3>, s4, P.n_fluid), kBlockMT, s4, st>>>(P.fluid, P.n_fluid, P.scenes)));
-    LAUNCH(K_RK4, P.n_fluid, (k_rk<L, K, 4><<<pgrid(k_rk<L, K, 4>, s4, P.n_fluid), kBlockMT, s4, st>>>(P.fluid, P.n_fluid, P.scenes)));
+           (k_filter<L, K><<<pgrid(k_filter<L, K>, s2, P.n_all_mt), FB, s2, st>>>(P.all_mt, P.n_all_mt, P.scenes)));
+    LAUNCH(K_RK1, P.n_fluid, (k_rk<L, K, 1><<<pgrid_b(k_rk<L, K, 1>, s4, P.n_fluid, RB, bps), RB, s4, st>>>(P.fluid, P.n_fluid, P.scenes)));
+    LAUNCH(K_RK2, P.n_fluid, (k_rk<L, K, 2><<<pgrid_b(k_rk<L, K, 2>, s4, P.n_fluid, RB, bps), RB, s4, st>>>(P.fluid, P.n_fluid, P.scenes)));
+    LAUNCH(K_RK3, P.n_fluid, (k_rk<L, K, 3><<<pgrid_b(k_rk<L, K, 3>, s4, P.n_fluid, RB, bps), RB, s4, st>>>(P.fluid, P.n_fluid, P.scenes)));
+    LAUNCH(K_RK4, P.n_fluid, (k_rk<L, K, 4><<<pgrid_b(k_rk<L, K, 4>, s4, P.n_fluid, RB, bps), RB, s4, st>>>(P.fluid, P.n_fluid, P.scenes)));
     LAUNCH(K_EDGE_INTERP, P.n_edge,
-           (k_edge_interp<L, KB><<<pgrid(k_edge_interp<L, KB>, sb, P.n_edge), kBlockMT, sb, st>>>(P.edge, P.n_edge, P.scenes)));
+           (k_edge_interp<L, KB><<<pgrid(k_edge_interp<L, KB>, sb, P.n_edge), FB, sb, st>>>(P.edge, P.n_edge, P.scenes)));
 #undef LAUNCH
     NAGA_CUDA_TRY(cudaGetLastError());
     return NAGA_OK;
@@ -1421,7 +1459,8 @@ int tune_k(const StepLaunch& P, cudaStream_t st) {
     }
     if ((rc = set_blocks_per_sm(k_rk<L, K, 1>, s4, 0))) return rc;
     int maxr = 0;
-    NAGA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxr, k_rk<L, K, 1>, kBlockMT, s4));
+    constexpr int RB = MTR<L>::BLOCK;
+    NAGA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxr, k_rk<L, K, 1>, RB, s4));
     maxr = std::max(maxr, 1);
     const int sms = sm_count();
     cudaEvent_t e0, e1;
@@ -1438,14 +1477,14 @@ int tune_k(const StepLaunch& P, cudaStream_t st) {
         // batch costs two launches per candidate)
         auto timed = [&](int reps, float* ms) -> bool {
             cudaEventRecord(e0, st);
-            for (int r = 0; r < reps; ++r) k_rk<L, K, 1><<<g, kBlockMT, s4, st>>>(P.fluid, P.n_fluid, P.scenes);
+            for (int r = 0; r < reps; ++r) k_rk<L, K, 1><<<g, RB, s4, st>>>(P.fluid, P.n_fluid, P.scenes);
             cudaEventRecord(e1, st);
             if (cudaEventSynchronize(e1) != cudaSuccess || cudaGetLastError() != cudaSuccess) return false;
             cudaEventElapsedTime(ms, e0, e1);
             *ms /= reps;
             return true;
         };
-        k_rk<L, K, 1><<<g, kBlockMT, s4, st>>>(P.fluid, P.n_fluid, P.scenes);
+        k_rk<L, K, 1><<<g, RB, s4, st>>>(P.fluid, P.n_fluid, P.scenes);
         float ms = 0.f;
         bool ok = timed(1, &ms);
         if (ok && ms < 0.4f) ok = timed(std::min(8, std::max(2, (int)(2.f / std::max(ms, 1e-3f)))), &ms);
