@@ -611,15 +611,34 @@ __global__ void __launch_bounds__(256) k_scene_tail(const SceneDev* __restrict__
     const SceneDev& S = scenes[blockIdx.x];
     const int t = blockIdx.y;
     if (t < 2 * QP) {
+        // the thread's partials in item order, loads issued eight at a time
+        // ahead of their adds (same order of additions)
         double acc = 0.0;
-        for (int it = threadIdx.x; it < S.n_all_items; it += blockDim.x) acc += S.partials[(int64_t)it * 2 * QP + t];
+        const double* col = S.partials + t;
+        const int bs = (int)blockDim.x;
+        int it = threadIdx.x;
+        for (; it + 7 * bs < S.n_all_items; it += 8 * bs) {
+            double v[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) v[u] = col[(int64_t)(it + u * bs) * 2 * QP];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) acc += v[u];
+        }
+        for (; it < S.n_all_items; it += bs) acc += col[(int64_t)it * 2 * QP];
         red[threadIdx.x] = acc;
         __syncthreads();
-        for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        for (int o = blockDim.x / 2; o >= 32; o >>= 1) {
             if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
             __syncthreads();
         }
-        if (threadIdx.x == 0) S.means[t] = S.nl > 0 ? (float)red[0] / (float)S.nl : 0.f;
+        // the last five levels of the same tree in warp 0 (lane l < o adds
+        // lane l + o, as the shared-memory levels do)
+        if (threadIdx.x < 32) {
+            double v = red[threadIdx.x];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(kFull, v, o);
+            if (threadIdx.x == 0) S.means[t] = S.nl > 0 ? (float)v / (float)S.nl : 0.f;
+        }
         return;
     }
     const unsigned long long step = *S.step;
