@@ -1,5 +1,5 @@
 // CPU oracle for the NAGA nonlocal LBM acoustics step.
-// TEST INFRASTRUCTURE ONLY: the checker for the CUDA product. See
+// TEST INFRASTRUCTURE ONLY: the reference the CUDA product is tested against. See
 // naga_oracle.h for what may call it. Build with -ffp-contract=off so that
 // FP32 distances match the reference formula bit for bit.
 //

@@ -1,7 +1,7 @@
 /*
  * CPU oracle for the NAGA nonlocal lattice-Boltzmann acoustics step.
  *
- * TEST INFRASTRUCTURE ONLY. This library is the checker: tests/, the smoke
+ * TEST INFRASTRUCTURE ONLY. The CUDA product is tested against it: tests/, the smoke
  * entry and bench.py's CPU-baseline leg may call it. The product
  * (naga_b200/, include/) never links, loads or executes anything here.
  *

@@ -1,6 +1,6 @@
 """ctypes binding of the CPU oracle (oracle/libnaga_oracle.so).
 
-TEST INFRASTRUCTURE ONLY: the checker. Only tests/, __graft_entry__.smoke()
+TEST INFRASTRUCTURE ONLY. Only tests/, __graft_entry__.smoke()
 and bench.py's CPU-baseline leg may import this module; the product never
 does. `build()` compiles the library from the sources beside this file.
 """
