@@ -407,16 +407,45 @@ __device__ __forceinline__ void quad_rhs(const double* xs, int k, int nsys, int 
         b0[d] = b1[d] = 0;
         cself[d] = tq.ksum[d] * rdel;
     }
+    // rows lane and lane + 32: support coordinates kept in registers (RBF
+    // rows), the table read through the read-only path; same arithmetic as
+    // gx_row
+    const int r0 = lane, r1 = lane + 32;
+    double x0[D], x1[D];
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        x0[d] = r0 < k ? xs[r0 * D + d] : 0.0;
+        x1[d] = r1 < k ? xs[r1 * D + d] : 0.0;
+    }
+    const double* tu = &tq.u[0][0];
+    const double* tk = &tq.K[0][0];
 #pragma unroll 4
     for (int q = 0; q < nq; ++q) {
         double xq[D];
 #pragma unroll
-        for (int d = 0; d < D; ++d) xq[d] = us * tq.u[q][d];
-        const double g0 = lane < nsys ? gx_row<D>(xs, k, shape, xq, lane) : 0.0;
-        const double g1 = lane + 32 < nsys ? gx_row<D>(xs, k, shape, xq, lane + 32) : 0.0;
+        for (int d = 0; d < D; ++d) xq[d] = us * __ldg(tu + 3 * q + d);
+        auto row = [&](int r, const double* xr) -> double {
+            if (r >= nsys) return 0.0;
+            if (r < k) {
+                double r2 = 0;
+#pragma unroll
+                for (int d = 0; d < D; ++d) {
+                    const double t = xr[d] - xq[d];
+                    r2 += t * t;
+                }
+                return shape_fn(r2, shape);
+            }
+            if (r == k) return 1.0;
+            double v = xq[0];
+#pragma unroll
+            for (int d = 1; d < D; ++d)
+                if (r - k - 1 == d) v = xq[d];
+            return v;
+        };
+        const double g0 = row(r0, x0), g1 = row(r1, x1);
 #pragma unroll
         for (int d = 0; d < D; ++d) {
-            const double aw = tq.K[q][d] * rdel;
+            const double aw = __ldg(tk + 3 * q + d) * rdel;
             b0[d] += aw * g0;
             b1[d] += aw * g1;
         }
