@@ -250,12 +250,16 @@ def batched_block(naga, torch, args, rank, world, dist, W, K):
     nodes = int(replicas.sum_over_ranks(sum(s.N for s in scenes), dist, "cuda"))
     p99 = replicas.max_over_ranks(float(np.percentile(b_per, 99)), dist, "cuda")
     bm = nodes * K / (b_ms * 1e-3) / 1e6
+    # per-kernel device time of this rank's batch step (event-bracketed
+    # launches, after the timed region)
+    prof = profile_kernels(naga, lambda: b.step(1))
     b.close()
     for s in scenes:
         s.close()
     return {"scenes": len(specs), "nodes": nodes, "mnups": bm, "plain_2d_mnups": plain_mnups,
             "ratio_vs_plain": bm / plain_mnups, "p50_step_ms": float(np.percentile(b_per, 50)),
-            "p99_step_ms": p99, "sharding": f"{world} rank(s), size-balanced"}
+            "p99_step_ms": p99, "sharding": f"{world} rank(s), size-balanced",
+            "kernel_ms_rank0": {n: round(t / 5, 4) for n, (l, t) in prof.items() if l}}
 
 
 def serving_block(naga, torch, args, rank, world, dist, step_priority=0):
