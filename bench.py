@@ -189,12 +189,25 @@ def headline_config(n_nodes, world):
             "parallelism": f"replicas x{world}"}
 
 
-def cpu_baseline(cfg, max_seconds=20.0, warmup=1):
-    """The oracle in NAGA's FP32 arithmetic on all host threads: set-up and
-    `warmup` steps are not timed; steps are timed until max_seconds (at
-    least one)."""
+def physical_cores() -> int:
+    """Physical cores of this host (distinct (core, socket) pairs of lscpu),
+    else the logical CPU count."""
+    try:
+        out = subprocess.run(["lscpu", "-p=CORE,SOCKET"], capture_output=True, text=True,
+                             timeout=10).stdout
+        pairs = {ln for ln in out.splitlines() if ln and not ln.startswith("#")}
+        if pairs:
+            return len(pairs)
+    except (OSError, subprocess.SubprocessError):
+        pass
+    return os.cpu_count() or 1
+
+
+def cpu_scene(cfg):
+    """The oracle in NAGA's FP32 arithmetic on the workload's scene. The grid
+    and the pulse come from the oracle's own generator (bit-identical to the
+    library's, tests/test_oracle.py), so this leg never loads libnaga_b200."""
     from oracle import oracle
-    import naga_b200 as naga
 
     arch = os.environ.get("NAGA_ORACLE_ARCH", "-march=native")
     path = os.path.join(ROOT, "oracle", "_native", "libnaga_oracle.so")
@@ -205,11 +218,21 @@ def cpu_baseline(cfg, max_seconds=20.0, warmup=1):
     except Exception:
         L, arch = oracle.lib(), ""
     oracle._lib = L
-    g = naga.generate_grid(cfg["dim"], cfg["n_side"], cfg["layers"], cfg["seed"])
+    g = oracle.generate_grid(cfg["dim"], cfg["n_side"], cfg["layers"], cfg["seed"])
     S = oracle.Scene(cfg["dim"], g["points"], g["n_bulk"], g["n_layer"], g["n_boundary"],
                      g["normals"], g["sigma"], g["h"], k=cfg["k"], shape=cfg["shape"], precision=1,
                      probes=np.array(cfg["probes"], np.float32))
-    S.set_density(naga.gaussian_pulse(g["points"], [0.5] * cfg["dim"], 1e-3, cfg["width"]))
+    S.set_density(oracle.gaussian_pulse(g["points"], [0.5] * cfg["dim"], 1e-3, cfg["width"]))
+    return oracle, S, g["points"].shape[0], arch
+
+
+def cpu_baseline(cfg, steps=None, warmup=1, max_seconds=15.0, one_thread_steps=2):
+    """The CPU leg: the oracle in NAGA's FP32 arithmetic, set-up untimed.
+    With `steps`, exactly that many steps are timed after `warmup` untimed
+    ones on all host threads; otherwise steps are timed until max_seconds.
+    Then `one_thread_steps` steps on one thread (0 skips them)."""
+    oracle, S, N, arch = cpu_scene(cfg)
+    threads = oracle.set_threads(os.cpu_count() or 1)
     for _ in range(warmup):
         S.step(1)
     n, t0 = 0, time.perf_counter()
@@ -217,13 +240,45 @@ def cpu_baseline(cfg, max_seconds=20.0, warmup=1):
         S.step(1)
         n += 1
         el = time.perf_counter() - t0
-        if el > max_seconds or n >= 50:
+        if (steps is not None and n >= steps) or (steps is None and (el > max_seconds or n >= 50)):
             break
-    N = g["points"].shape[0]
-    return {"value": N * n / el / 1e6, "unit": "MNUPS", "cores": os.cpu_count(), "kind": "port",
-            "ms_per_step": el / n * 1e3, "nodes": N,
-            "sample": f"{n} time steps of the {N:,}-node scene after {warmup} untimed (set-up excluded), "
-                      f"FP32 as NAGA, OpenMP, {arch or 'generic x86-64'}"}
+    out = {"value": N * n / el / 1e6, "unit": "MNUPS", "cores": threads, "kind": "port",
+           "physical_cores": physical_cores(), "ms_per_step": el / n * 1e3, "nodes": N,
+           "sample": f"{n} time steps of the {N:,}-node scene after {warmup} untimed (set-up "
+                     f"excluded), FP32 as NAGA, OpenMP on {threads} threads, {arch or 'generic x86-64'}"}
+    if one_thread_steps:
+        oracle.set_threads(1)
+        t0 = time.perf_counter()
+        S.step(one_thread_steps)
+        el1 = time.perf_counter() - t0
+        oracle.set_threads(threads)
+        out["one_thread"] = {"value": N * one_thread_steps / el1 / 1e6, "unit": "MNUPS",
+                             "ms_per_step": el1 / one_thread_steps * 1e3,
+                             "sample": f"{one_thread_steps} further steps of the same scene on 1 thread"}
+    return out
+
+
+def probe_error_block(scene, g, drho):
+    """Probe error of the benchmarked scene: the scene restarts from its
+    initial pulse, takes the fixture's steps (1000) and its probe trace is
+    compared with the FP64 oracle's trace of the same scene
+    (tests/golden/trace_d3q27_63.npz; the input digest must match):
+    max_t |p_gpu - p_oracle| / max_t |p_oracle| over all probes."""
+    path = os.path.join(ROOT, "tests", "golden", "trace_d3q27_63.npz")
+    if not os.path.exists(path):
+        return {"value": None, "reason": "fixture missing"}
+    from tests.golden.make_config2_trace import scene_hash
+
+    fx = np.load(path)
+    if scene_hash(g, drho) != str(fx["sha256"]):
+        return {"value": None, "reason": "scene differs from the fixture's"}
+    ref = fx["probes"]
+    scene.set_density(drho)
+    scene.step(len(ref))
+    got = scene.probes(0, len(ref)).astype(np.float64)
+    err = float(np.abs(got - ref).max() / np.abs(ref).max())
+    return {"value": err, "steps": int(len(ref)), "bar": 1e-5, "ok": err <= 1e-5,
+            "against": "FP64 CPU oracle trace of the same scene (tests/golden/trace_d3q27_63.npz)"}
 
 
 # ------------------------------------------------------------ extra blocks
@@ -262,19 +317,20 @@ def batched_block(naga, torch, args, rank, world, dist, W, K):
             "kernel_ms_rank0": {n: round(t / 5, 4) for n, (l, t) in prof.items() if l}}
 
 
-def serving_block(naga, torch, args, rank, world, dist, step_priority=0):
+def serving_block(naga, torch, args, rank, world, dist, step_priority=0, target_step_ms=0.0, seconds=None):
     """The continuous-batching loop on the 3-D serving workload, for a
     bounded window: requests arrive as a Poisson process (20/s, seeded) with
     point counts log-uniform in [1e4, 1e6] (jittered unit cubes seeded per
     request), 2000 steps each, FP64 weight solves, admitted under a 150 GB
-    device budget; each rank serves the requests the deterministic router
-    gives it. Requests still running at the end of the window count by the
-    steps they took. step_priority 1 runs the batch's steps ahead of the
-    admissions' set-up (lower step latency, fewer admissions)."""
+    device budget and, with target_step_ms > 0, a per-step latency target of
+    the batch; each rank serves the requests the deterministic router gives
+    it. Requests still running at the end of the window count by the steps
+    they took. step_priority 1 runs the batch's steps ahead of the set-up
+    kernels of admissions."""
     from naga_b200 import replicas
 
     rng = np.random.default_rng(2024)
-    T = args.serving_seconds
+    T = args.serving_seconds if seconds is None else seconds
     arrivals, t = [], 0.0
     while True:
         t += float(rng.exponential(1 / 20.0))
@@ -285,7 +341,8 @@ def serving_block(naga, torch, args, rank, world, dist, step_priority=0):
     router = replicas.Router(world)
     owner = [router.place(n_side ** 3, 2000) for (_, n_side, _) in arrivals]
     mine = [a for a, o in zip(arrivals, owner) if o == rank]
-    server = naga.Server(3, memory_budget=150 * 10 ** 9, steps_per_tick=20, step_priority=step_priority)
+    server = naga.Server(3, memory_budget=150 * 10 ** 9, steps_per_tick=20, step_priority=step_priority,
+                         target_step_ms=target_step_ms)
     probes = np.array(PROBES3, np.float32)
     # the clients: a producer thread builds each request's point cloud and
     # pulse in arrival order (the generator releases the GIL), the loop
@@ -330,12 +387,18 @@ def serving_block(naga, torch, args, rank, world, dist, step_priority=0):
     server.close()
     node_updates = replicas.sum_over_ranks(st["node_updates"], dist, "cuda")
     busy = replicas.max_over_ranks(st["busy_ms"], dist, "cuda")
-    return {"window_s": T, "arrivals": len(arrivals), "submitted_rank0": submitted,
+    done = int(replicas.sum_over_ranks(st["done"], dist, "cuda"))
+    return {"window_s": T, "target_step_ms": target_step_ms, "step_priority": step_priority,
+            "arrivals": len(arrivals), "submitted_rank0": submitted,
             "node_updates": int(node_updates), "mnups_busy": node_updates / max(busy, 1e-9) / 1e3,
             "mnups_wall": node_updates / T / 1e6,
             "p50_step_ms": replicas.max_over_ranks(st["p50_step_ms"], dist, "cuda"),
             "p99_step_ms": replicas.max_over_ranks(st["p99_step_ms"], dist, "cuda"),
-            "ticks_rank0": st["ticks"], "done": st["done"], "active_at_end": st["active"],
+            "step_latency": "per-step CUDA events on the batch stream",
+            "done": done, "p50_request_ms": replicas.max_over_ranks(st["p50_request_ms"], dist, "cuda"),
+            "p99_request_ms": replicas.max_over_ranks(st["p99_request_ms"], dist, "cuda"),
+            "p50_queue_ms_rank0": st["p50_queue_ms"], "admitted_rank0": st["admitted"],
+            "ticks_rank0": st["ticks"], "active_at_end": st["active"],
             "queued_at_end": st["queued"], "failed": st["failed"], "peak_bytes_rank0": st["peak_bytes"],
             "host_ms_rank0": {k: round(st[k + "_ms"], 1) for k in ("prepare", "admit", "wait", "retire")}}
 
@@ -405,7 +468,7 @@ def run_reference(args, rank, world):
     cfg = CONFIG3
     if rank != 0:
         return 0
-    cb = cpu_baseline(cfg, max_seconds=max(5.0, 4.0 * args.steps / 100.0), warmup=min(args.warmup, 3))
+    cb = cpu_baseline(cfg, steps=args.steps, warmup=args.warmup)
     v = cb["value"]
     line = {"metric": "MNUPS (node updates/s) of the nonlocal LBM acoustics step", "value": v,
             "unit": "MNUPS", "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
@@ -472,6 +535,10 @@ def run_naga(args, rank, world, local_rank):
     e2e_s = replicas.max_over_ranks(e2e_s, dist, "cuda")
     e2e = world * N * K / e2e_s / 1e6
 
+    # ---- the probe error the throughput is quoted at (1000 steps against
+    # the FP64 oracle; after the timed regions)
+    probe_error = probe_error_block(scene, g, drho) if args.n_side == 63 else None
+
     # ---- batched form (every rank steps its size-balanced share of the
     # scenes; time = slowest rank) vs the plain single 2-D scene
     batched = None
@@ -481,7 +548,9 @@ def run_naga(args, rank, world, local_rank):
     serving = serving_latency = None
     if not args.no_serving:
         serving = serving_block(naga, torch, args, rank, world, dist)
-        serving_latency = serving_block(naga, torch, args, rank, world, dist, step_priority=1)
+        serving_latency = serving_block(naga, torch, args, rank, world, dist, step_priority=1,
+                                        target_step_ms=args.target_step_ms,
+                                        seconds=args.serving_target_seconds)
     setup = None
     if not args.no_setup and rank == 0:
         setup = setup_block(naga, torch, args)
@@ -523,11 +592,11 @@ def run_naga(args, rank, world, local_rank):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": headline_config(N, world),
         "p50_step_ms": float(np.percentile(per, 50)), "p99_step_ms": float(np.percentile(per, 99)),
-        "roofline": roof, "cpu_baseline": cb,
+        "probe_error": probe_error, "roofline": roof, "cpu_baseline": cb,
         "e2e": {"value": e2e, "unit": "MNUPS", "h2d_bytes_per_step": int(N * 4 / K),
                 "d2h_bytes_per_step": 4 * len(cfg["probes"]), "probe_trace_read_back": e2e_trace_ok},
         "gpu_launches": int(gpu_launches), "clocks": clk.summary(), "batched": batched,
-        "serving": serving, "serving_steps_first": serving_latency, "setup": setup,
+        "serving": serving, "serving_latency_target": serving_latency, "setup": setup,
         "launch_shapes": naga.tuning_report().strip().splitlines(),
     }
     print(json.dumps(line), flush=True)
@@ -546,7 +615,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batched-scenes", type=int, default=256)
     ap.add_argument("--no-serving", action="store_true")
-    ap.add_argument("--serving-seconds", type=float, default=12.0)
+    ap.add_argument("--serving-seconds", type=float, default=10.0)
+    ap.add_argument("--serving-target-seconds", type=float, default=20.0)
+    ap.add_argument("--target-step-ms", type=float, default=4.0,
+                    help="per-step latency target of the second serving run")
     ap.add_argument("--no-setup", action="store_true")
     ap.add_argument("--setup-systems", type=int, default=1_000_000)
     ap.add_argument("--n-side", type=int, default=63,

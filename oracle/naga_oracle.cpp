@@ -191,51 +191,66 @@ static void knn_grid(const float* src, int64_t n, const float* q, int64_t nq, in
 // change the result only where candidates tie at the k-th distance. The
 // cell index is clamped to the grid (the reference's floor can reach `shape`
 // through rounding).
-static void knn_ring_reference(const float* src, int64_t n, const float* q, int64_t nq, int dim,
-                               int k, int approx, uint32_t* idx, float* d2) {
-    float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
-    for (int d = 0; d < dim; ++d) {
-        lo[d] = INFINITY;
-        hi[d] = -INFINITY;
-    }
-    for (int64_t j = 0; j < n; ++j)
-        for (int d = 0; d < dim; ++d) {
-            lo[d] = std::min(lo[d], src[j * dim + d]);
-            hi[d] = std::max(hi[d], src[j * dim + d]);
-        }
-    const float tol = 1e-3f;
-    float vol = 1.0f;
-    for (int d = 0; d < dim; ++d) {
-        if (hi[d] - lo[d] < tol) hi[d] = lo[d] + tol;
-        vol *= hi[d] - lo[d];
-    }
-    const float w = std::pow((float)approx / (float)n * vol, 1.0f / (float)dim);
+struct CubicSeg {
+    int dim = 0;
+    float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0}, w = 0;
     int64_t shape[3] = {1, 1, 1};
-    for (int d = 0; d < dim; ++d) {
-        shape[d] = (int64_t)std::ceil((hi[d] - lo[d]) / w);
-        hi[d] = lo[d] + (float)shape[d] * w;
-    }
-    auto cell_of = [&](const float* p, int64_t* c) {
+    std::vector<int64_t> start;  // [cells + 1], exclusive prefix sums of the sizes
+    std::vector<uint32_t> order; // point indices grouped by cell, ascending within a cell
+    void cell_of(const float* p, int64_t* c) const {
         for (int d = 0; d < dim; ++d) {
             if (p[d] < lo[d]) c[d] = 0;
             else if (p[d] >= hi[d]) c[d] = shape[d] - 1;
             else c[d] = std::min<int64_t>((int64_t)std::floor((p[d] - lo[d]) / w), shape[d] - 1);
         }
-    };
-    const int64_t ncell = shape[0] * shape[1] * shape[2];
-    std::vector<int64_t> start(ncell + 1, 0), cell(n);
+    }
+};
+
+static void cubic_segmentation(const float* src, int64_t n, int dim, int approx, CubicSeg& S) {
+    S.dim = dim;
+    for (int d = 0; d < dim; ++d) {
+        S.lo[d] = INFINITY;
+        S.hi[d] = -INFINITY;
+    }
+    for (int64_t j = 0; j < n; ++j)
+        for (int d = 0; d < dim; ++d) {
+            S.lo[d] = std::min(S.lo[d], src[j * dim + d]);
+            S.hi[d] = std::max(S.hi[d], src[j * dim + d]);
+        }
+    const float tol = 1e-3f;
+    float vol = 1.0f;
+    for (int d = 0; d < dim; ++d) {
+        if (S.hi[d] - S.lo[d] < tol) S.hi[d] = S.lo[d] + tol;
+        vol *= S.hi[d] - S.lo[d];
+    }
+    S.w = std::pow((float)approx / (float)n * vol, 1.0f / (float)dim);
+    for (int d = 0; d < dim; ++d) {
+        S.shape[d] = (int64_t)std::ceil((S.hi[d] - S.lo[d]) / S.w);
+        S.hi[d] = S.lo[d] + (float)S.shape[d] * S.w;
+    }
+    const int64_t ncell = S.shape[0] * S.shape[1] * S.shape[2];
+    S.start.assign(ncell + 1, 0);
+    std::vector<int64_t> cell(n);
     for (int64_t j = 0; j < n; ++j) {
         int64_t c[3] = {0, 0, 0};
-        cell_of(src + j * dim, c);
-        cell[j] = c[0] + shape[0] * (c[1] + shape[1] * c[2]);
-        start[cell[j] + 1]++;
+        S.cell_of(src + j * dim, c);
+        cell[j] = c[0] + S.shape[0] * (c[1] + S.shape[1] * c[2]);
+        S.start[cell[j] + 1]++;
     }
-    for (int64_t c = 0; c < ncell; ++c) start[c + 1] += start[c];
-    std::vector<uint32_t> order(n);
-    {
-        std::vector<int64_t> fill(start.begin(), start.end() - 1);
-        for (int64_t j = 0; j < n; ++j) order[fill[cell[j]]++] = (uint32_t)j;
-    }
+    for (int64_t c = 0; c < ncell; ++c) S.start[c + 1] += S.start[c];
+    S.order.assign(n, 0);
+    std::vector<int64_t> fill(S.start.begin(), S.start.end() - 1);
+    for (int64_t j = 0; j < n; ++j) S.order[fill[cell[j]]++] = (uint32_t)j;
+}
+
+static void knn_ring_reference(const float* src, int64_t n, const float* q, int64_t nq, int dim,
+                               int k, int approx, uint32_t* idx, float* d2) {
+    CubicSeg S;
+    cubic_segmentation(src, n, dim, approx, S);
+    const int64_t* shape = S.shape;
+    const std::vector<int64_t>& start = S.start;
+    const std::vector<uint32_t>& order = S.order;
+    auto cell_of = [&](const float* p, int64_t* c) { S.cell_of(p, c); };
     int64_t max_r = 0;
     for (int d = 0; d < dim; ++d) max_r = std::max<int64_t>(max_r, (shape[d] + 1) / 2);
 #pragma omp parallel
@@ -414,6 +429,28 @@ extern "C" int orc_knn(const float* src, int64_t n, const float* qry, int64_t nq
         knn_grid(src, n, qry, nq, dim, k, idx, d2);
     else
         knn_brute(src, n, qry, nq, dim, k, idx, d2);
+    return 0;
+}
+
+extern "C" int orc_cubic_segmentation(const float* src, int64_t n, int dim, int approx, float* lower,
+                                      float* upper, float* width, int64_t* shape, int64_t* n_cells,
+                                      uint32_t* sizes, uint32_t* offsets, uint32_t* indices) {
+    if (n < 1 || (dim != 2 && dim != 3) || approx < 1) return 1;
+    orc::CubicSeg S;
+    orc::cubic_segmentation(src, n, dim, approx, S);
+    const int64_t cells = S.shape[0] * S.shape[1] * S.shape[2];
+    for (int d = 0; d < dim; ++d) {
+        if (lower) lower[d] = S.lo[d];
+        if (upper) upper[d] = S.hi[d];
+        if (shape) shape[d] = S.shape[d];
+    }
+    if (width) *width = S.w;
+    if (n_cells) *n_cells = cells;
+    for (int64_t c = 0; c < cells; ++c) {
+        if (sizes) sizes[c] = (uint32_t)(S.start[c + 1] - S.start[c]);
+        if (offsets) offsets[c] = (uint32_t)S.start[c];
+    }
+    if (indices) std::copy(S.order.begin(), S.order.end(), indices);
     return 0;
 }
 
@@ -1218,6 +1255,15 @@ extern "C" int orc_scene_create(const orc_scene_desc* d, orc_scene** out) {
     return 0;
 }
 extern "C" void orc_scene_destroy(orc_scene* s) { delete s; }
+extern "C" int orc_set_threads(int n) {
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+    return omp_get_max_threads();
+#else
+    (void)n;
+    return 1;
+#endif
+}
 extern "C" int orc_scene_set_sources(orc_scene* s, const int64_t* nodes, int64_t n, const float* values,
                                      int64_t n_steps) {
     return s->impl->set_sources(nodes, n, values, n_steps);

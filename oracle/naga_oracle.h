@@ -36,6 +36,16 @@ int orc_knn_ring_reference(const float* src, int64_t n, const float* qry,
                            int64_t nq, int dim, int k, int approx,
                            uint32_t* idx, float* d2);
 
+/* ---- NAGA's cubic segmentation (nd_cubic_segmentation.cuh:227-303,
+ * get_partition_index :376-392) in its FP32 arithmetic: bounds, width,
+ * shape; per partition (linear index x + shape0 (y + shape1 z)) its size,
+ * the exclusive prefix sums and the point indices grouped by partition,
+ * ascending within one. Call with NULL arrays to learn n_cells first.   */
+int orc_cubic_segmentation(const float* src, int64_t n, int dim, int approx,
+                           float* lower, float* upper, float* width,
+                           int64_t* shape, int64_t* n_cells, uint32_t* sizes,
+                           uint32_t* offsets, uint32_t* indices);
+
 /* ---- batched LU inverse (getrf + getri semantics), FP64 -------------- */
 /* A, Ainv: [batch][n][n] column-major per matrix; info[batch] (0 = ok,
  * j>0 = U(j,j) exactly zero, LAPACK convention).                          */
@@ -105,6 +115,23 @@ int orc_scene_tables(const orc_scene* s, uint32_t* idx, double* W,
  * phase 2: after RK4 and the final boundary interpolation.               */
 int orc_scene_step_phase(orc_scene* s, int phase);
 int orc_scene_pml_state(const orc_scene* s, double* q1, double* q2);
+
+/* OpenMP threads of the calling thread's later parallel regions (n <= 0
+ * leaves it); returns the number now in effect (1 without OpenMP).      */
+int orc_set_threads(int n);
+
+/* ---- synthetic scene inputs (scene_inputs.cpp) ---------------------- */
+/* Jittered n_side^dim grid of the unit square / cube with NAGA's node
+ * classes; counts[3] = {bulk, layer, boundary}; outputs may be NULL (call
+ * once with NULL outputs for the counts). points [N][dim], normals
+ * [n_boundary][dim] (inward), sigma [n_layer], h = 1 / (n_side - 1).      */
+int orc_grid_generate(int dim, int64_t n_side, int n_layers, double jitter,
+                      double sigma_peak, uint64_t seed, int64_t* counts,
+                      float* points, float* normals, float* sigma, double* h);
+/* drho_i = amplitude exp(-|x_i - center|^2 / (2 width^2)) (FP64, stored FP32) */
+int orc_gaussian_pulse(const float* points, int64_t n, int dim,
+                       const double* center, double amplitude, double width,
+                       float* drho);
 
 /* ---- lattice tables (for tests of the product's tables) -------------- */
 int orc_lattice(int dim, int* Q, double* c /*[Q][dim]*/, double* w /*[Q]*/,

@@ -66,6 +66,10 @@ def lib(path: str | None = None):
     L.orc_scene_set_sources.argtypes = [vp, vp, i64, vp, i64]
     L.orc_lattice.argtypes = [i32, vp, vp, vp, vp, vp]
     L.orc_collision.argtypes = [i32, vp, dbl, vp, dbl, dbl, vp]
+    L.orc_grid_generate.argtypes = [i32, i64, i32, dbl, dbl, C.c_uint64, vp, vp, vp, vp, vp]
+    L.orc_gaussian_pulse.argtypes = [vp, i64, i32, vp, dbl, dbl, vp]
+    L.orc_set_threads.argtypes = [i32]
+    L.orc_cubic_segmentation.argtypes = [vp, i64, i32, i32] + [vp] * 8
     if path is None:
         _lib = L
     return L
@@ -73,6 +77,38 @@ def lib(path: str | None = None):
 
 def _p(a):
     return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+def set_threads(n: int) -> int:
+    """OpenMP threads for the oracle's later calls from this thread (n <= 0
+    keeps the current number); returns the number in effect."""
+    return lib().orc_set_threads(n)
+
+
+def generate_grid(dim, n_side, n_layers, seed, jitter=0.25, sigma_peak=0.1):
+    """The jittered benchmark grid (orc_grid_generate), as a dict with the
+    keys of the scene constructors: points, normals, sigma, class counts, h."""
+    counts = np.zeros(3, np.int64)
+    h = C.c_double()
+    assert lib().orc_grid_generate(dim, n_side, n_layers, jitter, sigma_peak, seed, _p(counts), None,
+                                   None, None, C.byref(h)) == 0
+    nb, nl, nw = (int(c) for c in counts)
+    pts = np.zeros((nb + nl + nw, dim), np.float32)
+    nrm = np.zeros((nw, dim), np.float32)
+    sig = np.zeros(nl, np.float32)
+    assert lib().orc_grid_generate(dim, n_side, n_layers, jitter, sigma_peak, seed, None, _p(pts),
+                                   _p(nrm), _p(sig), None) == 0
+    return dict(dim=dim, points=pts, n_bulk=nb, n_layer=nl, n_boundary=nw, normals=nrm, sigma=sig,
+                h=h.value)
+
+
+def gaussian_pulse(points, center, amplitude, width):
+    pts = np.ascontiguousarray(points, np.float32)
+    c = np.ascontiguousarray(center, np.float64)
+    out = np.zeros(pts.shape[0], np.float32)
+    assert lib().orc_gaussian_pulse(_p(pts), pts.shape[0], pts.shape[1], _p(c), amplitude, width,
+                                    _p(out)) == 0
+    return out
 
 
 def knn(src, qry, k, grid=True):
@@ -84,6 +120,24 @@ def knn(src, qry, k, grid=True):
     rc = lib().orc_knn(_p(src), src.shape[0], _p(qry), qry.shape[0], dim, k, int(grid), _p(idx), _p(d2))
     assert rc == 0, rc
     return idx, d2
+
+
+def cubic_segmentation(src, approx):
+    """NAGA's nd_cubic_segmentation restated: dict of lower, upper, width,
+    shape, sizes, offsets, indices (ascending within a partition)."""
+    src = np.ascontiguousarray(src, np.float32)
+    n, dim = src.shape
+    lo, hi, shape = np.zeros(3, np.float32), np.zeros(3, np.float32), np.zeros(3, np.int64)
+    w, cells = C.c_float(), C.c_int64()
+    assert lib().orc_cubic_segmentation(_p(src), n, dim, approx, _p(lo), _p(hi), C.byref(w), _p(shape),
+                                        C.byref(cells), None, None, None) == 0
+    sizes = np.zeros(cells.value, np.uint32)
+    offsets = np.zeros(cells.value, np.uint32)
+    indices = np.zeros(n, np.uint32)
+    assert lib().orc_cubic_segmentation(_p(src), n, dim, approx, None, None, None, None, None, _p(sizes),
+                                        _p(offsets), _p(indices)) == 0
+    return dict(lower=lo[:dim], upper=hi[:dim], width=w.value, shape=shape[:dim], sizes=sizes,
+                offsets=offsets, indices=indices)
 
 
 def knn_ring_reference(src, qry, k, approx=None):

@@ -1,7 +1,7 @@
 """Generates the golden fixtures in tests/golden/ from NAGA's known-answer
-programs. Run where the reference tree is mounted:
+programs. Run where the reference tree is available, giving its path:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <path-to-NAGA-checkout>
 
 Fixtures written:
   inverse_3x3.json     the 3x3 matrix and its hard-coded inverse from
@@ -97,4 +97,6 @@ def main(ref: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <path-to-NAGA-checkout>")
+    main(sys.argv[1])

@@ -87,6 +87,30 @@ def test_config1_probe_trace_500_steps(naga, oracle):
     assert rel_err(gpu.probes(0, 500), po) <= 1e-5
 
 
+@pytest.mark.slow
+def test_config2_probe_trace_1000_steps(naga, golden_dir):
+    """The benchmarked 3-D scene at full size: D3Q27, 250,047 jittered nodes
+    (63^3, h = 1/62, seed 1), k = 32, multiquadric RBF, FP64 weight solves,
+    8-layer PML, Gaussian pulse (1e-3, width 0.05), dt = 0.5 h / c, 8 probes,
+    1000 steps. Probe error <= 1e-5 against the FP64 oracle's trace of the
+    same scene (tests/golden/trace_d3q27_63.npz, made by
+    tests/golden/make_config2_trace.py; the input digest proves the scene is
+    the same)."""
+    import os
+
+    from tests.golden.make_config2_trace import PROBES3 as P3, scene_hash
+
+    fx = np.load(os.path.join(golden_dir, "trace_d3q27_63.npz"))
+    g = naga.generate_grid(3, 63, 8, 1)
+    drho = naga.gaussian_pulse(g["points"], [0.5, 0.5, 0.5], 1e-3, 0.05)
+    assert scene_hash(g, drho) == str(fx["sha256"])
+    po = fx["probes"]
+    gpu = naga.Scene(g, k=32, shape=0, probes=P3, probe_capacity=len(po))
+    gpu.set_density(drho)
+    gpu.step(len(po))
+    assert rel_err(gpu.probes(0, len(po)), po) <= 1e-5
+
+
 @pytest.mark.parametrize("priority", [0, 1])
 def test_batch_equals_individual_scenes(naga, oracle, priority):
     gs = [naga.generate_grid(2, n, 3, s) for n, s in ((25, 1), (33, 2), (41, 3))]

@@ -227,3 +227,52 @@ def test_oracle_density_sources(naga, oracle):
     c.step(5)
     assert np.array_equal(a.state()[0], b.state()[0])
     assert c.state()[1][centre] > a.state()[1][centre]
+
+
+@pytest.mark.parametrize("dim,n_side,layers,seed", [(2, 142, 10, 0), (3, 63, 8, 1), (2, 40, 4, 0),
+                                                    (3, 14, 3, 0), (3, 25, 2, 7)])
+def test_oracle_grid_equals_library_grid(naga, oracle, dim, n_side, layers, seed):
+    """The oracle's own restatement of the jittered benchmark grids (which the
+    CPU baseline and the fixture scripts use, so they never load the
+    product library) equals the library's naga_grid_generate and
+    naga_gaussian_pulse bit for bit."""
+    a = oracle.generate_grid(dim, n_side, layers, seed)
+    b = naga.generate_grid(dim, n_side, layers, seed)
+    for key in ("n_bulk", "n_layer", "n_boundary", "h"):
+        assert a[key] == b[key], key
+    for key in ("points", "normals", "sigma"):
+        assert a[key].tobytes() == b[key].tobytes(), key
+    pa = oracle.gaussian_pulse(a["points"], [0.5] * dim, 1e-3, 0.05)
+    pb = naga.gaussian_pulse(b["points"], [0.5] * dim, 1e-3, 0.05)
+    assert pa.tobytes() == pb.tobytes()
+
+
+def _max_abs_g(oracle, dim, n_side, shape, checkpoints, width):
+    g = oracle.generate_grid(dim, n_side, max(2, n_side // 8), 1)
+    k = 32 if dim == 3 else 16
+    S = oracle.Scene(dim, g["points"], g["n_bulk"], g["n_layer"], g["n_boundary"], g["normals"],
+                     g["sigma"], g["h"], k=k, shape=shape)
+    S.set_density(oracle.gaussian_pulse(g["points"], [0.5] * dim, 1e-3, width))
+    out, done = [], 0
+    for c in checkpoints:
+        S.step(c - done)
+        done = c
+        out.append(float(np.abs(S.state()[0]).max()))
+    return out
+
+
+def test_cubic_rbf_is_unstable_in_3d_multiquadric_is_not(oracle):
+    """Why the 3-D workloads run NAGA's multiquadric RBF instead of the cubic
+    r^3 the benchmark configurations name: with r^3 stencils the FP64 oracle
+    of the D3Q27 step (NAGA's algorithm restated) grows without bound, while
+    the same scene with the multiquadric decays as the PML absorbs the pulse.
+    Measured on a 16^3 cube: max |g| of r^3 rises ~8x per 20 steps from
+    step ~50 (1.3e-5 at step 30, 3.4e-2 at step 110, NaN by step 170); the
+    multiquadric falls from 1.6e-5 to 1.5e-7 over the same steps. In 2-D the
+    cubic r^3 D2Q9 step stays bounded (the 2-D workloads run r^3)."""
+    r3 = _max_abs_g(oracle, 3, 16, 1, (30, 110), 0.1)
+    mq = _max_abs_g(oracle, 3, 16, 0, (30, 110), 0.1)
+    assert r3[1] > 100 * r3[0], r3
+    assert mq[1] < mq[0], mq
+    r3_2d = _max_abs_g(oracle, 2, 40, 1, (30, 300), 0.08)
+    assert np.isfinite(r3_2d).all() and r3_2d[1] < r3_2d[0], r3_2d
