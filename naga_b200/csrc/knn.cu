@@ -23,6 +23,7 @@
 #include <cstring>
 
 #include <cub/device/device_scan.cuh>
+#include <cuda.h>
 
 #include <cmath>
 #include <mutex>
@@ -467,21 +468,54 @@ struct NoAllocScratch {
 
 static __device__ __align__(256) unsigned char g_knn_scratch[sizeof(NoAllocScratch)];
 
-// device address of g_knn_scratch for the current device, looked up once
+// Unique id of the calling thread's current context (cuCtxGetId through the
+// runtime's driver entry points, so the library needs no libcuda link);
+// false when it cannot be had (no current context, an older driver).
+bool current_context_id(unsigned long long* id) {
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", (void**)&get_current, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            get_current = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", (void**)&get_id, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            get_id = nullptr;
+    });
+    CUcontext ctx = nullptr;
+    if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx) return false;
+    return get_id(ctx, id) == CUDA_SUCCESS;
+}
+
+// device address of g_knn_scratch in the current context: looked up once
+// per device and context, and again when the device's context changed (a
+// cudaDeviceReset or a host framework resetting the primary context loads
+// the module anew, and the array may move); without a context id the
+// lookup is made on every call
 int noalloc_scratch(NoAllocScratch** out) {
     static std::mutex mu;
     static void* addr[64] = {nullptr};
+    static unsigned long long ctx_of[64] = {0};
     int dev = 0;
     NAGA_CUDA_TRY(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64) return set_error(NAGA_EINVAL, "naga_knn_noalloc: device ordinal above 63");
+    unsigned long long ctx = 0;
+    const bool known = current_context_id(&ctx);
     std::lock_guard<std::mutex> lk(mu);
-    if (!addr[dev]) {
+    if (!known || !addr[dev] || ctx_of[dev] != ctx) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_knn_scratch);
         if (e != cudaSuccess)
             return set_error(NAGA_ECUDA, std::string("naga_knn_noalloc: cudaGetSymbolAddress: ") +
                                              cudaGetErrorString(e));
-        addr[dev] = p;
+        addr[dev] = known ? p : nullptr;
+        ctx_of[dev] = ctx;
+        *out = reinterpret_cast<NoAllocScratch*>(p);
+        return NAGA_OK;
     }
     *out = reinterpret_cast<NoAllocScratch*>(addr[dev]);
     return NAGA_OK;

@@ -75,3 +75,36 @@ def test_knn_noalloc_rejects_nonfinite_coordinates(naga):
     assert rc == naga.NAGA_OK
     ri, rd = _reference(naga, src, qry, 8)
     assert np.array_equal(idx, ri) and np.array_equal(d2, rd)
+
+
+def test_knn_noalloc_edge_cases_match_knn(naga):
+    """The cases that take the allocation-free search's own paths, each
+    compared with naga_knn bit for bit: a 3-D cloud on a plane (its flat
+    bounding box makes the first cell grid far larger than the fixed
+    scratch, so the cells are coarsened), k = 64 (two list registers per
+    lane), exactly 65,536 source points (the scratch's limit) and an empty
+    cloud with queries (every slot the sentinel)."""
+    rng = np.random.default_rng(13)
+    plane = rng.random((40000, 3)).astype(np.float32)
+    plane[:, 2] = 0.5
+    slab = rng.random((20000, 3)).astype(np.float32)
+    slab[:, 1] *= 1e-3
+    full = rng.random((65536, 3)).astype(np.float32)
+    cases = [
+        (plane, rng.random((3000, 3)).astype(np.float32), 32),
+        (slab, rng.random((2000, 3)).astype(np.float32), 16),
+        (rng.random((5000, 3)).astype(np.float32), rng.random((1500, 3)).astype(np.float32), 64),
+        (full, rng.random((4000, 3)).astype(np.float32), 32),
+        (full[:, :2].copy(), rng.random((4000, 2)).astype(np.float32), 48),
+    ]
+    for src, qry, k in cases:
+        rc, idx, d2 = _noalloc(naga, src, qry, k)
+        assert rc == naga.NAGA_OK, naga.lib().naga_last_error()
+        ri, rd = _reference(naga, src, qry, k)
+        assert np.array_equal(idx, ri), (src.shape, k)
+        assert np.array_equal(d2, rd), (src.shape, k)
+    empty = np.zeros((0, 3), np.float32)
+    qry = rng.random((10, 3)).astype(np.float32)
+    rc, idx, d2 = _noalloc(naga, empty, qry, 8)
+    assert rc == naga.NAGA_OK
+    assert (idx.view(np.uint32) == 0xFFFFFFFF).all() and np.isinf(d2).all()
