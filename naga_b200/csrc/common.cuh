@@ -38,6 +38,9 @@ int sm_count();
 struct D2Q9 {
     static constexpr int D = 2, Q = 9, QP = 12;  // QP: padded row (3 x float4)
     static constexpr int NGATHER = 2;             // chunks with a nonzero streaming rate
+    // rows of the RK stage buffers and the PML field: only the gathered
+    // chunks, 32 B (one sector per neighbour gather instead of 1.5 at 48 B)
+    static constexpr int QS = 4 * NGATHER;
     static constexpr __host__ __device__ int row(int slot) {
         constexpr int t[12] = {1, 5, 2, 6, 3, 7, 4, 8, 0, -1, -1, -1};
         return t[slot];
@@ -50,6 +53,7 @@ struct D2Q9 {
 struct D3Q27 {
     static constexpr int D = 3, Q = 27, QP = 28;  // QP: padded row (7 x float4)
     static constexpr int NGATHER = 7;              // chunk 0 holds the rest population and a pair
+    static constexpr int QS = QP;                  // stage and PML field rows: the full row
     static constexpr __host__ __device__ int row(int slot) {
         constexpr int t[28] = {0,  -1, 1,  2,  3,  4,  5,  6,  7,  10, 8,  9,  11, 14,
                                12, 13, 15, 18, 16, 17, 19, 26, 20, 25, 21, 24, 22, 23};

@@ -394,10 +394,13 @@ int scene_setup(naga_scene* s) {
     V.sigma = sig;
 
     // state buffers
+    // (the RK stage buffers G1, G2 hold rows of the gathered chunks only)
+    const int QS = D == 2 ? D2Q9::QS : D3Q27::QS;
     float* bufs[7];
     for (int b = 0; b < 7; ++b) {
-        if ((rc = s->alloc(&bufs[b], N * QP))) return rc;
-        NAGA_CUDA_TRY(cudaMemsetAsync(bufs[b], 0, sizeof(float) * N * QP, st));
+        const int64_t row = (b == 1 || b == 2) ? QS : QP;
+        if ((rc = s->alloc(&bufs[b], N * row))) return rc;
+        NAGA_CUDA_TRY(cudaMemsetAsync(bufs[b], 0, sizeof(float) * N * row, st));
     }
     V.G = bufs[0];
     V.G1 = bufs[1];
@@ -441,8 +444,8 @@ int scene_setup(naga_scene* s) {
     float* phi = nullptr;
     float4* pv = nullptr;
     if (s->nl > 0) {
-        if ((rc = s->alloc(&phi, s->nl * QP))) return rc;
-        NAGA_CUDA_TRY(cudaMemsetAsync(phi, 0, sizeof(float) * s->nl * QP, st));
+        if ((rc = s->alloc(&phi, s->nl * QS))) return rc;
+        NAGA_CUDA_TRY(cudaMemsetAsync(phi, 0, sizeof(float) * s->nl * QS, st));
     }
     if ((rc = s->alloc(&pv, 2 * std::max<int64_t>(s->nbl, 1)))) return rc;
     NAGA_CUDA_TRY(cudaMemsetAsync(pv, 0, sizeof(float4) * 2 * std::max<int64_t>(s->nbl, 1), st));

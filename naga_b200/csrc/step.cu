@@ -154,6 +154,14 @@ __device__ __forceinline__ float4 ld4g(const float* base, int64_t i, int c) {
     else
         return __ldg(reinterpret_cast<const float4*>(base + i * L::QP) + c);
 }
+// the same gather load on a stage or PML field row (L::QS floats)
+template <class L>
+__device__ __forceinline__ float4 ld4s(const float* base, int64_t i, int c) {
+    if constexpr (L::D == 3)
+        return ld4cg(base, i, L::QS, c);
+    else
+        return __ldg(reinterpret_cast<const float4*>(base + i * L::QS) + c);
+}
 __device__ __forceinline__ float4 ld4rw(const float* base, int64_t i, int qp, int c) {
     return reinterpret_cast<const float4*>(base + i * qp)[c];
 }
@@ -564,7 +572,13 @@ __global__ void __launch_bounds__(kBlock, (L::D == 3 ? 4 : 8)) k_macro_pml(const
             out[t] = layer ? g[a] - sg * (3.f * ft + 3.f * sg * q1[t] + sg * sg * q2) : g[a];
         }
         store_row<L>(Q1cur, i, q1);
-        if (field) store_row<L>(S.PHI, jf - S.nb, phi);
+        if (field) {
+            // the field row holds the gathered chunks (L::QS floats)
+            float4* pr = reinterpret_cast<float4*>(S.PHI + (jf - S.nb) * L::QS);
+#pragma unroll
+            for (int c = 0; c < L::QS / 4; ++c)
+                pr[c] = make_float4(phi[4 * c], phi[4 * c + 1], phi[4 * c + 2], phi[4 * c + 3]);
+        }
         if (src) store_row<L>(S.S1P, i, out);
         const bool boundary = i >= S.nbl && i < S.nbl + S.nbd;
 #pragma unroll
@@ -881,7 +895,7 @@ __global__ void __launch_bounds__(MTR<L>::BLOCK) k_pml_gather(const WorkItem* __
             const float4 rec = tile[s * nn + ns];
             const uint32_t jl = __float_as_uint(rec.w);
             const float wz = L::D == 3 ? rec.z : 0.f;
-            const float4 v = ld4g<L>(S.PHI, jl, c);
+            const float4 v = ld4s<L>(S.PHI, jl, c);
             const float p0 = d0[0] * rec.x + d0[1] * rec.y + d0[2] * wz;
             const float p1 = d1[0] * rec.x + d1[1] * rec.y + d1[2] * wz;
             dv.x = fmaf(p0, v.x, dv.x);
@@ -1015,12 +1029,20 @@ __global__ void __launch_bounds__(MTF<L>::BLOCK) k_filter(const WorkItem* __rest
             out = f;
         }
         st4(S.G, i, QP, c, out);
-        if (i >= S.nbl) {
+        if constexpr (L::D == 2) {
+            // the gathered chunks of every row also go to G2, the compact
+            // (32-B) rows RK stage 1 gathers from; boundary and ghost rows
+            // keep their values through the stages, so G1 carries them too
+            if (c < L::NGATHER) {
+                st4(S.G2, i, L::QS, c, out);
+                if (i >= S.nbl) st4(S.G1, i, L::QS, c, out);
+            }
+        } else if (i >= S.nbl) {
             // boundary and ghost rows keep their values through the RK
             // stages: the stage buffers carry them so the gathers read
             // every support from one array
-            st4(S.G1, i, QP, c, out);
-            st4(S.G2, i, QP, c, out);
+            st4(S.G1, i, L::QS, c, out);
+            st4(S.G2, i, L::QS, c, out);
         }
     }
     NAGA_PIPE_END
@@ -1061,8 +1083,12 @@ __global__ void __launch_bounds__(MTR<L>::BLOCK) k_rk(const WorkItem* __restrict
     if (ns < nn && c < L::NGATHER) {
         // Horner stages: G1 = g + dt/4 A g, G2 = g + dt/3 A G1, G1 = g + dt/2 A G2,
         // G = g + dt A G1
-        const float* src = (STAGE == 1) ? S.G : (STAGE == 2) ? S.G1 : (STAGE == 3) ? S.G2 : S.G1;
+        // (D2Q9's stage 1 gathers the filter's compact copy of G in G2;
+        // every stage buffer row holds L::QS floats, G rows L::QP)
+        const float* src = (STAGE == 1) ? (D2 ? S.G2 : S.G) : (STAGE == 2) ? S.G1 : (STAGE == 3) ? S.G2 : S.G1;
         float* dst = (STAGE == 1) ? S.G1 : (STAGE == 2) ? S.G2 : (STAGE == 3) ? S.G1 : S.G;
+        constexpr int QSRC = (STAGE == 1 && !D2) ? QP : L::QS;
+        constexpr int QDST = STAGE == 4 ? QP : L::QS;
         const float a = S.rk_a[STAGE - 1];
         const float4 f0 = ld4(S.G, i, QP, c);
         float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -1077,7 +1103,7 @@ __global__ void __launch_bounds__(MTR<L>::BLOCK) k_rk(const WorkItem* __restrict
             }
             const uint32_t j = __float_as_uint(rec.w);
             const float wz = L::D == 3 ? rec.z : 0.f;
-            const float4 v = ld4g<L>(src, j, c);
+            const float4 v = QSRC == QP ? ld4g<L>(src, j, c) : ld4s<L>(src, j, c);
             const float p0 = d0[0] * rec.x + d0[1] * rec.y + d0[2] * wz;
             const float p1 = d1[0] * rec.x + d1[1] * rec.y + d1[2] * wz;
             r.x = fmaf(p0, v.x, r.x);
@@ -1086,8 +1112,8 @@ __global__ void __launch_bounds__(MTR<L>::BLOCK) k_rk(const WorkItem* __restrict
             r.w = fmaf(-p1, v.w, r.w);
         }
         // rate = -r; stage value = g + a rate
-        st4(dst, i, QP, c, make_float4(fmaf(-a, r.x, f0.x), fmaf(-a, r.y, f0.y), fmaf(-a, r.z, f0.z),
-                                      fmaf(-a, r.w, f0.w)));
+        st4(dst, i, QDST, c, make_float4(fmaf(-a, r.x, f0.x), fmaf(-a, r.y, f0.y), fmaf(-a, r.z, f0.z),
+                                        fmaf(-a, r.w, f0.w)));
     }
     NAGA_PIPE_END
 }
