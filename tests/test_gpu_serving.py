@@ -1,6 +1,8 @@
 """The continuous-batching request loop: results alone equal results in the
 mix; admission respects the memory budget and slot limit; a bad request
 fails alone."""
+import time
+
 import numpy as np
 import pytest
 
@@ -15,9 +17,19 @@ def _req(naga, n_side, seed, width):
     return g, drho
 
 
-def _run_until_done(srv, ids, max_ticks=10000):
-    for _ in range(max_ticks):
-        srv.tick()
+def _tick(srv):
+    """One tick; while no scene is active (set-up still running on the
+    server's own thread) it returns at once, so wait a moment then."""
+    active, queued = srv.tick()
+    if active == 0 and queued > 0:
+        time.sleep(0.002)
+    return active, queued
+
+
+def _run_until_done(srv, ids, seconds=120.0):
+    deadline = time.time() + seconds
+    while time.time() < deadline:
+        _tick(srv)
         if all(srv.state(i)[0] in (srv.DONE, srv.FAILED) for i in ids):
             return
     raise AssertionError("requests did not finish")
@@ -37,8 +49,9 @@ def test_results_alone_equal_results_in_the_mix(naga):
     # (steps ahead of set-up on the device: same results)
     srv = naga.Server(2, memory_budget=1 << 30, steps_per_tick=10, max_active=2, step_priority=1)
     ids = [srv.submit(reqs[0][0], reqs[0][1], steps[0], k=16, probes=PROBES2)]
-    srv.tick()
-    srv.tick()
+    deadline = time.time() + 60
+    while time.time() < deadline and srv.stats()["ticks"] < 2:
+        _tick(srv)
     ids += [srv.submit(g, d, n, k=16, probes=PROBES2) for (g, d), n in zip(reqs[1:], steps[1:])]
     _run_until_done(srv, ids)
     st = srv.stats()
@@ -63,7 +76,10 @@ def test_admission_by_memory_budget(naga):
     srv = naga.Server(2, memory_budget=int(est * 1.5), steps_per_tick=10)
     a = srv.submit(g, d, 30, k=16, probes=PROBES2)
     b = srv.submit(g, d, 30, k=16, probes=PROBES2)
-    srv.tick()
+    # set-up runs on the server's own thread: tick until the first joins
+    deadline = time.time() + 60
+    while time.time() < deadline and srv.state(a)[0] != srv.ACTIVE:
+        _tick(srv)
     assert srv.state(a)[0] == srv.ACTIVE and srv.state(b)[0] == srv.QUEUED
     assert srv.stats()["bytes_in_use"] <= int(est * 1.5)
     _run_until_done(srv, [a, b])
@@ -86,4 +102,35 @@ def test_invalid_request_fails_alone(naga):
     assert srv.state(bad)[0] == srv.FAILED
     assert srv.state(ok)[0] == srv.DONE
     assert srv.result(ok).shape == (20, 2)
+    srv.close()
+
+
+def test_latency_target_bounds_the_batch(naga):
+    """With a per-step latency target below any two scenes' step time, the
+    set-up thread admits one request at a time (after the first measured
+    step): the requests still all finish, with results identical to a server
+    without the target, and completion latencies are reported."""
+    reqs = [_req(naga, n, s, w) for n, s, w in ((34, 11, 0.06), (30, 12, 0.07), (40, 13, 0.05))]
+    free = naga.Server(2, memory_budget=1 << 30, steps_per_tick=10)
+    ids = [free.submit(g, d, 30, k=16, probes=PROBES2) for g, d in reqs]
+    _run_until_done(free, ids)
+    ref = [free.result(i) for i in ids]
+    free.close()
+    srv = naga.Server(2, memory_budget=1 << 30, steps_per_tick=10, target_step_ms=1e-4)
+    ids = [srv.submit(g, d, 30, k=16, probes=PROBES2) for g, d in reqs]
+    most = 0
+    deadline = time.time() + 120
+    while time.time() < deadline:
+        active, _ = _tick(srv)
+        if srv.stats()["ticks"] > 0:
+            most = max(most, active)
+        if all(srv.state(i)[0] in (srv.DONE, srv.FAILED) for i in ids):
+            break
+    st = srv.stats()
+    assert st["done"] == 3 and st["failed"] == 0
+    assert most == 1
+    assert st["p50_request_ms"] > 0 and st["p99_request_ms"] >= st["p50_request_ms"]
+    assert st["p50_step_ms"] > 0 and st["admitted"] == 3
+    for i, r in zip(ids, ref):
+        assert np.array_equal(srv.result(i), r)
     srv.close()
