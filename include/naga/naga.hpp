@@ -24,8 +24,11 @@
 #include <naga_b200.h>
 
 #include <algorithm>
+#include <cmath>
+#include <future>
 #include <limits>
 #include <array>
+#include <type_traits>
 #include <cstdint>
 #include <memory>
 #include <stdexcept>
@@ -558,6 +561,86 @@ class simulation_engine {
 
 }  // namespace fluids::nonlocal_lbm
 
+// ------------------------------------------------------------ device arrays
+// A typed device buffer in the role of NAGA's sclx::array: a reference-
+// counted handle (copies share the buffer), either owning memory it
+// allocated (freed with its last copy) or viewing memory the caller owns
+// (never freed here), so the primitives below run on the caller's device
+// pointers without a copy. Sizes are element counts; a NAGA array of shape
+// {D, N} is D * N elements with a point's coordinates adjacent.
+template <class T>
+class device_array {
+  public:
+    using value_type = T;
+    using mutable_type = std::remove_const_t<T>;
+
+    device_array() = default;
+    explicit device_array(size_t n) : n_(n) {
+        mutable_type* p = nullptr;
+        if (cudaMalloc((void**)&p, sizeof(T) * (n ? n : 1)) != cudaSuccess)
+            throw std::runtime_error("naga::device_array: cudaMalloc failed");
+        p_ = std::shared_ptr<T>(p, [](T* q) { cudaFree((void*)q); });
+    }
+    // a view of caller memory (device pointer, n elements); not freed here
+    static device_array view(T* p, size_t n) {
+        device_array a;
+        a.p_ = std::shared_ptr<T>(p, [](T*) {});
+        a.n_ = n;
+        return a;
+    }
+    static device_array from_host(const std::vector<mutable_type>& v, cudaStream_t st = nullptr) {
+        device_array a(v.size());
+        if (!v.empty() && (cudaMemcpyAsync((void*)a.data(), v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice,
+                                           st) != cudaSuccess ||
+                           cudaStreamSynchronize(st) != cudaSuccess))
+            throw std::runtime_error("naga::device_array: host to device copy failed");
+        return a;
+    }
+    // copy to the host after the work queued on `st` has finished
+    std::vector<mutable_type> to_host(cudaStream_t st = nullptr) const {
+        std::vector<mutable_type> v(n_);
+        if (cudaStreamSynchronize(st) != cudaSuccess ||
+            (n_ && cudaMemcpy(v.data(), (const void*)p_.get(), sizeof(T) * n_, cudaMemcpyDeviceToHost) != cudaSuccess))
+            throw std::runtime_error("naga::device_array: device to host copy failed");
+        return v;
+    }
+    // a read-only handle on the same buffer
+    template <class U = T, class = std::enable_if_t<!std::is_const_v<U>>>
+    operator device_array<const U>() const {
+        return device_array<const U>::share(p_, n_);
+    }
+    static device_array share(std::shared_ptr<T> p, size_t n) {
+        device_array a;
+        a.p_ = std::move(p);
+        a.n_ = n;
+        return a;
+    }
+    T* data() const { return p_.get(); }
+    size_t size() const { return n_; }
+    size_t elements() const { return n_; }
+    bool empty() const { return n_ == 0; }
+
+  private:
+    std::shared_ptr<T> p_;
+    size_t n_ = 0;
+};
+
+// NAGA's default_point_map (point_map.cuh:45-81): the points of a {D, N}
+// array, here a device array of D * N values.
+template <class T, unsigned D>
+struct default_point_map {
+    using value_type = T;
+    static constexpr unsigned dimensions = D;
+    device_array<const T> points;
+    default_point_map() = default;
+    default_point_map(device_array<const T> p) : points(std::move(p)) {
+        if (points.size() % D != 0) throw std::invalid_argument("naga::default_point_map: size is not a multiple of D");
+    }
+    template <class U = T, class = std::enable_if_t<!std::is_const_v<U>>>
+    default_point_map(const device_array<U>& p) : default_point_map(device_array<const T>(p)) {}
+    size_t size() const { return points.size() / D; }
+};
+
 namespace detail {
 // device copy of a host vector, freed on scope exit
 template <class T>
@@ -582,9 +665,156 @@ struct device_vec {
     device_vec(const device_vec&) = delete;
     device_vec& operator=(const device_vec&) = delete;
 };
+
+// NAGA's asynchronous calls return std::future<void>; here the work is
+// queued on a stream and the future's get() waits for it
+inline std::future<void> stream_future(cudaStream_t st) {
+    return std::async(std::launch::deferred, [st] {
+        if (cudaStreamSynchronize(st) != cudaSuccess) throw std::runtime_error("naga: stream synchronisation failed");
+    });
+}
 }  // namespace detail
 
 namespace segmentation {
+// NAGA's nd_cubic_segmentation<T, D>(points, approx_partition_size)
+// (segmentation/nd_cubic_segmentation.cuh:227-303): the uniform partition of
+// a point cloud into cells of about approx_partition_size points, built on
+// the device (naga_segmentation_shape / _build). Bounds, width and shape
+// follow NAGA's FP32 arithmetic; every partition lists its points in
+// ascending index order. T = float.
+template <class T, unsigned D>
+class nd_cubic_segmentation {
+    static_assert(std::is_same_v<T, float>, "nd_cubic_segmentation: T = float");
+    static_assert(D == 2 || D == 3, "nd_cubic_segmentation: D = 2 or 3");
+
+  public:
+    nd_cubic_segmentation() = default;
+    nd_cubic_segmentation(const device_array<const T>& points, unsigned approx_partition_size,
+                          cudaStream_t stream = nullptr)
+        : points_(points) {
+        if (points.size() % D != 0)
+            throw std::invalid_argument(
+                "The number of dimensions in the points array does not match the number of dimensions in the "
+                "segmentation");
+        const int64_t n = (int64_t)(points.size() / D);
+        float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0}, w = 0;
+        int64_t shape[3] = {1, 1, 1};
+        detail::check(naga_segmentation_shape(points.data(), n, (int)D, (int)approx_partition_size, lo, hi, &w, shape,
+                                              stream),
+                      "nd_cubic_segmentation");
+        size_t cells = 1;
+        for (unsigned d = 0; d < D; ++d) {
+            lower_[d] = lo[d];
+            upper_[d] = hi[d];
+            shape_[d] = (size_t)shape[d];
+            cells *= shape_[d];
+        }
+        width_ = w;
+        sizes_ = device_array<uint32_t>(cells);
+        offsets_ = device_array<uint32_t>(cells);
+        indices_ = device_array<uint32_t>((size_t)n);
+        detail::check(naga_segmentation_build(points.data(), n, (int)D, lo, hi, w, shape, sizes_.data(),
+                                              offsets_.data(), indices_.data(), stream),
+                      "nd_cubic_segmentation");
+        if (cudaStreamSynchronize(stream) != cudaSuccess)
+            throw std::runtime_error("nd_cubic_segmentation: stream synchronisation failed");
+    }
+
+    // get_partition_index (nd_cubic_segmentation.cuh:376-392) on the host,
+    // in the same FP32 arithmetic (a quotient that rounds up to the shape is
+    // clamped to the last cell)
+    template <class PointType>
+    std::array<size_t, D> get_partition_index(const PointType& p) const {
+        std::array<size_t, D> c{};
+        for (unsigned d = 0; d < D; ++d) {
+            const float x = (float)p[d];
+            if (x < lower_[d])
+                c[d] = 0;
+            else if (x >= upper_[d])
+                c[d] = shape_[d] - 1;
+            else
+                c[d] = std::min((size_t)std::floor((x - lower_[d]) / width_), shape_[d] - 1);
+        }
+        return c;
+    }
+    size_t linear_index(const std::array<size_t, D>& c) const {
+        size_t lin = 0, mul = 1;
+        for (unsigned d = 0; d < D; ++d) {
+            lin += c[d] * mul;
+            mul *= shape_[d];
+        }
+        return lin;
+    }
+    // point indices of one partition (get_partition), copied to the host
+    std::vector<uint32_t> get_partition(size_t linear) const {
+        if (linear >= partition_count()) throw std::invalid_argument("nd_cubic_segmentation: partition out of range");
+        uint32_t size = 0, off = 0;
+        if (cudaMemcpy(&size, sizes_.data() + linear, 4, cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(&off, offsets_.data() + linear, 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+            throw std::runtime_error("nd_cubic_segmentation: copy failed");
+        std::vector<uint32_t> v(size);
+        if (size && cudaMemcpy(v.data(), indices_.data() + off, 4 * size, cudaMemcpyDeviceToHost) != cudaSuccess)
+            throw std::runtime_error("nd_cubic_segmentation: copy failed");
+        return v;
+    }
+
+    const std::array<size_t, D>& shape() const { return shape_; }
+    size_t partition_count() const {
+        size_t c = 1;
+        for (unsigned d = 0; d < D; ++d) c *= shape_[d];
+        return c;
+    }
+    size_t point_count() const { return points_.size() / D; }
+    T partition_width() const { return width_; }
+    const std::array<T, D>& lower_bounds() const { return lower_; }
+    const std::array<T, D>& upper_bounds() const { return upper_; }
+    device_array<const T> points() const { return points_; }
+    // device arrays: partition sizes and their exclusive prefix sums (one per
+    // partition, linear index x + shape[0] (y + shape[1] z)), point indices
+    // grouped by partition
+    device_array<const uint32_t> partition_sizes() const { return sizes_; }
+    device_array<const uint32_t> partition_index_offsets() const { return offsets_; }
+    device_array<const uint32_t> indices() const { return indices_; }
+
+  private:
+    device_array<const T> points_;
+    device_array<uint32_t> sizes_, offsets_, indices_;
+    std::array<T, D> lower_{}, upper_{};
+    std::array<size_t, D> shape_{};
+    T width_{};
+};
+
+// batched_nearest_neighbors(k, distances_squared, indices, query_points,
+// segmented_ref_points) (nearest_neighbors.cuh:95-108): the exact k nearest
+// of every query among the segmentation's points under the (dist^2, index)
+// order (naga_knn), into caller arrays of k * n_queries elements (a query's
+// k entries adjacent, ascending). Queued on `stream`.
+template <class T, unsigned D>
+void batched_nearest_neighbors(unsigned k, device_array<T>& distances_squared, device_array<uint32_t>& indices,
+                               const default_point_map<T, D>& query_points,
+                               const nd_cubic_segmentation<T, D>& segmented_ref_points,
+                               cudaStream_t stream = nullptr) {
+    const size_t nq = query_points.size();
+    if (distances_squared.size() != (size_t)k * nq || indices.size() != (size_t)k * nq)
+        throw std::invalid_argument("batched_nearest_neighbors: output arrays must hold k x n_queries values");
+    detail::check(naga_knn(segmented_ref_points.points().data(), (int64_t)segmented_ref_points.point_count(),
+                           query_points.points.data(), (int64_t)nq, (int)D, (int)k, indices.data(),
+                           distances_squared.data(), stream),
+                  "batched_nearest_neighbors");
+}
+
+// batched_nearest_neighbors(k, query_points, segmented_ref_points)
+// (nearest_neighbors.cuh:444-477): returns {distances_squared, indices}.
+template <class T, unsigned D>
+std::tuple<device_array<T>, device_array<uint32_t>> batched_nearest_neighbors(
+    unsigned k, const default_point_map<T, D>& query_points, const nd_cubic_segmentation<T, D>& segmented_ref_points,
+    cudaStream_t stream = nullptr) {
+    device_array<T> d2((size_t)k * query_points.size());
+    device_array<uint32_t> idx((size_t)k * query_points.size());
+    batched_nearest_neighbors(k, d2, idx, query_points, segmented_ref_points, stream);
+    return {d2, idx};
+}
+
 // Exact k nearest neighbours of `queries` among `points` (host arrays,
 // D x count with a point's coordinates adjacent). Returns {dist^2, indices},
 // k x count with a query's k entries adjacent, ascending in (dist^2, index).
@@ -600,6 +830,212 @@ std::tuple<std::vector<float>, std::vector<uint32_t>> batched_nearest_neighbors(
     return {dd.host(nq * k, stream), di.host(nq * k, stream)};
 }
 }  // namespace segmentation
+
+namespace interpolation {
+// NAGA's multiquadric (interpolation/radial_point_method.cuh:44-66):
+// (r^2 + (alpha_c h)^2)^q; the device solves implement q = 1/2, alpha_c =
+// 1/10 (NAGA's defaults and the only values its callers use)
+template <class T = float>
+struct mq_shape_function {
+    static constexpr int id = 0;
+    T q_ = T(0.5), alpha_c_ = T(0.1);
+    mq_shape_function(const T& q = T(0.5), const T& alpha_c = T(0.1)) : q_(q), alpha_c_(alpha_c) {}
+    void check() const {
+        if (q_ != T(0.5) || alpha_c_ != T(0.1))
+            throw std::invalid_argument("mq_shape_function: the device solves implement q = 0.5, alpha_c = 0.1");
+    }
+};
+// the cubic polyharmonic spline r^3 (no NAGA counterpart; the benchmark
+// configurations name it)
+template <class T = float>
+struct cubic_shape_function {
+    static constexpr int id = 1;
+    void check() const {}
+};
+
+// NAGA's radial_point_method<T> (interpolation/radial_point_method.cuh:
+// 92-280) for T = float: weights from augmented RBF systems solved on the
+// device (FP64, or FP32 with FP64-residual refinement when precision = 1),
+// and the interpolation gather. interpolate() queues the gather on the
+// stream and returns a future whose get() waits for it, as NAGA's does.
+template <class T = float>
+class radial_point_method {
+    static_assert(std::is_same_v<T, float>, "radial_point_method: T = float");
+
+  public:
+    radial_point_method() = default;
+
+    // weights [n_queries][k] (NAGA's {k, n_queries}); interpolating_indices
+    // [n_queries / group_size][k], indices into source_points (D x N)
+    template <unsigned D, class ShapeFunctionType = mq_shape_function<T>>
+    static device_array<T> compute_weights(const device_array<const T>& source_points,
+                                           const device_array<const uint32_t>& interpolating_indices,
+                                           const default_point_map<T, D>& query_points,
+                                           const T& approx_particle_spacing, unsigned group_size = 1,
+                                           const ShapeFunctionType& shape_function = ShapeFunctionType{},
+                                           int precision = 0, cudaStream_t stream = nullptr) {
+        shape_function.check();
+        const size_t nq = query_points.size();
+        if (group_size == 0 || nq % group_size != 0)
+            throw std::invalid_argument("query_size must be a multiple of group_size");
+        const size_t ngroups = nq / group_size;
+        if (ngroups == 0) return device_array<T>(0);
+        if (interpolating_indices.size() % ngroups != 0)
+            throw std::invalid_argument("radial_point_method: indices must hold k x (n_queries / group_size) values");
+        const int k = (int)(interpolating_indices.size() / ngroups);
+        device_array<T> w(nq * (size_t)k);
+        detail::check(naga_rbf_weights_f32(source_points.data(), (int64_t)(source_points.size() / D), (int)D,
+                                           interpolating_indices.data(), k, query_points.points.data(),
+                                           (int64_t)ngroups, (int)group_size, approx_particle_spacing,
+                                           ShapeFunctionType::id, precision, w.data(), stream),
+                      "radial_point_method::compute_weights");
+        return w;
+    }
+
+    template <unsigned D, class ShapeFunctionType = mq_shape_function<T>>
+    static radial_point_method create_interpolator(const device_array<const T>& source_points,
+                                                   const device_array<const uint32_t>& interpolating_indices,
+                                                   const default_point_map<T, D>& query_points,
+                                                   const T& approx_particle_spacing, unsigned group_size = 1,
+                                                   const ShapeFunctionType& shape_function = ShapeFunctionType{},
+                                                   int precision = 0, cudaStream_t stream = nullptr) {
+        radial_point_method r;
+        r.weights_ = compute_weights<D>(source_points, interpolating_indices, query_points, approx_particle_spacing,
+                                        group_size, shape_function, precision, stream);
+        r.indices_ = interpolating_indices;
+        r.group_size_ = group_size;
+        r.n_queries_ = query_points.size();
+        r.k_ = r.n_queries_ ? r.weights_.size() / r.n_queries_ : 0;
+        r.source_points_size_ = source_points.size() / D;
+        return r;
+    }
+
+    // destination = sum_s w (field(support) - offset) + offset for every
+    // query; field holds C values per source point and destination C per
+    // query (C = 1: NAGA's one-dimensional overload, C > 1: its {C, N} one)
+    std::future<void> interpolate(const device_array<const T>& field, const device_array<T>& destination,
+                                  T centering_offset = T(0), cudaStream_t stream = nullptr) const {
+        if (source_points_size_ == 0 || field.size() % source_points_size_ != 0)
+            throw std::invalid_argument(
+                "field array must have the same number of rows as the number of source points used to construct "
+                "the interpolator");
+        const size_t C = field.size() / source_points_size_;
+        if (destination.size() != C * n_queries_)
+            throw std::invalid_argument(
+                "destination array must have the same number of columns as the number of points used to "
+                "construct the interpolator");
+        detail::check(naga_rbf_interpolate(weights_.data(), indices_.data(), (int64_t)n_queries_, (int)group_size_,
+                                           (int)k_, field.data(), (int64_t)source_points_size_, (int)C,
+                                           centering_offset, destination.data(), stream),
+                      "radial_point_method::interpolate");
+        return detail::stream_future(stream);
+    }
+
+    device_array<const T> weights() const { return weights_; }
+    device_array<const uint32_t> indices() const { return indices_; }
+    unsigned group_size() const { return group_size_; }
+    size_t support_size() const { return k_; }
+
+  private:
+    device_array<T> weights_;
+    device_array<const uint32_t> indices_;
+    unsigned group_size_ = 1;
+    size_t n_queries_ = 0, k_ = 0, source_points_size_ = 0;
+};
+}  // namespace interpolation
+
+namespace nonlocal_calculus {
+// NAGA's divergence_operator<T, D> (nonlocal_calculus/divergence.cuh:44-
+// 212): the nonlocal divergence stencil of a point cloud (kNN, interaction
+// radii, quadrature RPIM weights; naga_divergence_build[_f32]) and its
+// gather apply(field, result, centering_offset) (naga_divergence_apply
+// [_f64]). T = float stores FP32 weights (the engine's instantiation), T =
+// double FP64 ones (NAGA's nonlocal_divergence_3d example). The stencil
+// size is NAGA's num_interp_support, 32, unless `k` says otherwise;
+// `shape` picks the RBF (0 multiquadric, NAGA's; 1 r^3).
+template <class T, unsigned D>
+class divergence_operator {
+    static_assert(std::is_same_v<T, float> || std::is_same_v<T, double>, "divergence_operator: float or double");
+
+  public:
+    using default_field_map = default_point_map<T, D>;
+    divergence_operator() = default;
+
+    // create(domain, query_points, override_query_size): NAGA's weight
+    // kernel reads the node position from the domain array
+    // (detail/divergence.inl:171), so its every caller passes the domain as
+    // the query set; so must callers here (the same array). Rows past the
+    // point count up to override_query_size are zero, as NAGA's.
+    static divergence_operator create(const device_array<const T>& domain, const device_array<const T>& query_points,
+                                      size_t override_query_size = 0, int k = 32, int shape = 0, int precision = 0,
+                                      cudaStream_t stream = nullptr) {
+        if (query_points.data() != domain.data() || query_points.size() != domain.size())
+            throw std::invalid_argument(
+                "divergence_operator::create: the query points must be the domain (the stencil weights are built at "
+                "the domain's nodes)");
+        const size_t n = domain.size() / D;
+        const size_t rows = override_query_size == 0 ? n : override_query_size;
+        if (rows < n)
+            throw std::invalid_argument("override_query_size must be at least as large as the number of query points.");
+        device_array<float> pts32;
+        const float* pts = nullptr;
+        if constexpr (std::is_same_v<T, float>) {
+            pts = domain.data();
+        } else {
+            std::vector<double> h = domain.to_host(stream);
+            pts32 = device_array<float>::from_host(std::vector<float>(h.begin(), h.end()), stream);
+            pts = pts32.data();
+        }
+        divergence_operator op;
+        op.k_ = (size_t)k;
+        op.rows_ = rows;
+        op.weights_ = device_array<T>(rows * (size_t)k * D);
+        op.support_indices_ = device_array<uint32_t>(rows * (size_t)k);
+        if (cudaMemsetAsync(op.weights_.data(), 0, sizeof(T) * op.weights_.size(), stream) != cudaSuccess ||
+            cudaMemsetAsync(op.support_indices_.data(), 0, 4 * op.support_indices_.size(), stream) != cudaSuccess)
+            throw std::runtime_error("divergence_operator::create: memset failed");
+        if constexpr (std::is_same_v<T, float>)
+            detail::check(naga_divergence_build_f32(pts, (int64_t)n, (int)D, k, shape, precision,
+                                                    op.support_indices_.data(), op.weights_.data(), nullptr, stream),
+                          "divergence_operator::create");
+        else
+            detail::check(naga_divergence_build(pts, (int64_t)n, (int)D, k, shape, precision,
+                                                op.support_indices_.data(), op.weights_.data(), nullptr, stream),
+                          "divergence_operator::create");
+        return op;
+    }
+    static divergence_operator create(const device_array<const T>& domain, cudaStream_t stream = nullptr) {
+        return create(domain, domain, 0, 32, 0, 0, stream);
+    }
+
+    // result_i = sum_s sum_d W(d, s, i) (field_d(support(s, i)) - offset),
+    // queued on `stream` (divergence.cuh:377-488)
+    void apply(const default_field_map& field, const device_array<T>& result, const T& centering_offset = T(0),
+               cudaStream_t stream = nullptr) const {
+        if (result.size() != rows_) throw std::invalid_argument("Result array has incorrect shape.");
+        if (result.size() != field.size()) throw std::invalid_argument("Result array has incorrect size.");
+        if constexpr (std::is_same_v<T, float>)
+            detail::check(naga_divergence_apply(weights_.data(), support_indices_.data(), (int64_t)rows_, (int)D,
+                                                (int)k_, field.points.data(), centering_offset, result.data(), stream),
+                          "divergence_operator::apply");
+        else
+            detail::check(naga_divergence_apply_f64(weights_.data(), support_indices_.data(), (int64_t)rows_,
+                                                    (int)D, (int)k_, field.points.data(), centering_offset,
+                                                    result.data(), stream),
+                          "divergence_operator::apply");
+    }
+
+    // weights [rows][k][D] (NAGA's {D, k, rows}); support indices [rows][k]
+    device_array<const T> weights() const { return weights_; }
+    device_array<const uint32_t> support_indices() const { return support_indices_; }
+    size_t support_size() const { return k_; }
+
+  private:
+    device_array<T> weights_;
+    device_array<uint32_t> support_indices_;
+    size_t k_ = 0, rows_ = 0;
+};
+}  // namespace nonlocal_calculus
 
 namespace linalg {
 // Inverse of `batch` n x n matrices stored back to back, column-major
@@ -617,6 +1053,29 @@ inline std::vector<double> batched_matrix_inverse(const std::vector<double>& A, 
     for (int v : inf)
         if (v != 0) throw std::runtime_error("batched_matrix_inverse: singular or unconverged matrix in the batch");
     return dX.host(A.size(), stream);
+}
+
+// batched_matrix_inverse(A, A_inv) (linalg/batched_matrix_inverse.cuh:
+// 389-397) on caller device arrays of `batch` column-major n x n matrices;
+// info (batch entries, or empty) receives getrf's status per matrix. Queued
+// on `stream`; the future's get() waits for it.
+inline std::future<void> batched_matrix_inverse(const device_array<const double>& A, const device_array<double>& A_inv,
+                                                int n, const device_array<int>& info = {}, bool refined = false,
+                                                cudaStream_t stream = nullptr) {
+    if (n < 1 || A.size() % ((size_t)n * n) != 0 || A_inv.size() != A.size())
+        throw std::invalid_argument("batched_matrix_inverse: A and A_inv must hold batch x n x n values");
+    const int64_t batch = (int64_t)(A.size() / ((size_t)n * n));
+    if (!info.empty() && info.size() != (size_t)batch)
+        throw std::invalid_argument("batched_matrix_inverse: info must hold one entry per matrix");
+    if (refined)
+        detail::check(naga_batched_inverse_f32r(A.data(), A_inv.data(), n, batch, 30, 1e-14,
+                                                info.empty() ? nullptr : info.data(), stream),
+                      "batched_matrix_inverse");
+    else
+        detail::check(naga_batched_inverse_f64(A.data(), A_inv.data(), n, batch, info.empty() ? nullptr : info.data(),
+                                               stream),
+                      "batched_matrix_inverse");
+    return detail::stream_future(stream);
 }
 }  // namespace linalg
 

@@ -117,17 +117,21 @@ int naga_knn(const float* src, int64_t n, const float* qry, int64_t nq,
 /* The same search without allocating device memory, for callers that
  * cannot call cudaMalloc while they run: processes that handed the free
  * device memory to their own caching allocator at start-up and live on a
- * fixed budget, and latency-critical paths where cudaMalloc / cudaFree may
- * synchronise the device and stall other streams. No reference counterpart
- * (NAGA allocates its segmentation arrays on every call).
+ * fixed budget, and paths that must not let cudaMalloc / cudaFree
+ * synchronise the whole device and stall other streams. No reference
+ * counterpart (NAGA allocates its segmentation arrays on every call).
  * Scratch is one fixed device array of ~1.8 MB inside the library, held by
  * every GPU that loads it until the process exits; hence n <= 65536 source
  * points (larger n returns NAGA_EINVAL), any number of queries. The first
  * call on a device looks up the array's device address
- * (cudaGetSymbolAddress); make that first call before any stream capture.
- * Every call shares the one array: calls that overlap on the GPU (other
- * streams, other host threads) race, so serialise them. Each call resets
- * the counters it needs. Results equal naga_knn's bit for bit.             */
+ * (cudaGetSymbolAddress), and so does the first call after the device's
+ * context was re-created (cudaDeviceReset); make that first call before any
+ * stream capture. Each call synchronises `stream` once: it reads the
+ * cloud's bounding box back to the host to size its cell grid, then queues
+ * the search behind it and returns. Every call shares the one array: calls
+ * that overlap on the GPU (other streams, other host threads) race, so
+ * serialise them. Each call resets the counters it needs. Results equal
+ * naga_knn's bit for bit.                                                  */
 int naga_knn_noalloc(const float* src, int64_t n, const float* qry,
                      int64_t nq, int dim, int k, uint32_t* idx, float* d2,
                      void* stream);
@@ -188,13 +192,71 @@ int64_t naga_refinement_fallbacks(void);
 int naga_divergence_build(const float* pts, int64_t n, int dim, int k,
                           int shape, int precision, uint32_t* idx, double* W,
                           double* delta, void* stream);
-/* result_i = sum_s sum_d W(d,s,i) * field[idx(s,i)][d] with W stored FP32
- * [n][k][dim] and field [n][dim] (device). Replaces
- * divergence_operator::apply with default_point_map
- * (nonlocal_calculus/divergence.cuh:183-212, 377-488).                      */
+/* The same stencil with FP32 outputs: W [n][k][dim] and delta [n] (or
+ * NULL) as floats (the solves stay FP64 or refined FP32 as `precision`
+ * says). Replaces divergence_operator<float, D>::create(domain) (the
+ * engine's T = float instantiation, detail/simulation_engine.cuh:169-181). */
+int naga_divergence_build_f32(const float* pts, int64_t n, int dim, int k,
+                              int shape, int precision, uint32_t* idx,
+                              float* W, float* delta, void* stream);
+/* result_i = sum_s t_s, t_s = sum_d W(d,s,i) (field[idx(s,i)][d] - offset)
+ * with W stored [n][k][dim] and field [n][dim] (device); the t_s are summed
+ * by NAGA's pairwise tree (stride 1, 2, 4, ...), k <= 64. Replaces
+ * divergence_operator<T, D>::apply(field, result, centering_offset) with
+ * default_point_map (nonlocal_calculus/divergence.cuh:183-212, 377-488):
+ * FP32 here, FP64 in naga_divergence_apply_f64.                            */
 int naga_divergence_apply(const float* W, const uint32_t* idx, int64_t n,
-                          int dim, int k, const float* field, float* result,
-                          void* stream);
+                          int dim, int k, const float* field,
+                          float centering_offset, float* result, void* stream);
+int naga_divergence_apply_f64(const double* W, const uint32_t* idx, int64_t n,
+                              int dim, int k, const double* field,
+                              double centering_offset, double* result,
+                              void* stream);
+
+/* RBF weights with FP32 queries and FP32 weights (the solves are FP64, or
+ * refined FP32 with precision 1): radial_point_method<float>::
+ * compute_weights(source_points, interpolating_indices, query_points,
+ * approx_particle_spacing, group_size, shape_function)
+ * (interpolation/radial_point_method.cuh:118-139). Arguments as
+ * naga_rbf_weights; weights [ngroups * group][k] (NAGA's {k, n_queries}).  */
+int naga_rbf_weights_f32(const float* src, int64_t n, int dim,
+                         const uint32_t* support, int k, const float* qry,
+                         int64_t ngroups, int group, float spacing, int shape,
+                         int precision, float* weights, void* stream);
+/* out[q][c] = sum_s weights[q][s] (field[support[q / group][s]][c] - offset)
+ * + offset, summed over s in order in FP32: radial_point_method<float>::
+ * interpolate(field, destination, centering_offset)
+ * (interpolation/radial_point_method.cuh:172-280) for n_fields components
+ * per point (field [n_src][n_fields], out [nq][n_fields]; n_fields = 1 is
+ * the one-dimensional overload). Device arrays.                           */
+int naga_rbf_interpolate(const float* weights, const uint32_t* support,
+                         int64_t nq, int group, int k, const float* field,
+                         int64_t n_src, int n_fields, float centering_offset,
+                         float* out, void* stream);
+
+/* NAGA's nd_cubic_segmentation<float, D>(points, approx_partition_size)
+ * (segmentation/nd_cubic_segmentation.cuh:227-303) in two calls. First the
+ * partition grid, on the host in NAGA's FP32 arithmetic from the device
+ * bounds: lower / upper bounds (an axis thinner than 1e-3 widened to 1e-3),
+ * width = (approx / n * volume)^(1/dim), shape[d] = ceil(extent / width),
+ * upper = lower + shape * width (host outputs, dim entries each; the call
+ * synchronises the stream). Then the partitions: every point's partition
+ * as get_partition_index (:376-392; x >= upper -> shape - 1, and a
+ * quotient that rounds up to shape is clamped to shape - 1), linear index
+ * x + shape[0] (y + shape[1] z); sizes [n_partitions], their exclusive
+ * prefix sums offsets [n_partitions] and the point indices grouped by
+ * partition indices [n] (device outputs; n_partitions = product of
+ * shape). Within a partition the indices ascend (NAGA's order there is that
+ * of its atomic increments).                                              */
+int naga_segmentation_shape(const float* pts, int64_t n, int dim,
+                            int approx_partition_size, float* lower,
+                            float* upper, float* width, int64_t* shape,
+                            void* stream);
+int naga_segmentation_build(const float* pts, int64_t n, int dim,
+                            const float* lower, const float* upper,
+                            float width, const int64_t* shape,
+                            uint32_t* sizes, uint32_t* offsets,
+                            uint32_t* indices, void* stream);
 
 /* ---------------------------------------------------------------- scenes */
 /* One acoustic scene: domain, stencils and device-resident state.
@@ -354,16 +416,20 @@ int naga_batch_sync(naga_batch* batch);
 
 /* --------------------------------------------------------------- serving */
 /* Continuous-batching request loop: requests (a scene and a step count)
- * queue FIFO; every naga_server_tick advances all active scenes by
- * steps_per_tick steps as one batch while queued requests that fit the
- * device-memory budget and the slot limit are set up on their own streams,
- * then retires finished requests (their probe traces kept on the host) and
- * admits the new ones into the batch. Set-ups in one tick stop once their
- * host time exceeds the previous tick's step time (at least one per tick),
- * so a burst of arrivals does not stall the running scenes. Batch changes
- * (naga_batch_prepare) happen before the timed steps of a tick, so the
- * latency samples are the steps themselves. No reference counterpart: NAGA
- * steps one engine at a time (simulation_engine.cuh:76).                  */
+ * queue FIFO. A set-up thread of the server admits them -- scene set-up
+ * (kNN, RPIM and stencil weight solves) on each scene's own stream,
+ * overlapping the running batch on the device -- while the requests fit
+ * the device-memory budget and the slot limit and, with a per-step latency
+ * target, while the batch's step time with them (estimated from the
+ * measured time per node-step) stays within the target; it also frees the
+ * scenes of retired requests. Every naga_server_tick, on the caller's
+ * thread, advances all active scenes by steps_per_tick steps as one batch
+ * (a CUDA event after each step gives the per-step latency samples), then
+ * retires finished requests (their probe traces kept on the host) and adds
+ * the scenes whose set-up finished; batch changes (naga_batch_prepare)
+ * happen before the timed steps of a tick. The tick never waits for
+ * set-up. No reference counterpart: NAGA steps one engine at a time
+ * (simulation_engine.cuh:76).                                              */
 typedef struct naga_server naga_server;
 
 typedef struct naga_server_config {
@@ -371,23 +437,30 @@ typedef struct naga_server_config {
     int steps_per_tick;    /* steps per tick (>= 1)                          */
     int max_active;        /* scene slots, 0 = limited by memory only        */
     int step_priority;     /* 0: the batch's steps and admissions' set-up
-                              share the device (more admissions); 1: steps
-                              first (naga_batch_create_with_priority): lower
-                              step latency, slower admission                */
+                              share the device; 1: steps first
+                              (naga_batch_create_with_priority)             */
     int64_t memory_budget; /* device bytes the active scenes may hold        */
+    double target_step_ms; /* per-step latency target of the batch, 0 = none:
+                              admission stops while the estimated step time
+                              with the next request would exceed it (an
+                              empty batch always takes one request)        */
 } naga_server_config;
 
 typedef struct naga_server_stats {
     int64_t ticks, steps, node_updates;
     double busy_ms;         /* device time of the batch steps               */
-    double p50_step_ms, p99_step_ms;
+    double p50_step_ms, p99_step_ms;  /* per-step device time (events)     */
     int64_t bytes_in_use, peak_bytes;
     int64_t done, failed;
-    int active, queued;
-    /* host wall time spent in each phase of naga_server_tick, summed:
-     * preparing the batch (membership changes, graph capture), admitting
-     * (scene set-up), waiting for the batch, retiring and growing it      */
+    int active, queued;     /* queued includes requests in set-up          */
+    /* host wall time summed per activity: preparing the batch (membership
+     * changes, graph capture), scene set-up (on the set-up thread), waiting
+     * for the batch's steps, retiring and growing the batch               */
     double prepare_ms, admit_ms, wait_ms, retire_ms;
+    /* wall time from submission to completion of the finished requests,
+     * and from submission to the end of set-up of the admitted ones        */
+    double p50_request_ms, p99_request_ms, p50_queue_ms;
+    int64_t admitted;
 } naga_server_stats;
 
 /* estimated device bytes of a scene (resident state plus set-up scratch)  */

@@ -18,7 +18,8 @@ import numpy as np
 __all__ = [
     "NagaError", "lib", "build", "GridSpec", "SceneDesc", "generate_grid", "gaussian_pulse",
     "Scene", "Batch", "knn", "knn_clouds", "batched_inverse_f64", "batched_inverse_f32r",
-    "rbf_weights", "divergence_build", "profile", "Q_OF", "lattice_weights",
+    "rbf_weights", "divergence_build", "profile", "Q_OF", "lattice_weights", "divergence_build_f32",
+    "divergence_apply", "rbf_weights_f32", "rbf_interpolate", "cubic_segmentation",
 ]
 
 PKG = os.path.dirname(os.path.abspath(__file__))
@@ -80,7 +81,19 @@ _SIGS = {
     "naga_divergence_build": ([C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
                                C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "naga_divergence_apply": ([C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_void_p,
-                               C.c_void_p, C.c_void_p], C.c_int),
+                               C.c_float, C.c_void_p, C.c_void_p], C.c_int),
+    "naga_divergence_apply_f64": ([C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_void_p,
+                                   C.c_double, C.c_void_p, C.c_void_p], C.c_int),
+    "naga_divergence_build_f32": ([C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                                   C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "naga_rbf_weights_f32": ([C.c_void_p, C.c_int64, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int64,
+                              C.c_int, C.c_float, C.c_int, C.c_int, C.c_void_p, C.c_void_p], C.c_int),
+    "naga_rbf_interpolate": ([C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_void_p, C.c_int64,
+                              C.c_int, C.c_float, C.c_void_p, C.c_void_p], C.c_int),
+    "naga_segmentation_shape": ([C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                 C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "naga_segmentation_build": ([C.c_void_p, C.c_int64, C.c_int, C.c_void_p, C.c_void_p, C.c_float,
+                                 C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "naga_scene_create": ([C.c_void_p, C.c_void_p], C.c_int),
     "naga_scene_destroy": ([C.c_void_p], C.c_int),
     "naga_scene_stream": ([C.c_void_p], C.c_void_p),
@@ -442,7 +455,7 @@ class Batch:
 # ---------------------------------------------------------------- serving
 class ServerConfig(C.Structure):
     _fields_ = [("dim", C.c_int), ("steps_per_tick", C.c_int), ("max_active", C.c_int),
-                ("step_priority", C.c_int), ("memory_budget", C.c_int64)]
+                ("step_priority", C.c_int), ("memory_budget", C.c_int64), ("target_step_ms", C.c_double)]
 
 
 class ServerStats(C.Structure):
@@ -451,7 +464,8 @@ class ServerStats(C.Structure):
                 ("bytes_in_use", C.c_int64), ("peak_bytes", C.c_int64), ("done", C.c_int64),
                 ("failed", C.c_int64), ("active", C.c_int), ("queued", C.c_int),
                 ("prepare_ms", C.c_double), ("admit_ms", C.c_double), ("wait_ms", C.c_double),
-                ("retire_ms", C.c_double)]
+                ("retire_ms", C.c_double), ("p50_request_ms", C.c_double), ("p99_request_ms", C.c_double),
+                ("p50_queue_ms", C.c_double), ("admitted", C.c_int64)]
 
 
 def scene_desc(grid: dict, *, k: int, k_boundary=None, k_probe=None, shape=1, pml_indexing=0,
@@ -485,9 +499,9 @@ class Server:
     QUEUED, ACTIVE, DONE, FAILED = 0, 1, 2, 3
 
     def __init__(self, dim: int, memory_budget: int, steps_per_tick: int = 50, max_active: int = 0,
-                 step_priority: int = 0):
+                 step_priority: int = 0, target_step_ms: float = 0.0):
         self.h = C.c_void_p()
-        cfg = ServerConfig(dim, steps_per_tick, max_active, step_priority, memory_budget)
+        cfg = ServerConfig(dim, steps_per_tick, max_active, step_priority, memory_budget, target_step_ms)
         _check(lib().naga_server_create(C.byref(cfg), C.byref(self.h)))
         self.n_probes = {}
 
@@ -622,6 +636,84 @@ def divergence_build(pts, k: int, shape: int, precision: int = 0):
     _check(lib().naga_divergence_build(_dptr(pts), n, dim, k, shape, precision, _dptr(idx), _dptr(W),
                                        _dptr(delta), _stream_ptr()))
     return idx, W, delta
+
+
+def divergence_build_f32(pts, k: int, shape: int, precision: int = 0):
+    """The stencil with FP32 outputs: (idx int32 [n][k], W float32 [n][k][dim],
+    delta float32 [n])."""
+    torch = _torch()
+    pts = pts.contiguous().float()
+    n, dim = pts.shape
+    idx = torch.empty((n, k), dtype=torch.int32, device=pts.device)
+    W = torch.empty((n, k, dim), dtype=torch.float32, device=pts.device)
+    delta = torch.empty(n, dtype=torch.float32, device=pts.device)
+    _check(lib().naga_divergence_build_f32(_dptr(pts), n, dim, k, shape, precision, _dptr(idx), _dptr(W),
+                                           _dptr(delta), _stream_ptr()))
+    return idx, W, delta
+
+
+def divergence_apply(W, idx, field, centering_offset: float = 0.0):
+    """divergence_operator::apply: result_i = sum_s sum_d W[i, s, d]
+    (field[idx[i, s], d] - offset); FP32 or FP64 by W's dtype."""
+    torch = _torch()
+    W = W.contiguous()
+    idx = idx.contiguous().to(torch.int32)
+    field = field.contiguous().to(W.dtype)
+    n, k, dim = W.shape
+    out = torch.empty(n, dtype=W.dtype, device=W.device)
+    fn = lib().naga_divergence_apply_f64 if W.dtype == torch.float64 else lib().naga_divergence_apply
+    _check(fn(_dptr(W), _dptr(idx), n, dim, k, _dptr(field), centering_offset, _dptr(out), _stream_ptr()))
+    return out
+
+
+def rbf_weights_f32(src, support, qry, group: int, spacing: float, shape: int, precision: int = 0):
+    """RBF weights with FP32 queries and outputs (FP64 solves)."""
+    torch = _torch()
+    src = src.contiguous().float()
+    support = support.contiguous().to(torch.int32)
+    qry = qry.contiguous().float()
+    ng, k = support.shape
+    w = torch.empty((ng * group, k), dtype=torch.float32, device=src.device)
+    _check(lib().naga_rbf_weights_f32(_dptr(src), src.shape[0], src.shape[1], _dptr(support), k, _dptr(qry),
+                                      ng, group, spacing, shape, precision, _dptr(w), _stream_ptr()))
+    return w
+
+
+def rbf_interpolate(weights, support, field, group: int = 1, centering_offset: float = 0.0):
+    """radial_point_method::interpolate: field [n_src] or [n_src][c] float32
+    -> [nq] or [nq][c]."""
+    torch = _torch()
+    weights = weights.contiguous().float()
+    support = support.contiguous().to(torch.int32)
+    one = field.dim() == 1
+    f = field.contiguous().float().reshape(field.shape[0], -1)
+    nq, k = weights.shape
+    out = torch.empty((nq, f.shape[1]), dtype=torch.float32, device=f.device)
+    _check(lib().naga_rbf_interpolate(_dptr(weights), _dptr(support), nq, group, k, _dptr(f), f.shape[0],
+                                      f.shape[1], centering_offset, _dptr(out), _stream_ptr()))
+    return out[:, 0] if one else out
+
+
+def cubic_segmentation(pts, approx_partition_size: int) -> dict:
+    """NAGA's nd_cubic_segmentation of a device point cloud [n][dim]: bounds,
+    width, shape and (device) partition sizes, offsets and indices."""
+    torch = _torch()
+    pts = pts.contiguous().float()
+    n, dim = pts.shape
+    lo = np.zeros(3, np.float32)
+    hi = np.zeros(3, np.float32)
+    w = C.c_float()
+    shape = np.zeros(3, np.int64)
+    _check(lib().naga_segmentation_shape(_dptr(pts), n, dim, approx_partition_size, _p(lo), _p(hi), C.byref(w),
+                                         _p(shape), _stream_ptr()))
+    cells = int(np.prod(shape[:dim]))
+    sizes = torch.empty(cells, dtype=torch.int32, device=pts.device)
+    offsets = torch.empty(cells, dtype=torch.int32, device=pts.device)
+    indices = torch.empty(n, dtype=torch.int32, device=pts.device)
+    _check(lib().naga_segmentation_build(_dptr(pts), n, dim, _p(lo), _p(hi), w.value, _p(shape), _dptr(sizes),
+                                         _dptr(offsets), _dptr(indices), _stream_ptr()))
+    return dict(lower=lo[:dim].copy(), upper=hi[:dim].copy(), width=w.value, shape=shape[:dim].copy(),
+                sizes=sizes, offsets=offsets, indices=indices)
 
 
 class profile:

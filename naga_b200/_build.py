@@ -16,7 +16,7 @@ CSRC = os.path.join(PKG, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libnaga_b200.so")
-SOURCES = ["errors.cpp", "scene_gen.cpp", "knn.cu", "linalg.cu", "rbf.cu", "step.cu", "engine.cu", "server.cu"]
+SOURCES = ["errors.cpp", "scene_gen.cpp", "knn.cu", "linalg.cu", "rbf.cu", "primitives.cu", "step.cu", "engine.cu", "server.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -476,6 +476,9 @@ __device__ __forceinline__ void write_node(const StencilOut& out, int64_t i, int
         if (out.W64)
 #pragma unroll
             for (int d = 0; d < D; ++d) out.W64[(i * k + t) * D + d] = Wt[d];
+        if (out.W32)
+#pragma unroll
+            for (int d = 0; d < D; ++d) out.W32[(i * k + t) * D + d] = (float)Wt[d];
         const int64_t at = out.npb > 0 ? pass_record(i, t, k, out.split, out.n_total, out.npb) : i * k + t;
         if (out.Wf) {
             const float fz = D == 3 ? (float)Wt[D - 1] : (float)(r == 0 ? fw0 : fw1);
@@ -484,6 +487,7 @@ __device__ __forceinline__ void write_node(const StencilOut& out, int64_t i, int
         if (out.Ff) out.Ff[at] = make_float2((float)(r == 0 ? fw0 : fw1), __uint_as_float(ns.jl[r]));
     }
     if (out.delta && lane == 0) out.delta[i] = ns.delta;
+    if (out.delta32 && lane == 0) out.delta32[i] = (float)ns.delta;
 }
 
 // Any k and both precisions: G0 column-major, factored by warp_lu, the D
@@ -938,39 +942,11 @@ extern "C" int naga_divergence_build(const float* pts, int64_t n, int dim, int k
     return divergence_build_device(pts, n, dim, k, shape, precision, idx, out, (cudaStream_t)stream);
 }
 
-namespace naga {
-namespace {
-template <int D>
-__global__ void divergence_apply_kernel(const float* __restrict__ W, const uint32_t* __restrict__ idx, int64_t n,
-                                        int k, const float* __restrict__ field, float* __restrict__ out) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        float acc = 0.f;
-        for (int s = 0; s < k; ++s) {
-            const uint32_t j = idx[i * k + s];
-            float t = 0.f;
-#pragma unroll
-            for (int d = 0; d < D; ++d) t = fmaf(W[(i * k + s) * D + d], field[(int64_t)j * D + d], t);
-            acc += t;
-        }
-        out[i] = acc;
-    }
-}
-}  // namespace
-}  // namespace naga
-
-// Generic gather of a vector field through a stored stencil (the default
-// path of divergence_operator::apply, nonlocal_calculus/divergence.cuh:377-488).
-extern "C" int naga_divergence_apply(const float* W, const uint32_t* idx, int64_t n, int dim, int k,
-                                     const float* field, float* result, void* stream) {
-    if (n < 0 || k < 1 || (dim != 2 && dim != 3)) return set_error(NAGA_EINVAL, "naga_divergence_apply: bad sizes");
-    if (n == 0) return NAGA_OK;
-    if (!W || !idx || !field || !result) return set_error(NAGA_EINVAL, "naga_divergence_apply: null pointer");
-    cudaStream_t st = (cudaStream_t)stream;
-    const int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)sm_count() * 8);
-    if (dim == 2)
-        divergence_apply_kernel<2><<<blocks, 256, 0, st>>>(W, idx, n, k, field, result);
-    else
-        divergence_apply_kernel<3><<<blocks, 256, 0, st>>>(W, idx, n, k, field, result);
-    NAGA_CUDA_TRY(cudaGetLastError());
-    return NAGA_OK;
+extern "C" int naga_divergence_build_f32(const float* pts, int64_t n, int dim, int k, int shape, int precision,
+                                         uint32_t* idx, float* W, float* delta, void* stream) {
+    if (!pts || !idx) return set_error(NAGA_EINVAL, "naga_divergence_build_f32: null pointer");
+    StencilOut out{};
+    out.W32 = W;
+    out.delta32 = delta;
+    return divergence_build_device(pts, n, dim, k, shape, precision, idx, out, (cudaStream_t)stream);
 }

@@ -108,6 +108,8 @@ namespace naga {
 struct StencilOut {
     double* W64;          // [n][k][D], FP64
     double* delta;        // [n]
+    float* W32;           // [n][k][D], FP32 (the C++ facade's divergence_operator<float, D>)
+    float* delta32;       // [n]
     float4* Wf;           // scene records [n][k]: (Wx, Wy, Wz | filter weight, index bits)
     float2* Ff;           // D == 3 filter records [n][k] (weight, index bits)
     double filter_sigma;  // Gaussian sigma of the selective filter (h / 2.5)

@@ -95,14 +95,16 @@ def test_scene_argument_validation_precedes_device(naga):
     assert e.value.code == naga.NAGA_EINVAL
 
 
-def test_cpp_facade_compiles():
+@pytest.mark.parametrize("name", sorted(f for f in os.listdir(os.path.join(ROOT, "tests", "cpp"))
+                                         if f.endswith(".cpp")))
+def test_cpp_facade_compiles(name):
     import shutil
     import subprocess
 
     gxx = shutil.which("g++-13") or shutil.which("g++")
-    src = os.path.join(ROOT, "tests", "cpp", "facade_pulse.cpp")
-    r = subprocess.run([gxx, "-std=c++17", "-fsyntax-only", f"-I{ROOT}/include", "-I/usr/local/cuda/include",
-                        src], capture_output=True, text=True)
+    src = os.path.join(ROOT, "tests", "cpp", name)
+    r = subprocess.run([gxx, "-std=c++17", "-fsyntax-only", "-Wall", f"-I{ROOT}/include",
+                        "-I/usr/local/cuda/include", src], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
 
 

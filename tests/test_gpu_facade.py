@@ -69,3 +69,55 @@ def test_facade_save_and_load_state(naga):
     """simulation_engine / density_observer save_state and load_state with a
     cereal-style archive: the restored engine continues bit for bit."""
     assert _run_program(naga, "facade_state").strip() == "ok"
+
+
+def test_facade_primitive_classes(naga, oracle):
+    """nd_cubic_segmentation, batched_nearest_neighbors(k, query_map,
+    segmentation), radial_point_method<float> and divergence_operator<T, 3>
+    (T = double and float) driven as NAGA's examples drive them
+    (tests/cpp/facade_primitives.cpp), against the oracle: the partition and
+    the neighbours bit for bit, weights and fields within FP32 / FP64
+    rounding."""
+    with tempfile.TemporaryDirectory() as out:
+        assert _run_program(naga, "facade_primitives", out).strip() == "ok"
+        rd = lambda name, dt: np.fromfile(os.path.join(out, name), dt)
+        seg_sizes, seg_idx = rd("seg_sizes.u32", np.uint32), rd("seg_indices.u32", np.uint32)
+        seg_meta = rd("seg_meta.f32", np.float32)
+        knn_idx, knn_d2 = rd("knn_idx.u32", np.uint32), rd("knn_d2.f32", np.float32)
+        w, vals = rd("rpim_weights.f32", np.float32), rd("rpim_values.f32", np.float32)
+        div64, div_idx = rd("div_f64.f64", np.float64), rd("div_idx.u32", np.uint32)
+        div32 = rd("div_f32_offset.f32", np.float32)
+
+    def grid(m, spacing, dt):
+        i = np.arange(m ** 3)
+        return np.stack([(i % m).astype(dt) * spacing, ((i // m) % m).astype(dt) * spacing,
+                         (i // (m * m)).astype(dt) * spacing], -1).astype(dt)
+
+    pi = np.float32(3.14159265358979)
+    m, mi = 24, 17
+    sp = np.float32(2) * pi / np.float32(m - 1)
+    isp = np.float32(2) * pi / np.float32(mi - 1)
+    src, qry = grid(m, sp, np.float32), grid(mi, isp, np.float32)
+    seg = oracle.cubic_segmentation(src, 32)
+    assert np.array_equal(seg_sizes, seg["sizes"]) and np.array_equal(seg_idx, seg["indices"])
+    assert seg_meta[0] == np.float32(seg["width"]) and np.array_equal(seg_meta[1:], seg["shape"])
+    oi, od = oracle.knn(src, qry, 32)
+    assert np.array_equal(knn_idx.reshape(oi.shape), oi) and np.array_equal(knn_d2.reshape(od.shape), od)
+    ow = oracle.rbf_weights(src, oi, qry.astype(np.float64), 1, float(sp), 0)
+    assert np.abs(w.reshape(ow.shape) - ow).max() <= 1e-6 * np.abs(ow).max()
+    S = src.astype(np.float64)
+    f = np.sin(S[:, 0]) * np.cos(S[:, 1]) * S[:, 2]
+    ref = np.einsum("qs,qs->q", ow, f[oi])
+    assert np.abs(vals - ref).max() <= 1e-5 * np.abs(f).max()
+
+    md = 20
+    dg = grid(md, 2 * np.pi / (md - 1), np.float64)
+    F = np.stack([np.sin(dg[:, 0]), 0 * dg[:, 0], np.cos(dg[:, 2])], -1)
+    di, dW, _ = oracle.divergence_stencil(dg.astype(np.float32), 32, 0)
+    assert np.array_equal(div_idx.reshape(di.shape), di)
+    ref64 = np.einsum("nsd,nsd->n", dW, F[di])
+    scale = np.abs(ref64).max()
+    assert np.abs(div64 - ref64).max() <= 1e-9 * scale
+    F32 = F.astype(np.float32).astype(np.float64)
+    ref32 = np.einsum("nsd,nsd->n", dW, F32[di] - 0.25)
+    assert np.abs(div32 - ref32).max() <= 2e-5 * scale

@@ -292,3 +292,146 @@ def test_inverse_register_sizes_singular_and_ties(naga, oracle, n):
     ok = [b for b in range(7) if b != 2]
     assert (info[ok] == 0).all()
     _assert_inverse_close(_np(out)[ok], ref[ok], A[ok])
+
+
+def _jittered_box(dim, m, L, seed=0):
+    rng = np.random.default_rng(seed)
+    g = np.stack(np.meshgrid(*[np.arange(m)] * dim, indexing="ij"), -1).reshape(-1, dim).astype(np.float64)
+    h = L / (m - 1)
+    pts = g * h + rng.uniform(-0.25 * h, 0.25 * h, g.shape)
+    return pts.astype(np.float32), h
+
+
+@pytest.mark.parametrize("dim,shape", [(2, 1), (3, 0)])
+def test_divergence_apply_matches_oracle_and_analytic_fields(naga, oracle, dim, shape):
+    """naga_divergence_apply (FP32) and naga_divergence_apply_f64 against the
+    FP64 oracle's stencil applied in FP64, on NAGA's known-answer field
+    (examples/nonlocal_divergence_3d.cu:40-51: F = (sin x, 0, cos z), div F =
+    cos x - sin z; 2-D: F = (sin x, cos y)) over a jittered grid of
+    [0, 2 pi]^dim; the FP32 stencil comes from naga_divergence_build_f32."""
+    L = 2 * np.pi
+    m = 16 if dim == 3 else 40
+    k = 32 if dim == 3 else 16
+    pts, h = _jittered_box(dim, m, L)
+    P = pts.astype(np.float64)
+    if dim == 3:
+        F = np.stack([np.sin(P[:, 0]), 0 * P[:, 0], np.cos(P[:, 2])], -1)
+        exact = np.cos(P[:, 0]) - np.sin(P[:, 2])
+    else:
+        F = np.stack([np.sin(P[:, 0]), np.cos(P[:, 1])], -1)
+        exact = np.cos(P[:, 0]) - np.sin(P[:, 1])
+    oi, oW, _ = oracle.divergence_stencil(pts, k, shape)
+    ref = np.einsum("nsd,nsd->n", oW, F[oi])
+    scale = np.abs(ref).max()
+    # FP32 stencil and FP32 apply
+    idx, W, delta = naga.divergence_build_f32(_t(pts), k, shape)
+    assert np.array_equal(_np(idx).view(np.uint32), oi)
+    assert np.abs(_np(W) - oW).max() <= 1e-6 * np.abs(oW).max()
+    got = _np(naga.divergence_apply(W, idx, _t(F.astype(np.float32))))
+    assert np.abs(got - ref).max() <= 2e-5 * scale
+    inner = np.all((P > 3 * h) & (P < L - 3 * h), axis=1)
+    err = np.linalg.norm(got[inner] - exact[inner]) / np.linalg.norm(exact[inner])
+    assert err < 0.08
+    # the oracle's FP64 stencil through the FP64 apply
+    got64 = _np(naga.divergence_apply(_t(oW), _t(oi.view(np.int32)), _t(F)))
+    assert np.abs(got64 - ref).max() <= 1e-12 * scale
+    # centring offset: apply(F, c) == apply(F - c)
+    c = 0.75
+    a = _np(naga.divergence_apply(_t(oW), _t(oi.view(np.int32)), _t(F), centering_offset=c))
+    b = _np(naga.divergence_apply(_t(oW), _t(oi.view(np.int32)), _t(F - c)))
+    assert np.abs(a - b).max() <= 1e-12 * scale
+    assert np.abs(a - np.einsum("nsd,nsd->n", oW, F[oi] - c)).max() <= 1e-12 * scale
+
+
+def test_divergence_apply_summation_order(naga):
+    """The FP32 apply sums the per-support terms by NAGA's pairwise tree
+    (divergence.cuh:452-468), not left to right: checked on values whose
+    FP32 sum depends on the order, k = 32 and k = 20."""
+    rng = np.random.default_rng(5)
+    for k in (32, 20):
+        n = 64
+        W = np.zeros((n, k, 3), np.float32)
+        W[:, :, 0] = rng.choice([1.0, 1e8, -1e8, 3.0], size=(n, k)).astype(np.float32)
+        idx = np.zeros((n, k), np.int32)
+        F = np.ones((1, 3), np.float32)
+        got = _np(naga.divergence_apply(_t(W), _t(idx), _t(F)))
+        t = W[:, :, 0].copy()
+        s = 1
+        while s < k:
+            for j in range(0, k, 2 * s):
+                if j + s < k:
+                    t[:, j] = t[:, j] + t[:, j + s]
+            s *= 2
+        assert np.array_equal(got, t[:, 0].astype(np.float32)), k
+
+
+def test_rbf_weights_f32_and_interpolate(naga, oracle):
+    """radial_point_method<float>: weights from FP32 queries, and interpolate
+    (one field and three components, with a centring offset) against the FP64
+    oracle, on NAGA's known-answer field (examples/
+    radial_point_interpolation_3d.cu:48-50: sin x cos y z over [0, 2 pi]^3)."""
+    L = 2 * np.pi
+    src, h = _jittered_box(3, 14, L, seed=3)
+    rng = np.random.default_rng(4)
+    qry = (rng.random((2000, 3)) * (L - 2 * h) + h).astype(np.float32)
+    sup, _ = naga.knn(_t(src), _t(qry), 32)
+    sup_np = _np(sup).view(np.uint32)
+    for shape in (0, 1):
+        w32 = naga.rbf_weights_f32(_t(src), sup, _t(qry), 1, h, shape)
+        ow = oracle.rbf_weights(src, sup_np, qry.astype(np.float64), 1, h, shape)
+        assert np.abs(_np(w32) - ow).max() <= 1e-6 * np.abs(ow).max()
+        S = src.astype(np.float64)
+        f = np.sin(S[:, 0]) * np.cos(S[:, 1]) * S[:, 2]
+        ref = np.einsum("qs,qs->q", ow, f[sup_np])
+        got = _np(naga.rbf_interpolate(w32, sup, _t(f.astype(np.float32))))
+        assert np.abs(got - ref).max() <= 1e-5 * np.abs(f).max()
+        Q = qry.astype(np.float64)
+        exact = np.sin(Q[:, 0]) * np.cos(Q[:, 1]) * Q[:, 2]
+        assert np.sqrt(np.mean((got - exact) ** 2)) < 0.05 * np.abs(exact).max()
+        F3 = np.stack([f, 2 * f, f + 1.0], -1)
+        got3 = _np(naga.rbf_interpolate(w32, sup, _t(F3.astype(np.float32)), centering_offset=1.0))
+        ref3 = np.einsum("qs,qsc->qc", ow, F3[sup_np] - 1.0) + 1.0
+        assert np.abs(got3 - ref3).max() <= 2e-5 * np.abs(F3).max()
+
+
+def test_rbf_interpolate_groups(naga, oracle):
+    """group_size > 1: queries q share the support list of group q / group."""
+    src, h = _jittered_box(2, 30, 1.0, seed=6)
+    rng = np.random.default_rng(7)
+    centres = (rng.random((50, 2)) * 0.8 + 0.1).astype(np.float32)
+    sup, _ = naga.knn(_t(src), _t(centres), 16)
+    qry = (np.repeat(centres, 4, 0) + rng.normal(0, 0.2 * h, (200, 2))).astype(np.float32)
+    w32 = naga.rbf_weights_f32(_t(src), sup, _t(qry), 4, h, 1)
+    sup_np = _np(sup).view(np.uint32)
+    ow = oracle.rbf_weights(src, sup_np, qry.astype(np.float64), 4, h, 1)
+    assert np.abs(_np(w32) - ow).max() <= 1e-6 * np.abs(ow).max()
+    f = src[:, 0].astype(np.float64) ** 2 - src[:, 1]
+    got = _np(naga.rbf_interpolate(w32, sup, _t(f.astype(np.float32)), group=4))
+    ref = np.einsum("qs,qs->q", ow, f[np.repeat(sup_np, 4, 0)])
+    assert np.abs(got - ref).max() <= 1e-5 * np.abs(f).max()
+
+
+def _seg_clouds():
+    rng = np.random.default_rng(8)
+    flat = rng.random((3000, 3)).astype(np.float32)
+    flat[:, 2] = 0.25  # a plane: the thin axis is widened to 1e-3
+    shifted = (rng.random((4000, 2)) * 7.0 - 3.0).astype(np.float32)
+    return [("grid3", _jittered_box(3, 20, 1.0, seed=9)[0], 32), ("rand2", shifted, 16),
+            ("flat3", flat, 32), ("one", shifted, 1), ("big", shifted, 1000),
+            ("single", shifted[:1].copy(), 8)]
+
+
+@pytest.mark.parametrize("case", range(6))
+def test_cubic_segmentation_matches_oracle(naga, oracle, case):
+    """NAGA's nd_cubic_segmentation on the device against its FP32
+    restatement on the CPU: bounds, width, shape, partition sizes, offsets
+    and the grouped indices, bit for bit."""
+    name, pts, approx = _seg_clouds()[case]
+    g = naga.cubic_segmentation(_t(pts), approx)
+    o = oracle.cubic_segmentation(pts, approx)
+    for key in ("lower", "upper", "shape"):
+        assert np.array_equal(g[key], o[key]), (name, key)
+    assert np.float32(g["width"]) == np.float32(o["width"]), name
+    assert np.array_equal(_np(g["sizes"]).view(np.uint32), o["sizes"]), name
+    assert np.array_equal(_np(g["offsets"]).view(np.uint32), o["offsets"]), name
+    assert np.array_equal(_np(g["indices"]).view(np.uint32), o["indices"]), name
