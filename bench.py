@@ -537,7 +537,7 @@ def run_naga(args, rank, world, local_rank):
 
     # ---- the probe error the throughput is quoted at (1000 steps against
     # the FP64 oracle; after the timed regions)
-    probe_error = probe_error_block(scene, g, drho) if args.n_side == 63 else None
+    probe_error = probe_error_block(scene, g, drho) if args.n_side == 63 and not args.no_probe_error else None
 
     # ---- batched form (every rank steps its size-balanced share of the
     # scenes; time = slowest rank) vs the plain single 2-D scene
@@ -620,6 +620,8 @@ def main():
     ap.add_argument("--target-step-ms", type=float, default=4.0,
                     help="per-step latency target of the second serving run")
     ap.add_argument("--no-setup", action="store_true")
+    ap.add_argument("--no-probe-error", action="store_true",
+                    help="skip the 1000-step probe-error check (profiling runs)")
     ap.add_argument("--setup-systems", type=int, default=1_000_000)
     ap.add_argument("--n-side", type=int, default=63,
                     help="grid nodes per side of the 3-D scene (63 = the benchmark workload; "

@@ -491,15 +491,20 @@ int naga_profile_read(int* count, const char** names, int64_t* launches,
                       double* ms);
 
 /* ---------------------------------------------------------- launch shapes */
-/* The gather kernels' resident blocks per SM are tuned once per batch
- * shape (lattice, stencil sizes, size class) the first time such a batch
- * steps: RK stage 1 is timed on the batch's own items for each candidate
- * (the driver's default shared-memory carveout, then 2 .. max blocks per
- * SM) and the fastest kept; NAGA_GATHER_BPS=<n> in the environment fixes
- * it instead. Results never depend on the shape. No NAGA counterpart (its
- * launch shapes are fixed by its runtime). Writes the tuner's log (one line
- * per tuned shape: candidates and microseconds per launch) into buf
- * (NUL-terminated, truncated to cap) and returns its full length.         */
+/* The launch shape of the gather kernels is tuned once per batch shape
+ * (lattice, stencil sizes, size class) the first time such a batch steps:
+ * RK stage 1 is timed on the batch's own items for every candidate pair of
+ * threads per node of the RK stages (D3Q27: 8, 7, 4; D2Q9: 2, 1 -- the
+ * first is the default, one float4 chunk of the row per thread) and
+ * resident blocks per SM (the driver's default shared-memory carveout,
+ * then 2 .. max), and the fastest kept; a shape other than the default must
+ * beat it by 3%. NAGA_GATHER_BPS=<n> and NAGA_GATHER_TPN=<t> in the
+ * environment fix it instead. Results never depend on the shape. Nodes per
+ * pass (32 in 3-D, 64 in 2-D) are fixed by the layout of the stencil tables
+ * at scene creation. No NAGA counterpart (its launch shapes are fixed by
+ * its runtime). Writes the tuner's log (one line per tuned shape:
+ * candidates and microseconds per launch) into buf (NUL-terminated,
+ * truncated to cap) and returns its full length.                          */
 int64_t naga_tuning_report(char* buf, int64_t cap);
 
 /* ------------------------------------------------------ failure detection */

@@ -1060,19 +1060,20 @@ __global__ void __launch_bounds__(MTF<L>::BLOCK) k_filter(const WorkItem* __rest
 // rounding). Boundary and ghost nodes keep zero rates, so
 // their stage values equal the step's start values, which the filter kernel
 // also wrote into the stage buffers G1 and G2.
-template <class L, int K, int STAGE>
-__global__ void __launch_bounds__(MTR<L>::BLOCK) k_rk(const WorkItem* __restrict__ items, int nitems,
-                                                      const SceneDev* __restrict__ scenes) {
-    using G = MTR<L>;
+// TPN_ threads per node: with fewer threads than gathered chunks a thread
+// serves chunks c, c + TPN_, ... (the tuner picks TPN_ per batch shape; the
+// arithmetic of a chunk, and so the result, does not depend on it)
+template <class L, int K, int STAGE, int TPN_ = MTR<L>::TPN>
+__global__ void __launch_bounds__(MT<L>::NPB * TPN_) k_rk(const WorkItem* __restrict__ items, int nitems,
+                                                          const SceneDev* __restrict__ scenes) {
+    using G = Shape<L, TPN_>;
     // D3Q27 tiles hold (Wx, Wy, Wz, index) records; D2Q9 tiles the
     // (Wx, Wy, index) triplets, three floats per record
     constexpr bool D2 = L::D == 2;
     using T = typename std::conditional<D2, float, float4>::type;
     constexpr int QP = L::QP, K_ = D2 ? 3 * K : K;
     using Src = typename std::conditional<D2, CompactSrc, StencilSrc>::type;
-    const int c = threadIdx.x % G::TPN, ns = threadIdx.x / G::TPN;
-    float d0[3], d1[3];
-    pair_dirs<L>(c < G::NCH ? c : 0, d0, d1);
+    const int c0 = threadIdx.x % G::TPN, ns = threadIdx.x / G::TPN;
     NAGA_PIPE_BEGIN(T, ((D2 ? 3 : 1) * tile_cap<G::NPB, K>()), Src{})
     const int k = K > 0 ? K : S.k;
     const int nn = (int)(it.end - it.begin);
@@ -1080,7 +1081,11 @@ __global__ void __launch_bounds__(MTR<L>::BLOCK) k_rk(const WorkItem* __restrict
     // chunks past NGATHER (D2Q9's rest population and pads) have zero rate:
     // their stage values equal g, G keeps them and no gather reads them
     // from the stage buffers
-    if (ns < nn && c < L::NGATHER) {
+    if (ns < nn) {
+#pragma unroll 1
+    for (int c = c0; c < L::NGATHER; c += G::TPN) {
+        float d0[3], d1[3];
+        pair_dirs<L>(c, d0, d1);
         // Horner stages: G1 = g + dt/4 A g, G2 = g + dt/3 A G1, G1 = g + dt/2 A G2,
         // G = g + dt A G1
         // (D2Q9's stage 1 gathers the filter's compact copy of G in G2;
@@ -1115,8 +1120,25 @@ __global__ void __launch_bounds__(MTR<L>::BLOCK) k_rk(const WorkItem* __restrict
         st4(dst, i, QDST, c, make_float4(fmaf(-a, r.x, f0.x), fmaf(-a, r.y, f0.y), fmaf(-a, r.z, f0.z),
                                         fmaf(-a, r.w, f0.w)));
     }
+    }
     NAGA_PIPE_END
 }
+
+// threads-per-node candidates of the RK stages: the default first (one
+// chunk per thread), then a shape without idle lanes (D3Q27: 7) and one with
+// two chunks per thread (D3Q27: 4, D2Q9: 1)
+template <class L>
+struct RkShapes;
+template <>
+struct RkShapes<D3Q27> {
+    static constexpr int n = 3;
+    static constexpr int tpn[3] = {8, 7, 4};
+};
+template <>
+struct RkShapes<D2Q9> {
+    static constexpr int n = 2;
+    static constexpr int tpn[2] = {2, 1};
+};
 
 // boundary: f = interp(f of bulk + layer) (simulation_engine.cuh:1370)
 template <class L, int KB>
@@ -1351,8 +1373,14 @@ struct ShapeKey {
         return std::tie(dim, k, kb, bucket) < std::tie(o.dim, o.k, o.kb, o.bucket);
     }
 };
+// the tuned launch shape of a batch shape: resident blocks per SM of the
+// gather kernels (0: default carveout) and threads per node of the RK
+// stages (0: the default, one chunk per thread)
+struct TunedShape {
+    int bps = 0, tpn = 0;
+};
 std::mutex g_shape_mu;
-std::map<ShapeKey, int> g_shape;  // tuned bps per batch shape
+std::map<ShapeKey, TunedShape> g_shape;
 std::string g_tune_log;
 
 int smem_per_sm() {
@@ -1388,37 +1416,65 @@ ShapeKey shape_key(int dim, int k, int kb, int n_items) {
     return {dim, k, kb, b};
 }
 
-int tuned_bps(const ShapeKey& key) {
+TunedShape tuned_shape(const ShapeKey& key) {
     std::lock_guard<std::mutex> lk(g_shape_mu);
     auto f = g_shape.find(key);
-    return f == g_shape.end() ? 0 : f->second;
+    return f == g_shape.end() ? TunedShape{} : f->second;
+}
+
+// fn(kernel, threads per node) with RK stage STAGE's instantiation for tpn
+// (the unrolled stencil sizes have every RkShapes candidate; the generic
+// K == 0 kernels only the default)
+template <class L, int K, int STAGE, class Fn>
+int rk_dispatch(int tpn, Fn&& fn) {
+    if constexpr (K > 0) {
+        if constexpr (L::D == 3) {
+            if (tpn == 7) return fn(k_rk<L, K, STAGE, 7>, 7);
+            if (tpn == 4) return fn(k_rk<L, K, STAGE, 4>, 4);
+        } else {
+            if (tpn == 1) return fn(k_rk<L, K, STAGE, 1>, 1);
+        }
+    }
+    return fn(k_rk<L, K, STAGE, MTR<L>::TPN>, MTR<L>::TPN);
+}
+template <class L, int K, class Fn>
+int rk_each_stage(int tpn, Fn&& fn) {
+    int rc;
+    if ((rc = rk_dispatch<L, K, 1>(tpn, fn)) || (rc = rk_dispatch<L, K, 2>(tpn, fn)) ||
+        (rc = rk_dispatch<L, K, 3>(tpn, fn)) || (rc = rk_dispatch<L, K, 4>(tpn, fn)))
+        return rc;
+    return NAGA_OK;
 }
 
 template <class L, int K, int KB>
 struct AppliedShape {
-    static int bps;  // carveout currently set on the instantiation's kernels (-2: unknown)
+    static int bps, tpn;  // shape currently set on the instantiation's kernels (-2: unknown)
 };
 template <class L, int K, int KB>
 int AppliedShape<L, K, KB>::bps = -2;
+template <class L, int K, int KB>
+int AppliedShape<L, K, KB>::tpn = -2;
 
 // carveout of every gather kernel of an instantiation (set only when the
 // shape changes)
 template <class L, int K, int KB>
-int apply_shape(int bps) {
+int apply_shape(const TunedShape& sh) {
     int& applied = AppliedShape<L, K, KB>::bps;
+    int& applied_tpn = AppliedShape<L, K, KB>::tpn;
     std::lock_guard<std::mutex> lk(g_shape_mu);
-    if (applied == bps) return NAGA_OK;
+    const int bps = sh.bps;
+    if (applied == bps && applied_tpn == sh.tpn) return NAGA_OK;
     using TF = float2;  // filter records
     const size_t s4 = tile_bytes<L, K, float4>(), s2 = tile_bytes<L, K, TF>(), sb = tile_bytes<L, KB, float2>();
     int rc;
     const int bo = other_bps<L>(bps);
-    if ((rc = set_blocks_per_sm(k_pml_gather<L, K>, s4, bps)) || (rc = set_blocks_per_sm(k_rk<L, K, 1>, s4, bps)) ||
-        (rc = set_blocks_per_sm(k_rk<L, K, 2>, s4, bps)) || (rc = set_blocks_per_sm(k_rk<L, K, 3>, s4, bps)) ||
-        (rc = set_blocks_per_sm(k_rk<L, K, 4>, s4, bps)) || (rc = set_blocks_per_sm(k_filter<L, K>, s2, bo)) ||
-        (rc = set_blocks_per_sm(k_edge_collide<L, KB>, sb, bo)) ||
+    if ((rc = set_blocks_per_sm(k_pml_gather<L, K>, s4, bps)) ||
+        (rc = rk_each_stage<L, K>(sh.tpn, [&](auto kern, int) { return set_blocks_per_sm(kern, s4, bps); })) ||
+        (rc = set_blocks_per_sm(k_filter<L, K>, s2, bo)) || (rc = set_blocks_per_sm(k_edge_collide<L, KB>, sb, bo)) ||
         (rc = set_blocks_per_sm(k_edge_interp<L, KB>, sb, bo)))
         return rc;
     applied = bps;
+    applied_tpn = sh.tpn;
     return NAGA_OK;
 }
 
@@ -1428,17 +1484,18 @@ int enqueue_step_k(const StepLaunch& P, cudaStream_t st) {
     using TF = float2;  // filter records
     const size_t s4 = tile_bytes<L, K, float4>(), s2 = tile_bytes<L, K, TF>(), sb = tile_bytes<L, KB, float2>();
     int rc;
-    if ((rc = allow_smem(k_pml_gather<L, K>, s4)) || (rc = allow_smem(k_rk<L, K, 1>, s4)) ||
-        (rc = allow_smem(k_rk<L, K, 2>, s4)) || (rc = allow_smem(k_rk<L, K, 3>, s4)) ||
-        (rc = allow_smem(k_rk<L, K, 4>, s4)) || (rc = allow_smem(k_filter<L, K>, s2)) ||
-        (rc = allow_smem(k_edge_collide<L, KB>, sb)) || (rc = allow_smem(k_edge_interp<L, KB>, sb)))
+    const TunedShape sh = tuned_shape(shape_key(L::D, K, KB, P.n_fluid));
+    if ((rc = allow_smem(k_pml_gather<L, K>, s4)) ||
+        (rc = rk_each_stage<L, K>(sh.tpn, [&](auto kern, int) { return allow_smem(kern, s4); })) ||
+        (rc = allow_smem(k_filter<L, K>, s2)) || (rc = allow_smem(k_edge_collide<L, KB>, sb)) ||
+        (rc = allow_smem(k_edge_interp<L, KB>, sb)))
         return rc;
     auto grid = [&](int n) { return n < cap ? n : cap; };
     // the pipelined gather kernels loop over their items: one wave of
     // resident blocks, bps per SM when the tuned shape fixes it
     const int sms = sm_count();
-    const int bps = tuned_bps(shape_key(L::D, K, KB, P.n_fluid));
-    if ((rc = apply_shape<L, K, KB>(bps))) return rc;
+    const int bps = sh.bps;
+    if ((rc = apply_shape<L, K, KB>(sh))) return rc;
     const int bo = other_bps<L>(bps);
     // the RK stages and the PML gather at their block size and bps, the
     // filter and boundary kernels at theirs and bo
@@ -1464,10 +1521,16 @@ int enqueue_step_k(const StepLaunch& P, cudaStream_t st) {
            (k_edge_collide<L, KB><<<pgrid(k_edge_collide<L, KB>, sb, P.n_edge), FB, sb, st>>>(P.edge, P.n_edge, P.scenes)));
     LAUNCH(K_FILTER, P.n_all_mt,
            (k_filter<L, K><<<pgrid(k_filter<L, K>, s2, P.n_all_mt), FB, s2, st>>>(P.all_mt, P.n_all_mt, P.scenes)));
-    LAUNCH(K_RK1, P.n_fluid, (k_rk<L, K, 1><<<pgrid_b(k_rk<L, K, 1>, s4, P.n_fluid, RB, bps), RB, s4, st>>>(P.fluid, P.n_fluid, P.scenes)));
-    LAUNCH(K_RK2, P.n_fluid, (k_rk<L, K, 2><<<pgrid_b(k_rk<L, K, 2>, s4, P.n_fluid, RB, bps), RB, s4, st>>>(P.fluid, P.n_fluid, P.scenes)));
-    LAUNCH(K_RK3, P.n_fluid, (k_rk<L, K, 3><<<pgrid_b(k_rk<L, K, 3>, s4, P.n_fluid, RB, bps), RB, s4, st>>>(P.fluid, P.n_fluid, P.scenes)));
-    LAUNCH(K_RK4, P.n_fluid, (k_rk<L, K, 4><<<pgrid_b(k_rk<L, K, 4>, s4, P.n_fluid, RB, bps), RB, s4, st>>>(P.fluid, P.n_fluid, P.scenes)));
+    // the RK stages at the tuned threads per node
+    auto rk_launch = [&](auto kern, int tpn) {
+        const int blk = MT<L>::NPB * tpn;
+        kern<<<pgrid_b(kern, s4, P.n_fluid, blk, bps), blk, s4, st>>>(P.fluid, P.n_fluid, P.scenes);
+        return NAGA_OK;
+    };
+    LAUNCH(K_RK1, P.n_fluid, (rk_dispatch<L, K, 1>(sh.tpn, rk_launch)));
+    LAUNCH(K_RK2, P.n_fluid, (rk_dispatch<L, K, 2>(sh.tpn, rk_launch)));
+    LAUNCH(K_RK3, P.n_fluid, (rk_dispatch<L, K, 3>(sh.tpn, rk_launch)));
+    LAUNCH(K_RK4, P.n_fluid, (rk_dispatch<L, K, 4>(sh.tpn, rk_launch)));
     LAUNCH(K_EDGE_INTERP, P.n_edge,
            (k_edge_interp<L, KB><<<pgrid(k_edge_interp<L, KB>, sb, P.n_edge), FB, sb, st>>>(P.edge, P.n_edge, P.scenes)));
 #undef LAUNCH
@@ -1475,12 +1538,15 @@ int enqueue_step_k(const StepLaunch& P, cudaStream_t st) {
     return NAGA_OK;
 }
 
-// Launch-shape tuner: times RK stage 1 (it reads G and overwrites only the
-// stage scratch G1, so it can run between steps) on the batch's own
-// items for each candidate -- the default carveout (0), then 2 .. max
-// resident blocks per SM -- and keeps the fastest (a fixed carveout only
-// when it beats the default by 3%). NAGA_GATHER_BPS=<n>
-// fixes the choice instead (0: default carveout).
+// Launch-shape tuner: times RK stage 1 (it reads G or its compact copy and
+// overwrites only the stage scratch G1, so it can run between steps) on the
+// batch's own items for each candidate shape -- threads per node of the RK
+// stages (RkShapes: the default first) times resident blocks per SM (the
+// default carveout 0, then 2 .. max) -- and keeps the fastest; a shape other
+// than the default (default threads per node, default carveout) must beat
+// the best default-shape time by 3%, since the carveout also binds the other
+// gather kernels. NAGA_GATHER_BPS=<n> and NAGA_GATHER_TPN=<t> fix the choice
+// instead (bps 0: default carveout; tpn 0 or unlisted: the default).
 template <class L, int K, int KB>
 int tune_k(const StepLaunch& P, cudaStream_t st) {
     if (P.n_fluid <= 0) return NAGA_OK;
@@ -1490,70 +1556,90 @@ int tune_k(const StepLaunch& P, cudaStream_t st) {
         if (g_shape.count(key)) return NAGA_OK;
     }
     const size_t s4 = tile_bytes<L, K, float4>();
-    int rc;
-    if ((rc = allow_smem(k_rk<L, K, 1>, s4))) return rc;
-    char line[160];
-    if (const char* env = std::getenv("NAGA_GATHER_BPS")) {
-        const int v = std::atoi(env);
+    int rc = NAGA_OK;
+    char line[200];
+    const char* env_bps = std::getenv("NAGA_GATHER_BPS");
+    const char* env_tpn = std::getenv("NAGA_GATHER_TPN");
+    if (env_bps || env_tpn) {
+        TunedShape sh;
+        sh.bps = env_bps ? std::max(0, std::atoi(env_bps)) : 0;
+        const int t = env_tpn ? std::atoi(env_tpn) : 0;
+        for (int c = 0; c < RkShapes<L>::n; ++c)
+            if (RkShapes<L>::tpn[c] == t && (K > 0 || c == 0)) sh.tpn = c == 0 ? 0 : t;
         std::lock_guard<std::mutex> lk(g_shape_mu);
-        g_shape[key] = v > 0 ? v : 0;
-        std::snprintf(line, sizeof line, "dim %d k %d kb %d items 2^%d: bps %d (NAGA_GATHER_BPS)\n", key.dim, key.k,
-                      key.kb, key.bucket, g_shape[key]);
+        g_shape[key] = sh;
+        std::snprintf(line, sizeof line, "dim %d k %d kb %d items 2^%d: tpn %d bps %d (NAGA_GATHER_BPS / _TPN)\n",
+                      key.dim, key.k, key.kb, key.bucket, sh.tpn ? sh.tpn : MTR<L>::TPN, sh.bps);
         g_tune_log += line;
         return NAGA_OK;
     }
-    if ((rc = set_blocks_per_sm(k_rk<L, K, 1>, s4, 0))) return rc;
-    int maxr = 0;
-    constexpr int RB = MTR<L>::BLOCK;
-    NAGA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxr, k_rk<L, K, 1>, RB, s4));
-    maxr = std::max(maxr, 1);
     const int sms = sm_count();
     cudaEvent_t e0, e1;
     NAGA_CUDA_TRY(cudaEventCreate(&e0));
     NAGA_CUDA_TRY(cudaEventCreate(&e1));
-    int best = -1;
-    float best_ms = 0.f;
+    TunedShape best;
+    float best_ms = -1.f, best_default_ms = -1.f;
     std::string log;
-    for (int bps = 0; bps <= maxr; bps = bps == 0 ? 2 : bps + 1) {
-        if ((rc = set_blocks_per_sm(k_rk<L, K, 1>, s4, bps))) break;
-        const int g = std::min(P.n_fluid, (bps > 0 ? bps : maxr) * sms);
-        // one untimed and one timed launch; launches shorter than ~0.4 ms
-        // are timed again over enough repetitions to span ~2 ms (a large
-        // batch costs two launches per candidate)
-        auto timed = [&](int reps, float* ms) -> bool {
-            cudaEventRecord(e0, st);
-            for (int r = 0; r < reps; ++r) k_rk<L, K, 1><<<g, RB, s4, st>>>(P.fluid, P.n_fluid, P.scenes);
-            cudaEventRecord(e1, st);
-            if (cudaEventSynchronize(e1) != cudaSuccess || cudaGetLastError() != cudaSuccess) return false;
-            cudaEventElapsedTime(ms, e0, e1);
-            *ms /= reps;
-            return true;
-        };
-        k_rk<L, K, 1><<<g, RB, s4, st>>>(P.fluid, P.n_fluid, P.scenes);
-        float ms = 0.f;
-        bool ok = timed(1, &ms);
-        if (ok && ms < 0.4f) ok = timed(std::min(8, std::max(2, (int)(2.f / std::max(ms, 1e-3f)))), &ms);
-        if (!ok) {
-            rc = set_error(NAGA_ECUDA, "launch-shape tuning: a trial launch failed");
-            break;
-        }
-        std::snprintf(line, sizeof line, " %d:%.1fus", bps, ms * 1000.f);
-        log += line;
-        // a fixed carveout must beat the default by 3% to be kept: it also
-        // binds the other gather kernels, whose best split may differ
-        if (best < 0 || ms < best_ms * (best == 0 ? 0.97f : 1.f)) {
-            best = bps;
-            best_ms = ms;
-        }
+    const int ncand = K > 0 ? RkShapes<L>::n : 1;
+    for (int ci = 0; ci < ncand && rc == NAGA_OK; ++ci) {
+        const int tpn = ci == 0 ? 0 : RkShapes<L>::tpn[ci];
+        rc = rk_dispatch<L, K, 1>(tpn, [&](auto kern, int t) -> int {
+            const int blk = MT<L>::NPB * t;
+            int r;
+            if ((r = allow_smem(kern, s4)) || (r = set_blocks_per_sm(kern, s4, 0))) return r;
+            int maxr = 0;
+            NAGA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxr, kern, blk, s4));
+            maxr = std::max(maxr, 1);
+            std::snprintf(line, sizeof line, " | tpn %d", t);
+            log += line;
+            for (int bps = 0; bps <= maxr; bps = bps == 0 ? 2 : bps + 1) {
+                if ((r = set_blocks_per_sm(kern, s4, bps))) return r;
+                const int g = std::min(P.n_fluid, (bps > 0 ? bps : maxr) * sms);
+                // one untimed and one timed launch; launches shorter than
+                // ~0.4 ms are timed again over enough repetitions to span ~2 ms
+                auto timed = [&](int reps, float* ms) -> bool {
+                    cudaEventRecord(e0, st);
+                    for (int q = 0; q < reps; ++q) kern<<<g, blk, s4, st>>>(P.fluid, P.n_fluid, P.scenes);
+                    cudaEventRecord(e1, st);
+                    if (cudaEventSynchronize(e1) != cudaSuccess || cudaGetLastError() != cudaSuccess) return false;
+                    cudaEventElapsedTime(ms, e0, e1);
+                    *ms /= reps;
+                    return true;
+                };
+                kern<<<g, blk, s4, st>>>(P.fluid, P.n_fluid, P.scenes);
+                float ms = 0.f, ms2 = 0.f;
+                bool ok = timed(1, &ms);
+                if (ok && ms < 0.4f) ok = timed(std::min(8, std::max(2, (int)(2.f / std::max(ms, 1e-3f)))), &ms);
+                // twice, the faster kept: other streams' work (a server's
+                // scene set-up) can slow a single trial
+                const int reps2 = ms < 0.4f ? std::min(8, std::max(2, (int)(2.f / std::max(ms, 1e-3f)))) : 1;
+                if (ok && timed(reps2, &ms2)) ms = std::min(ms, ms2);
+                if (!ok) return set_error(NAGA_ECUDA, "launch-shape tuning: a trial launch failed");
+                std::snprintf(line, sizeof line, " %d:%.1fus", bps, ms * 1000.f);
+                log += line;
+                const bool is_default = tpn == 0 && bps == 0;
+                if (is_default) best_default_ms = ms;
+                if (best_ms < 0.f || ms < best_ms) {
+                    best.bps = bps;
+                    best.tpn = tpn;
+                    best_ms = ms;
+                }
+            }
+            // the trials changed this kernel's carveout
+            return set_blocks_per_sm(kern, s4, 0);
+        });
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    AppliedShape<L, K, KB>::bps = -2;  // the trials changed rk stage 1's carveout
+    AppliedShape<L, K, KB>::bps = -2;  // the trials changed rk stage 1's carveouts
+    AppliedShape<L, K, KB>::tpn = -2;
     if (rc) return rc;
+    // a non-default shape must beat the default by 3%
+    if (best_default_ms > 0.f && (best.bps != 0 || best.tpn != 0) && best_ms > 0.97f * best_default_ms) best = {};
     std::lock_guard<std::mutex> lk(g_shape_mu);
-    g_shape[key] = best < 0 ? 0 : best;
-    std::snprintf(line, sizeof line, "dim %d k %d kb %d items 2^%d: bps %d of", key.dim, key.k, key.kb, key.bucket,
-                  g_shape[key]);
+    g_shape[key] = best;
+    std::snprintf(line, sizeof line, "dim %d k %d kb %d items 2^%d: tpn %d bps %d of", key.dim, key.k, key.kb,
+                  key.bucket, best.tpn ? best.tpn : MTR<L>::TPN, best.bps);
     g_tune_log += line + log + "\n";
     return NAGA_OK;
 }

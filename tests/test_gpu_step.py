@@ -176,18 +176,24 @@ _SHAPE_RUN = """
 import sys, numpy as np
 sys.path.insert(0, {root!r})
 import naga_b200 as naga
-g = naga.generate_grid(3, 20, 3, 4)
-s = naga.Scene(g, k=32, shape=0, probes=np.array({probes!r}, np.float32))
-s.set_density(naga.gaussian_pulse(g["points"], [0.5] * 3, 1e-3, 0.05))
-s.step(15)
-np.save({out!r}, np.concatenate([s.state()[0].ravel(), s.probes().ravel()]))
+out = []
+for dim, n, k in ((3, 20, 32), (2, 48, 16)):
+    g = naga.generate_grid(dim, n, 3, 4)
+    pr = np.array({probes3!r} if dim == 3 else {probes2!r}, np.float32)
+    s = naga.Scene(g, k=k, shape=0 if dim == 3 else 1, probes=pr)
+    s.set_density(naga.gaussian_pulse(g["points"], [0.5] * dim, 1e-3, 0.05))
+    s.step(15)
+    out += [s.state()[0].ravel(), s.probes().ravel()]
+np.save({out!r}, np.concatenate(out))
 print(naga.tuning_report())
 """
 
 
 def test_launch_shape_does_not_change_results(tmp_path):
-    """The tuner's choice of resident blocks per SM changes only the grid:
-    a run with the tuned shape and one forced to 2 blocks per SM agree bit
+    """The tuner's choices -- resident blocks per SM of the gather kernels and
+    threads per node of the RK stages -- change only the launch: runs with
+    the tuned shape and with shapes forced through NAGA_GATHER_BPS /
+    NAGA_GATHER_TPN (D3Q27 at 7 and 4 threads per node, D2Q9 at 1) agree bit
     for bit, and the tuner logs what it measured."""
     import os
     import subprocess
@@ -195,20 +201,28 @@ def test_launch_shape_does_not_change_results(tmp_path):
 
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     outs, logs = [], []
-    for env_bps in (None, "2"):
-        out = str(tmp_path / f"run_{env_bps}.npy")
+    for env_bps, env_tpn in ((None, None), ("2", None), (None, "7"), ("3", "4"), (None, "1")):
+        out = str(tmp_path / f"run_{env_bps}_{env_tpn}.npy")
         env = dict(os.environ)
         env.pop("NAGA_GATHER_BPS", None)
+        env.pop("NAGA_GATHER_TPN", None)
         if env_bps:
             env["NAGA_GATHER_BPS"] = env_bps
-        code = _SHAPE_RUN.format(root=root, probes=PROBES3.tolist(), out=out)
+        if env_tpn:
+            env["NAGA_GATHER_TPN"] = env_tpn
+        code = _SHAPE_RUN.format(root=root, probes3=PROBES3.tolist(), probes2=PROBES2.tolist(), out=out)
         r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=300)
         assert r.returncode == 0, r.stderr
         outs.append(np.load(out))
         logs.append(r.stdout)
-    assert np.array_equal(outs[0], outs[1])
-    assert "dim 3 k 32 kb 32" in logs[0] and " 0:" in logs[0]
-    assert "bps 2 (NAGA_GATHER_BPS)" in logs[1]
+    for o in outs[1:]:
+        assert np.array_equal(outs[0], o)
+    assert "dim 3 k 32 kb 32" in logs[0] and "| tpn 8 0:" in logs[0] and "| tpn 7" in logs[0]
+    assert "dim 2 k 16 kb 16" in logs[0] and "| tpn 1" in logs[0]
+    assert "tpn 8 bps 2 (NAGA_GATHER_BPS" in logs[1]
+    assert "dim 3 k 32 kb 32 items 2^" in logs[2] and "tpn 7 bps 0 (NAGA_GATHER" in logs[2]
+    assert "tpn 4 bps 3 (NAGA_GATHER" in logs[3]
+    assert "dim 2 k 16 kb 16 items 2^" in logs[4] and "tpn 1 bps 0 (NAGA_GATHER" in logs[4]
 
 
 def test_async_probe_reads_match_synchronous(naga, oracle):
