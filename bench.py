@@ -84,27 +84,48 @@ def build_batched(naga, specs):
 # ------------------------------------------------------- algorithmic bytes
 def kernel_bytes(dim, N, nb, nl, nbd, k, kb):
     """Compulsory HBM bytes per launch of each step kernel (FP32 values, u32
-    indices; rows of Q populations; neighbour rows counted once)."""
+    indices; rows of Q populations; neighbour rows counted once). The RK
+    stages and the PML gather touch only the populations with a streaming
+    rate: all 27 in D3Q27, the 8 moving ones of D2Q9 (its rest population's
+    rate is zero)."""
     Q = 9 if dim == 2 else 27
     row = 4 * Q
+    grow = 4 * 8 if dim == 2 else row  # the gathered part of a row
     st = 4 * k * (dim + 1)  # weights + index per neighbour
     nbl = nb + nl
     return {
         # G, Q1_prev in; Q1, S1 out (+ S1P on sources, not counted); M in/out;
         # the PML field rows of the layer out
-        "macro_pml": N * (4 * row + 32) + nl * row,
+        "macro_pml": N * (4 * row + 32) + nl * grow,
         # stencil + S1 read/write + PV per node, the layer's field rows once
-        "pml_gather": nbl * (st + 2 * row + 32) + nl * row,
+        "pml_gather": nbl * (st + 2 * grow + 32) + nl * grow,
         "edge_collide": nbd * (2 * row + 8 * kb),
         "filter": N * 2 * row + nbl * 8 * k,
         # Horner RK4: stencil, the stage rows gathered (counted once), the
         # node's own start row in, the stage row out
-        "rk_stage1": nbl * (st + 2 * row),
-        "rk_stage2": nbl * (st + 3 * row),
-        "rk_stage3": nbl * (st + 3 * row),
-        "rk_stage4": nbl * (st + 3 * row),
+        "rk_stage1": nbl * (st + 2 * grow),
+        "rk_stage2": nbl * (st + 3 * grow),
+        "rk_stage3": nbl * (st + 3 * grow),
+        "rk_stage4": nbl * (st + 3 * grow),
         "edge_interp": nbd * (8 * kb + row),
     }
+
+
+def batch_roofline(scenes, prof, steps, peak):
+    """Roofline of the batch's longest step kernel: its algorithmic bytes
+    summed over the member scenes per launch, over its mean launch time."""
+    tot = {}
+    for sc in scenes:
+        d = sc.desc
+        for name, b in kernel_bytes(sc.dim, sc.N, d.n_bulk, d.n_layer, d.n_boundary, d.k, d.k_boundary).items():
+            tot[name] = tot.get(name, 0) + b
+    top = max(tot, key=lambda n: prof.get(n, (0, 0.0))[1])
+    launches, ms = prof[top]
+    achieved = tot[top] / (ms / launches * 1e-3) / 1e9
+    return {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "algorithmic_bytes_per_launch": tot[top], "avg_launch_ms": ms / launches,
+            "kernel_fracs": {n: round(tot[n] / (prof[n][1] / prof[n][0] * 1e-3) / 1e9 / peak, 3)
+                             for n in tot if prof.get(n, (0, 0.0))[0]}}
 
 
 # ------------------------------------------------------------- clocks
@@ -281,6 +302,15 @@ def probe_error_block(scene, g, drho):
             "against": "FP64 CPU oracle trace of the same scene (tests/golden/trace_d3q27_63.npz)"}
 
 
+def measured_hbm_peak():
+    """(GB/s, source): MEASURED_PEAKS.json's copy bandwidth, else the pool's
+    earlier measurement."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        return float(json.load(open(path))["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
 # ------------------------------------------------------------ extra blocks
 def batched_block(naga, torch, args, rank, world, dist, W, K):
     """256 D2Q9 scenes stepped as one batch (one launch per kernel, CUDA
@@ -306,15 +336,17 @@ def batched_block(naga, torch, args, rank, world, dist, W, K):
     p99 = replicas.max_over_ranks(float(np.percentile(b_per, 99)), dist, "cuda")
     bm = nodes * K / (b_ms * 1e-3) / 1e6
     # per-kernel device time of this rank's batch step (event-bracketed
-    # launches, after the timed region)
+    # launches, after the timed region) and the roofline of its top kernel
     prof = profile_kernels(naga, lambda: b.step(1))
+    roof = batch_roofline(scenes, prof, 5, measured_hbm_peak()[0])
     b.close()
     for s in scenes:
         s.close()
     return {"scenes": len(specs), "nodes": nodes, "mnups": bm, "plain_2d_mnups": plain_mnups,
             "ratio_vs_plain": bm / plain_mnups, "p50_step_ms": float(np.percentile(b_per, 50)),
             "p99_step_ms": p99, "sharding": f"{world} rank(s), size-balanced",
-            "kernel_ms_rank0": {n: round(t / 5, 4) for n, (l, t) in prof.items() if l}}
+            "kernel_ms_rank0": {n: round(t / 5, 4) for n, (l, t) in prof.items() if l},
+            "roofline_rank0": roof}
 
 
 def serving_block(naga, torch, args, rank, world, dist, step_priority=0, target_step_ms=0.0, seconds=None):
@@ -566,9 +598,7 @@ def run_naga(args, rank, world, local_rank):
     step_ms = sum(ms for (_, ms) in prof.values()) / 5
     top = max(kb, key=lambda n: prof.get(n, (0, 0.0))[1])
     launches, tot = prof[top]
-    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
-        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
-    peak = peaks.get("hbm_gbs", 6650.0)
+    peak, peak_source = measured_hbm_peak()
     achieved = kb[top] / (tot / launches * 1e-3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
@@ -576,9 +606,13 @@ def run_naga(args, rank, world, local_rank):
         traffic = json.load(open(tpath)).get(top)
     roof = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": traffic,
-            "peak_source": "measured" if peaks else "fallback",
+            "peak_source": peak_source,
             "algorithmic_bytes_per_launch": kb[top], "avg_launch_ms": tot / launches,
-            "kernel_share": {n: round(prof[n][1] / 5 / step_ms, 4) for n in prof if prof[n][0]}}
+            "kernel_share": {n: round(prof[n][1] / 5 / step_ms, 4) for n in prof if prof[n][0]},
+            # every step kernel's algorithmic bytes / its launch time / peak
+            "kernel_fracs": {n: round(kb[n] / (prof[n][1] / prof[n][0] * 1e-3) / 1e9 / peak, 3)
+                             for n in kb if prof.get(n, (0, 0.0))[0]},
+            "step_frac": sum(kb.values()) / (step_ms * 1e-3) / 1e9 / peak}
     gpu_launches = sum(l for (l, _) in prof.values()) // 5 * K
 
     cb = None

@@ -11,11 +11,17 @@
 //     simulation_observer.cuh:41-55                simulation_observer<Lattice>
 //     simulation_observers/density_observer.cuh    density_observer<Lattice>
 //     d2q9_lattice.cuh / d3q27_lattice.cuh         d2q9_lattice<T>, d3q27_lattice<T>
+//   segmentation/nd_cubic_segmentation.cuh       naga::segmentation::nd_cubic_segmentation<T, D>
 //   segmentation/nearest_neighbors.cuh:444-477   naga::segmentation::batched_nearest_neighbors
+//   interpolation/radial_point_method.cuh        naga::interpolation::radial_point_method<T>
+//   nonlocal_calculus/divergence.cuh, operators.cuh
+//                                                naga::nonlocal_calculus::divergence_operator<T, D>,
+//                                                operator_builder<T, D>
 //   linalg/batched_matrix_inverse.cuh:389-397    naga::linalg::batched_matrix_inverse
 //
-// Differences a caller sees: arrays are std::vector on the host (NAGA used
-// its unified-memory sclx::array); the engine owns device state; errors
+// Differences a caller sees: the engine's arrays are std::vector on the host
+// and the primitives' are naga::device_array (NAGA used its unified-memory
+// sclx::array for both); the engine owns device state; errors
 // from the C ABI are rethrown as std::invalid_argument (bad arguments) or
 // std::runtime_error (everything else), the exception types NAGA throws.
 #pragma once
@@ -1034,6 +1040,25 @@ class divergence_operator {
     device_array<T> weights_;
     device_array<uint32_t> support_indices_;
     size_t k_ = 0, rows_ = 0;
+};
+// NAGA's operator_builder<T, D> (nonlocal_calculus/operators.cuh:43-166):
+// holds the domain (and query points) and creates an operator over them,
+// builder.create<divergence_operator>() as in NAGA's examples
+// (examples/nonlocal_divergence_3d.cu:110-113). The query points must be
+// the domain, as for divergence_operator::create.
+template <class T, unsigned D>
+class operator_builder {
+  public:
+    explicit operator_builder(const device_array<const T>& domain) : domain_(domain), query_(domain) {}
+    operator_builder(const device_array<const T>& domain, const device_array<const T>& query_points)
+        : domain_(domain), query_(query_points) {}
+    template <template <class, unsigned> class Operator>
+    Operator<T, D> create(int k = 32, int shape = 0, int precision = 0, cudaStream_t stream = nullptr) const {
+        return Operator<T, D>::create(domain_, query_, 0, k, shape, precision, stream);
+    }
+
+  private:
+    device_array<const T> domain_, query_;
 };
 }  // namespace nonlocal_calculus
 

@@ -107,6 +107,12 @@ int main(int argc, char** argv) {
     divergence.apply(values_d, div_d);
     dump(dir, "div_f64.f64", div_d.to_host());
     dump(dir, "div_idx.u32", divergence.support_indices().to_host());
+    // the same operator through operator_builder, as NAGA's example builds it
+    naga::nonlocal_calculus::operator_builder<double, 3> builder(source_d);
+    auto built = builder.create<naga::nonlocal_calculus::divergence_operator>();
+    naga::device_array<double> div_b(md * md * md);
+    built.apply(values_d, div_b);
+    if (div_b.to_host() != div_d.to_host()) return 10;
 
     std::vector<float> fgrid(dgrid.begin(), dgrid.end()), fvals(dvals.begin(), dvals.end());
     auto source_f = naga::device_array<float>::from_host(fgrid);
