@@ -82,7 +82,22 @@ def build_batched(naga, specs):
 
 
 # ------------------------------------------------------- algorithmic bytes
-def kernel_bytes(dim, N, nb, nl, nbd, k, kb):
+def pml_counts(naga, scene):
+    """(nodes the PML gather visits, layer-support records they hold): a
+    bulk or layer node is visited when a stencil support lies in the
+    absorbing layer, and its tile holds those supports' records."""
+    import ctypes as C
+
+    d = scene.desc
+    nbl = d.n_bulk + d.n_layer
+    idx = np.zeros((scene.N, d.k), np.uint32)
+    naga._check(naga.lib().naga_scene_read_tables(scene.h, idx.ctypes.data_as(C.c_void_p), *([None] * 6)))
+    sup = idx[:nbl]
+    cnt = ((sup >= d.n_bulk) & (sup < nbl)).sum(1)
+    return int((cnt > 0).sum()), int(cnt.sum())
+
+
+def kernel_bytes(dim, N, nb, nl, nbd, k, kb, pml=None):
     """Compulsory HBM bytes per launch of each step kernel (FP32 values, u32
     indices; rows of Q populations; neighbour rows counted once). The RK
     stages and the PML gather touch only the populations with a streaming
@@ -97,8 +112,11 @@ def kernel_bytes(dim, N, nb, nl, nbd, k, kb):
         # G, Q1_prev in; Q1, S1 out (+ S1P on sources, not counted); M in/out;
         # the PML field rows of the layer out
         "macro_pml": N * (4 * row + 32) + nl * grow,
-        # stencil + S1 read/write + PV per node, the layer's field rows once
-        "pml_gather": nbl * (st + 2 * grow + 32) + nl * grow,
+        # per visited node its layer supports' records (16 B), S1 read and
+        # write, PV; the layer's field rows once (pml = (visited nodes,
+        # records), from pml_counts; without it every fluid node and its
+        # whole stencil, an upper bound)
+        "pml_gather": ((pml[1] * 16 + pml[0] * (2 * grow + 32)) if pml else nbl * (st + 2 * grow + 32)) + nl * grow,
         "edge_collide": nbd * (2 * row + 8 * kb),
         "filter": N * 2 * row + nbl * 8 * k,
         # Horner RK4: stencil, the stage rows gathered (counted once), the
@@ -111,13 +129,14 @@ def kernel_bytes(dim, N, nb, nl, nbd, k, kb):
     }
 
 
-def batch_roofline(scenes, prof, steps, peak):
+def batch_roofline(naga, scenes, prof, peak):
     """Roofline of the batch's longest step kernel: its algorithmic bytes
     summed over the member scenes per launch, over its mean launch time."""
     tot = {}
     for sc in scenes:
         d = sc.desc
-        for name, b in kernel_bytes(sc.dim, sc.N, d.n_bulk, d.n_layer, d.n_boundary, d.k, d.k_boundary).items():
+        for name, b in kernel_bytes(sc.dim, sc.N, d.n_bulk, d.n_layer, d.n_boundary, d.k, d.k_boundary,
+                                    pml_counts(naga, sc)).items():
             tot[name] = tot.get(name, 0) + b
     top = max(tot, key=lambda n: prof.get(n, (0, 0.0))[1])
     launches, ms = prof[top]
@@ -338,7 +357,7 @@ def batched_block(naga, torch, args, rank, world, dist, W, K):
     # per-kernel device time of this rank's batch step (event-bracketed
     # launches, after the timed region) and the roofline of its top kernel
     prof = profile_kernels(naga, lambda: b.step(1))
-    roof = batch_roofline(scenes, prof, 5, measured_hbm_peak()[0])
+    roof = batch_roofline(naga, scenes, prof, measured_hbm_peak()[0])
     b.close()
     for s in scenes:
         s.close()
@@ -594,7 +613,7 @@ def run_naga(args, rank, world, local_rank):
 
     # ---- per-kernel timing (CUDA events around each launch, separate run)
     prof = profile_kernels(naga, lambda: scene.step(1), steps=5)
-    kb = kernel_bytes(3, N, g["n_bulk"], g["n_layer"], g["n_boundary"], cfg["k"], cfg["k"])
+    kb = kernel_bytes(3, N, g["n_bulk"], g["n_layer"], g["n_boundary"], cfg["k"], cfg["k"], pml_counts(naga, scene))
     step_ms = sum(ms for (_, ms) in prof.values()) / 5
     top = max(kb, key=lambda n: prof.get(n, (0, 0.0))[1])
     launches, tot = prof[top]
