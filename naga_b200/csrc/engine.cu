@@ -815,21 +815,18 @@ extern "C" void* naga_scene_stream(naga_scene* s) { return s ? (void*)active_str
 extern "C" int naga_scene_set_density(naga_scene* s, const float* drho) {
     if (!s) return set_error(NAGA_EINVAL, "naga_scene_set_density: null scene");
     cudaStream_t st = active_stream(s);
-    NAGA_CUDA_TRY(cudaStreamSynchronize(st));
     const int QP = s->QP;
     SceneDev& V = s->dev;
-    // upload the N densities and expand them to population rows on the device
+    // upload the N densities into the collision scratch S1 (N QP floats; the
+    // next step's node-local kernel rewrites all of it before any read) and
+    // expand them to population rows on the device: no allocation, and the
+    // work is ordered on the scene's stream behind any steps still queued
     float* d = nullptr;
     if (drho) {
-        NAGA_CUDA_TRY(cudaMallocAsync(&d, sizeof(float) * std::max<int64_t>(s->N, 1), st));
-        cudaError_t e = cudaMemcpyAsync(d, drho, sizeof(float) * s->N, cudaMemcpyHostToDevice, st);
-        if (e != cudaSuccess) {
-            cudaFreeAsync(d, st);
-            return set_error(NAGA_ECUDA, std::string("naga_scene_set_density: ") + cudaGetErrorString(e));
-        }
+        d = V.S1;
+        NAGA_CUDA_TRY(cudaMemcpyAsync(d, drho, sizeof(float) * s->N, cudaMemcpyHostToDevice, st));
     }
     int rc = density_rows_device(s->dim, d, s->N, V.G, st);
-    if (d) cudaFreeAsync(d, st);
     if (rc) return rc;
     NAGA_CUDA_TRY(cudaMemsetAsync(V.M, 0, sizeof(float4) * s->N, st));
     NAGA_CUDA_TRY(cudaMemsetAsync(V.Q1a, 0, sizeof(float) * s->N * QP, st));

@@ -85,7 +85,11 @@ struct Shape {
 template <class L>
 using MTR = Shape<L, L::D == 3 ? 8 : L::NGATHER>;  // RK stages, PML gather
 template <class L>
-using MTF = Shape<L, L::D == 3 ? 8 : L::QP / 4>;   // filter, boundary kernels
+using MTF = Shape<L, L::D == 3 ? 8 : L::QP / 4>;   // boundary kernels
+// the filter: D2Q9 at two threads per node, thread 0 also filtering the
+// rest population (a scalar of the same row), so no lane works on pads
+template <class L>
+using MTFF = Shape<L, L::D == 3 ? 8 : L::NGATHER>;
 
 // blocks per SM of the MTF-shaped kernels for the RK stages' tuned bps: the
 // same threads per SM
@@ -983,9 +987,11 @@ __global__ void __launch_bounds__(MTF<L>::BLOCK, 5) k_edge_collide(const WorkIte
 // 1233-1323); boundary: bounce-back f_a <- f_bb(a) where c_a . n > 0
 // (:789-944), a swap within each opposite pair; ghost: copy
 template <class L, int K>
-__global__ void __launch_bounds__(MTF<L>::BLOCK) k_filter(const WorkItem* __restrict__ items, int nitems,
-                                                          const SceneDev* __restrict__ scenes) {
-    using G = MTF<L>;
+__global__ void __launch_bounds__(MTFF<L>::BLOCK) k_filter(const WorkItem* __restrict__ items, int nitems,
+                                                           const SceneDev* __restrict__ scenes) {
+    using G = MTFF<L>;
+    // D2Q9: slot of the rest population (chunk NGATHER, first float)
+    constexpr int REST = 4 * L::NGATHER;
     constexpr int QP = L::QP, K_ = K;
     // (weight, index) filter records, 8 B each
     using T = float2;
@@ -999,20 +1005,28 @@ __global__ void __launch_bounds__(MTF<L>::BLOCK) k_filter(const WorkItem* __rest
     const int64_t i = (int64_t)it.begin + ns;
     if (ns < nn && c < G::NCH) {
         const float4 f = ld4rw(S.S1, i, QP, c);
+        // D2Q9 thread 0 also carries the rest population
+        const bool rest = L::D == 2 && c == 0;
+        const float fr = rest ? S.S1[i * QP + REST] : 0.f;
+        float outr = fr;
         float4 out;
         if (i < S.nbl) {
             float4 sum = make_float4(0.f, 0.f, 0.f, 0.f);
+            float sumr = 0.f;
 #pragma unroll 8
             for (int s = 0; s < k; ++s) {
                 const float2 r = tile[s * nn + ns];
-                const float4 v = ld4g<L>(S.S1, __float_as_uint(r.y), c);
+                const uint32_t j = __float_as_uint(r.y);
+                const float4 v = ld4g<L>(S.S1, j, c);
                 sum.x = fmaf(r.x, v.x - f.x, sum.x);
                 sum.y = fmaf(r.x, v.y - f.y, sum.y);
                 sum.z = fmaf(r.x, v.z - f.z, sum.z);
                 sum.w = fmaf(r.x, v.w - f.w, sum.w);
+                if (rest) sumr = fmaf(r.x, __ldg(S.S1 + (int64_t)j * QP + REST) - fr, sumr);
             }
             out = make_float4(fmaf(0.75f, sum.x, f.x), fmaf(0.75f, sum.y, f.y), fmaf(0.75f, sum.z, f.z),
                               fmaf(0.75f, sum.w, f.w));
+            outr = fmaf(0.75f, sumr, fr);
         } else if (i - S.nbl < S.nbd) {
             const int64_t b = i - S.nbl;
             float n[3] = {0.f, 0.f, 0.f};
@@ -1029,6 +1043,10 @@ __global__ void __launch_bounds__(MTF<L>::BLOCK) k_filter(const WorkItem* __rest
             out = f;
         }
         st4(S.G, i, QP, c, out);
+        // the rest population: filtered on bulk and layer nodes, kept on
+        // boundary (zero velocity: no bounce-back partner) and ghost nodes;
+        // the row's pads stay zero
+        if (rest) S.G[i * QP + REST] = outr;
         if constexpr (L::D == 2) {
             // the gathered chunks of every row also go to G2, the compact
             // (32-B) rows RK stage 1 gathers from; boundary and ghost rows
@@ -1505,7 +1523,7 @@ int enqueue_step_k(const StepLaunch& P, cudaStream_t st) {
         const int g = r * sms;
         return n < g ? n : g;
     };
-    constexpr int RB = MTR<L>::BLOCK, FB = MTF<L>::BLOCK;
+    constexpr int RB = MTR<L>::BLOCK, FB = MTF<L>::BLOCK, FFB = MTFF<L>::BLOCK;
     auto pgrid = [&](auto kern, size_t smem, int n) { return pgrid_b(kern, smem, n, FB, bo); };
     const bool prof = prof_on();
 #define LAUNCH(id, n, ...)                      \
@@ -1520,7 +1538,7 @@ int enqueue_step_k(const StepLaunch& P, cudaStream_t st) {
     LAUNCH(K_EDGE_COLLIDE, P.n_edge,
            (k_edge_collide<L, KB><<<pgrid(k_edge_collide<L, KB>, sb, P.n_edge), FB, sb, st>>>(P.edge, P.n_edge, P.scenes)));
     LAUNCH(K_FILTER, P.n_all_mt,
-           (k_filter<L, K><<<pgrid(k_filter<L, K>, s2, P.n_all_mt), FB, s2, st>>>(P.all_mt, P.n_all_mt, P.scenes)));
+           (k_filter<L, K><<<pgrid_b(k_filter<L, K>, s2, P.n_all_mt, FFB, bo), FFB, s2, st>>>(P.all_mt, P.n_all_mt, P.scenes)));
     // the RK stages at the tuned threads per node
     auto rk_launch = [&](auto kern, int tpn) {
         const int blk = MT<L>::NPB * tpn;
@@ -1619,10 +1637,17 @@ int tune_k(const StepLaunch& P, cudaStream_t st) {
                 log += line;
                 const bool is_default = tpn == 0 && bps == 0;
                 if (is_default) best_default_ms = ms;
+                const bool hopeless = tpn != 0 && bps == 0 && best_ms > 0.f && ms > 1.25f * best_ms;
                 if (best_ms < 0.f || ms < best_ms) {
                     best.bps = bps;
                     best.tpn = tpn;
                     best_ms = ms;
+                }
+                // a thread shape 25% behind at the default carveout is not
+                // tried at the others (keeps the tuning of a large batch short)
+                if (hopeless) {
+                    log += " (skipped)";
+                    break;
                 }
             }
             // the trials changed this kernel's carveout
