@@ -90,6 +90,12 @@ using MTF = Shape<L, L::D == 3 ? 8 : L::QP / 4>;   // boundary kernels
 // rest population (a scalar of the same row), so no lane works on pads
 template <class L>
 using MTFF = Shape<L, L::D == 3 ? 8 : L::NGATHER>;
+// blocks per SM of the filter for the RK stages' tuned bps: the same threads
+// per SM (its blocks are the RK stages' size)
+template <class L>
+constexpr int filter_bps(int bps) {
+    return (bps * MTR<L>::BLOCK + MTFF<L>::BLOCK - 1) / MTFF<L>::BLOCK;
+}
 
 // blocks per SM of the MTF-shaped kernels for the RK stages' tuned bps: the
 // same threads per SM
@@ -465,6 +471,17 @@ __device__ __forceinline__ void collide(const float* g, float drho, const float*
 
 // ------------------------------------------------------------- kernels
 // SceneDev of the current item into shared memory (warp 0 copies words)
+// Programmatic dependent launch between the step's kernels: a kernel lets
+// the next one be scheduled once all its blocks have finished their work
+// (earlier, the waiting blocks of later kernels took SM slots from the
+// running one), and the next kernel's blocks run their prologue -- shared-memory set-up and the first
+// bulk copy of table records, which no kernel of the step writes -- before
+// waiting for the previous kernel's completion and memory (griddepcontrol.
+// wait) ahead of their first read of step data. Without a programmatic
+// dependency (a plain launch) the wait returns at once.
+__device__ __forceinline__ void pdl_allow_next() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait_prev() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 __device__ __forceinline__ void load_scene(SceneDev& dst, const SceneDev* src) {
     if (threadIdx.x < 32) {
         const int* a = reinterpret_cast<const int*>(src);
@@ -475,13 +492,16 @@ __device__ __forceinline__ void load_scene(SceneDev& dst, const SceneDev* src) {
 
 #define NAGA_FOR_ITEMS(items, nitems)                           \
     __shared__ SceneDev S;                                      \
+    pdl_wait_prev();                                            \
     for (int w_ = blockIdx.x; w_ < (nitems); w_ += gridDim.x) { \
         const WorkItem it = (items)[w_];                        \
         __syncthreads();                                        \
         load_scene(S, scenes + it.scene);                       \
         __syncthreads();
 
-#define NAGA_END_ITEMS }
+#define NAGA_END_ITEMS \
+    }                      \
+    pdl_allow_next();
 
 // Node-local part of the step, one thread per node (all nodes):
 // rho, u (stored for the probes and the next step); the PML trapezoid
@@ -626,6 +646,7 @@ __global__ void __launch_bounds__(kBlock, (L::D == 3 ? 4 : 8)) k_macro_pml(const
 template <int QP>
 __global__ void __launch_bounds__(256) k_scene_tail(const SceneDev* __restrict__ scenes) {
     __shared__ double red[256];
+    pdl_wait_prev();
     const SceneDev& S = scenes[blockIdx.x];
     const int t = blockIdx.y;
     if (t < 2 * QP) {
@@ -800,6 +821,7 @@ constexpr int tile_cap() {
     };                                                                                                 \
     uint32_t pipe_par_ = 0;                                                                            \
     if (threadIdx.x == 0 && (int)blockIdx.x < nitems) pipe_issue_(blockIdx.x, 0);                      \
+    pdl_wait_prev();                                                                                   \
     int pipe_t_ = 0;                                                                                   \
     for (int w_ = blockIdx.x; w_ < nitems; w_ += gridDim.x, ++pipe_t_) {                               \
         const int b_ = pipe_t_ & 1;                                                                    \
@@ -828,7 +850,9 @@ constexpr int tile_cap() {
             __syncthreads();                                                                           \
         }
 
-#define NAGA_PIPE_END }
+#define NAGA_PIPE_END \
+    }                     \
+    pdl_allow_next();
 
 // table blocks of the gather kernels
 struct StencilSrc {  // divergence stencil (Wx, Wy, Wz | filter weight, index)
@@ -986,7 +1010,10 @@ __global__ void __launch_bounds__(MTF<L>::BLOCK, 5) k_edge_collide(const WorkIte
 // bulk + layer: f = s1 + 0.75 sum_s w_s (s1_s - s1) (simulation_engine.cuh:
 // 1233-1323); boundary: bounce-back f_a <- f_bb(a) where c_a . n > 0
 // (:789-944), a swap within each opposite pair; ghost: copy
-template <class L, int K>
+// DRY (the launch-shape tuner's trials): the same gathers and arithmetic,
+// the result written into the interpolation-source scratch S1P (dead between
+// steps: the next step's node-local kernel rewrites it) instead of the state
+template <class L, int K, bool DRY = false>
 __global__ void __launch_bounds__(MTFF<L>::BLOCK) k_filter(const WorkItem* __restrict__ items, int nitems,
                                                            const SceneDev* __restrict__ scenes) {
     using G = MTFF<L>;
@@ -1042,12 +1069,14 @@ __global__ void __launch_bounds__(MTFF<L>::BLOCK) k_filter(const WorkItem* __res
         } else {
             out = f;
         }
-        st4(S.G, i, QP, c, out);
+        float* const Gout = DRY ? S.S1P : S.G;
+        st4(Gout, i, QP, c, out);
         // the rest population: filtered on bulk and layer nodes, kept on
         // boundary (zero velocity: no bounce-back partner) and ghost nodes;
         // the row's pads stay zero
-        if (rest) S.G[i * QP + REST] = outr;
-        if constexpr (L::D == 2) {
+        if (rest) Gout[i * QP + REST] = outr;
+        if constexpr (DRY) {
+        } else if constexpr (L::D == 2) {
             // the gathered chunks of every row also go to G2, the compact
             // (32-B) rows RK stage 1 gathers from; boundary and ghost rows
             // keep their values through the stages, so G1 carries them too
@@ -1396,6 +1425,7 @@ struct ShapeKey {
 // stages (0: the default, one chunk per thread)
 struct TunedShape {
     int bps = 0, tpn = 0;
+    int fbps = 0;  // the filter's resident blocks per SM (0: default carveout)
 };
 std::mutex g_shape_mu;
 std::map<ShapeKey, TunedShape> g_shape;
@@ -1466,12 +1496,14 @@ int rk_each_stage(int tpn, Fn&& fn) {
 
 template <class L, int K, int KB>
 struct AppliedShape {
-    static int bps, tpn;  // shape currently set on the instantiation's kernels (-2: unknown)
+    static int bps, tpn, fbps;  // shape currently set on the instantiation's kernels (-2: unknown)
 };
 template <class L, int K, int KB>
 int AppliedShape<L, K, KB>::bps = -2;
 template <class L, int K, int KB>
 int AppliedShape<L, K, KB>::tpn = -2;
+template <class L, int K, int KB>
+int AppliedShape<L, K, KB>::fbps = -2;
 
 // carveout of every gather kernel of an instantiation (set only when the
 // shape changes)
@@ -1479,21 +1511,49 @@ template <class L, int K, int KB>
 int apply_shape(const TunedShape& sh) {
     int& applied = AppliedShape<L, K, KB>::bps;
     int& applied_tpn = AppliedShape<L, K, KB>::tpn;
+    int& applied_fbps = AppliedShape<L, K, KB>::fbps;
     std::lock_guard<std::mutex> lk(g_shape_mu);
     const int bps = sh.bps;
-    if (applied == bps && applied_tpn == sh.tpn) return NAGA_OK;
+    if (applied == bps && applied_tpn == sh.tpn && applied_fbps == sh.fbps) return NAGA_OK;
     using TF = float2;  // filter records
     const size_t s4 = tile_bytes<L, K, float4>(), s2 = tile_bytes<L, K, TF>(), sb = tile_bytes<L, KB, float2>();
     int rc;
     const int bo = other_bps<L>(bps);
     if ((rc = set_blocks_per_sm(k_pml_gather<L, K>, s4, bps)) ||
         (rc = rk_each_stage<L, K>(sh.tpn, [&](auto kern, int) { return set_blocks_per_sm(kern, s4, bps); })) ||
-        (rc = set_blocks_per_sm(k_filter<L, K>, s2, bo)) || (rc = set_blocks_per_sm(k_edge_collide<L, KB>, sb, bo)) ||
+        (rc = set_blocks_per_sm(k_filter<L, K>, s2, sh.fbps)) ||
+        (rc = set_blocks_per_sm(k_edge_collide<L, KB>, sb, bo)) ||
         (rc = set_blocks_per_sm(k_edge_interp<L, KB>, sb, bo)))
         return rc;
     applied = bps;
     applied_tpn = sh.tpn;
+    applied_fbps = sh.fbps;
     return NAGA_OK;
+}
+
+// programmatic dependent launch of the step's kernels (see pdl_wait_prev);
+// NAGA_PDL=0 in the environment launches them plainly
+bool pdl_on() {
+    static const bool on = [] {
+        const char* e = std::getenv("NAGA_PDL");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+template <class... KArgs, class... Args>
+cudaError_t launch_step_kernel(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                               Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl_on() ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kern, args...);
 }
 
 template <class L, int K, int KB>
@@ -1526,23 +1586,28 @@ int enqueue_step_k(const StepLaunch& P, cudaStream_t st) {
     constexpr int RB = MTR<L>::BLOCK, FB = MTF<L>::BLOCK, FFB = MTFF<L>::BLOCK;
     auto pgrid = [&](auto kern, size_t smem, int n) { return pgrid_b(kern, smem, n, FB, bo); };
     const bool prof = prof_on();
+    cudaError_t lerr = cudaSuccess;
+    auto keep = [&](cudaError_t e) {
+        if (lerr == cudaSuccess) lerr = e;
+    };
 #define LAUNCH(id, n, ...)                      \
     if ((n) > 0) {                              \
         if (prof) prof_begin(id, st);           \
         __VA_ARGS__;                            \
         if (prof) prof_end(id, st);             \
     }
-    LAUNCH(K_MACRO, P.n_all, (k_macro_pml<L><<<grid(P.n_all), kBlock, 0, st>>>(P.all, P.n_all, P.scenes)));
-    LAUNCH(K_TAIL, P.nscenes, (k_scene_tail<L::QP><<<dim3(P.nscenes, 2 * L::QP + 1), 256, 0, st>>>(P.scenes)));
-    LAUNCH(K_PML, P.n_pml, (k_pml_gather<L, K><<<pgrid_b(k_pml_gather<L, K>, s4, P.n_pml, RB, bps), RB, s4, st>>>(P.pml, P.n_pml, P.scenes)));
+    LAUNCH(K_MACRO, P.n_all, keep(launch_step_kernel(k_macro_pml<L>, grid(P.n_all), kBlock, 0, st, P.all, P.n_all, P.scenes)));
+    LAUNCH(K_TAIL, P.nscenes, keep(launch_step_kernel(k_scene_tail<L::QP>, dim3(P.nscenes, 2 * L::QP + 1), 256, 0, st, P.scenes)));
+    LAUNCH(K_PML, P.n_pml, keep(launch_step_kernel(k_pml_gather<L, K>, pgrid_b(k_pml_gather<L, K>, s4, P.n_pml, RB, bps), RB, s4, st, P.pml, P.n_pml, P.scenes)));
     LAUNCH(K_EDGE_COLLIDE, P.n_edge,
-           (k_edge_collide<L, KB><<<pgrid(k_edge_collide<L, KB>, sb, P.n_edge), FB, sb, st>>>(P.edge, P.n_edge, P.scenes)));
+           keep(launch_step_kernel(k_edge_collide<L, KB>, pgrid(k_edge_collide<L, KB>, sb, P.n_edge), FB, sb, st, P.edge, P.n_edge, P.scenes)));
     LAUNCH(K_FILTER, P.n_all_mt,
-           (k_filter<L, K><<<pgrid_b(k_filter<L, K>, s2, P.n_all_mt, FFB, bo), FFB, s2, st>>>(P.all_mt, P.n_all_mt, P.scenes)));
+           keep(launch_step_kernel(k_filter<L, K>, pgrid_b(k_filter<L, K>, s2, P.n_all_mt, FFB, sh.fbps), FFB, s2, st, P.all_mt, P.n_all_mt, P.scenes)));
     // the RK stages at the tuned threads per node
     auto rk_launch = [&](auto kern, int tpn) {
         const int blk = MT<L>::NPB * tpn;
-        kern<<<pgrid_b(kern, s4, P.n_fluid, blk, bps), blk, s4, st>>>(P.fluid, P.n_fluid, P.scenes);
+        keep(launch_step_kernel(kern, pgrid_b(kern, s4, P.n_fluid, blk, bps), blk, s4, st, P.fluid, P.n_fluid,
+                                P.scenes));
         return NAGA_OK;
     };
     LAUNCH(K_RK1, P.n_fluid, (rk_dispatch<L, K, 1>(sh.tpn, rk_launch)));
@@ -1550,8 +1615,9 @@ int enqueue_step_k(const StepLaunch& P, cudaStream_t st) {
     LAUNCH(K_RK3, P.n_fluid, (rk_dispatch<L, K, 3>(sh.tpn, rk_launch)));
     LAUNCH(K_RK4, P.n_fluid, (rk_dispatch<L, K, 4>(sh.tpn, rk_launch)));
     LAUNCH(K_EDGE_INTERP, P.n_edge,
-           (k_edge_interp<L, KB><<<pgrid(k_edge_interp<L, KB>, sb, P.n_edge), FB, sb, st>>>(P.edge, P.n_edge, P.scenes)));
+           keep(launch_step_kernel(k_edge_interp<L, KB>, pgrid(k_edge_interp<L, KB>, sb, P.n_edge), FB, sb, st, P.edge, P.n_edge, P.scenes)));
 #undef LAUNCH
+    NAGA_CUDA_TRY(lerr);
     NAGA_CUDA_TRY(cudaGetLastError());
     return NAGA_OK;
 }
@@ -1581,13 +1647,15 @@ int tune_k(const StepLaunch& P, cudaStream_t st) {
     if (env_bps || env_tpn) {
         TunedShape sh;
         sh.bps = env_bps ? std::max(0, std::atoi(env_bps)) : 0;
+        sh.fbps = filter_bps<L>(sh.bps);
         const int t = env_tpn ? std::atoi(env_tpn) : 0;
         for (int c = 0; c < RkShapes<L>::n; ++c)
             if (RkShapes<L>::tpn[c] == t && (K > 0 || c == 0)) sh.tpn = c == 0 ? 0 : t;
         std::lock_guard<std::mutex> lk(g_shape_mu);
         g_shape[key] = sh;
-        std::snprintf(line, sizeof line, "dim %d k %d kb %d items 2^%d: tpn %d bps %d (NAGA_GATHER_BPS / _TPN)\n",
-                      key.dim, key.k, key.kb, key.bucket, sh.tpn ? sh.tpn : MTR<L>::TPN, sh.bps);
+        std::snprintf(line, sizeof line,
+                      "dim %d k %d kb %d items 2^%d: tpn %d bps %d filter bps %d (NAGA_GATHER_BPS / _TPN)\n",
+                      key.dim, key.k, key.kb, key.bucket, sh.tpn ? sh.tpn : MTR<L>::TPN, sh.bps, sh.fbps);
         g_tune_log += line;
         return NAGA_OK;
     }
@@ -1654,17 +1722,66 @@ int tune_k(const StepLaunch& P, cudaStream_t st) {
             return set_blocks_per_sm(kern, s4, 0);
         });
     }
+    // a non-default shape must beat the default by 3%
+    if (best_default_ms > 0.f && (best.bps != 0 || best.tpn != 0) && best_ms > 0.97f * best_default_ms) best = {};
+    // the filter's resident blocks per SM, timed on its dry variant (same
+    // gathers, result into dead scratch) over the batch's items: the default
+    // carveout, then 2 .. max; a fixed carveout must win by 3%
+    if (rc == NAGA_OK && P.n_all_mt > 0) {
+        auto fk = k_filter<L, K, true>;
+        const size_t s2 = tile_bytes<L, K, float2>();
+        constexpr int FFB = MTFF<L>::BLOCK;
+        float fbest = -1.f, fdefault = -1.f;
+        int fb = 0;
+        int maxr = 0;
+        if ((rc = allow_smem(fk, s2)) == NAGA_OK && (rc = set_blocks_per_sm(fk, s2, 0)) == NAGA_OK &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxr, fk, FFB, s2) == cudaSuccess) {
+            maxr = std::max(maxr, 1);
+            log += " | filter";
+            for (int bps = 0; bps <= maxr; bps = bps == 0 ? 2 : bps + 1) {
+                if ((rc = set_blocks_per_sm(fk, s2, bps))) break;
+                const int g = std::min(P.n_all_mt, (bps > 0 ? bps : maxr) * sms);
+                auto timed = [&](int reps, float* ms) -> bool {
+                    cudaEventRecord(e0, st);
+                    for (int q = 0; q < reps; ++q) fk<<<g, FFB, s2, st>>>(P.all_mt, P.n_all_mt, P.scenes);
+                    cudaEventRecord(e1, st);
+                    if (cudaEventSynchronize(e1) != cudaSuccess || cudaGetLastError() != cudaSuccess) return false;
+                    cudaEventElapsedTime(ms, e0, e1);
+                    *ms /= reps;
+                    return true;
+                };
+                fk<<<g, FFB, s2, st>>>(P.all_mt, P.n_all_mt, P.scenes);
+                float ms = 0.f, ms2 = 0.f;
+                const int reps = 1;
+                bool ok = timed(reps, &ms);
+                const int reps2 = ms < 0.4f ? std::min(8, std::max(2, (int)(2.f / std::max(ms, 1e-3f)))) : 1;
+                if (ok && timed(reps2, &ms2)) ms = std::min(ms, ms2);
+                if (!ok) {
+                    rc = set_error(NAGA_ECUDA, "launch-shape tuning: a filter trial launch failed");
+                    break;
+                }
+                std::snprintf(line, sizeof line, " %d:%.1fus", bps, ms * 1000.f);
+                log += line;
+                if (bps == 0) fdefault = ms;
+                if (fbest < 0.f || ms < fbest) {
+                    fbest = ms;
+                    fb = bps;
+                }
+            }
+            if (fb != 0 && fbest > 0.97f * fdefault) fb = 0;
+            best.fbps = fb;
+        }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     AppliedShape<L, K, KB>::bps = -2;  // the trials changed rk stage 1's carveouts
     AppliedShape<L, K, KB>::tpn = -2;
+    AppliedShape<L, K, KB>::fbps = -2;
     if (rc) return rc;
-    // a non-default shape must beat the default by 3%
-    if (best_default_ms > 0.f && (best.bps != 0 || best.tpn != 0) && best_ms > 0.97f * best_default_ms) best = {};
     std::lock_guard<std::mutex> lk(g_shape_mu);
     g_shape[key] = best;
-    std::snprintf(line, sizeof line, "dim %d k %d kb %d items 2^%d: tpn %d bps %d of", key.dim, key.k, key.kb,
-                  key.bucket, best.tpn ? best.tpn : MTR<L>::TPN, best.bps);
+    std::snprintf(line, sizeof line, "dim %d k %d kb %d items 2^%d: tpn %d bps %d filter bps %d of", key.dim,
+                  key.k, key.kb, key.bucket, best.tpn ? best.tpn : MTR<L>::TPN, best.bps, best.fbps);
     g_tune_log += line + log + "\n";
     return NAGA_OK;
 }

@@ -190,8 +190,9 @@ print(naga.tuning_report())
 
 
 def test_launch_shape_does_not_change_results(tmp_path):
-    """The tuner's choices -- resident blocks per SM of the gather kernels and
-    threads per node of the RK stages -- change only the launch: runs with
+    """The tuner's choices -- resident blocks per SM of the gather kernels, of
+    the filter, and threads per node of the RK stages -- change only the
+    launch: runs with
     the tuned shape and with shapes forced through NAGA_GATHER_BPS /
     NAGA_GATHER_TPN (D3Q27 at 7 and 4 threads per node, D2Q9 at 1) agree bit
     for bit, and the tuner logs what it measured."""
@@ -218,11 +219,11 @@ def test_launch_shape_does_not_change_results(tmp_path):
     for o in outs[1:]:
         assert np.array_equal(outs[0], o)
     assert "dim 3 k 32 kb 32" in logs[0] and "| tpn 8 0:" in logs[0] and "| tpn 7" in logs[0]
-    assert "dim 2 k 16 kb 16" in logs[0] and "| tpn 1" in logs[0]
-    assert "tpn 8 bps 2 (NAGA_GATHER_BPS" in logs[1]
-    assert "dim 3 k 32 kb 32 items 2^" in logs[2] and "tpn 7 bps 0 (NAGA_GATHER" in logs[2]
-    assert "tpn 4 bps 3 (NAGA_GATHER" in logs[3]
-    assert "dim 2 k 16 kb 16 items 2^" in logs[4] and "tpn 1 bps 0 (NAGA_GATHER" in logs[4]
+    assert "dim 2 k 16 kb 16" in logs[0] and "| tpn 1" in logs[0] and "| filter 0:" in logs[0]
+    assert "tpn 8 bps 2 filter bps" in logs[1] and "(NAGA_GATHER_BPS" in logs[1]
+    assert "dim 3 k 32 kb 32 items 2^" in logs[2] and "tpn 7 bps 0 filter bps 0 (NAGA_GATHER" in logs[2]
+    assert "tpn 4 bps 3 filter bps" in logs[3]
+    assert "dim 2 k 16 kb 16 items 2^" in logs[4] and "tpn 1 bps 0 filter bps 0 (NAGA_GATHER" in logs[4]
 
 
 def test_async_probe_reads_match_synchronous(naga, oracle):
