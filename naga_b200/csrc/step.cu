@@ -1426,6 +1426,7 @@ struct ShapeKey {
 struct TunedShape {
     int bps = 0, tpn = 0;
     int fbps = 0;  // the filter's resident blocks per SM (0: default carveout)
+    int pbps = 0;  // the PML gather's
 };
 std::mutex g_shape_mu;
 std::map<ShapeKey, TunedShape> g_shape;
@@ -1496,8 +1497,10 @@ int rk_each_stage(int tpn, Fn&& fn) {
 
 template <class L, int K, int KB>
 struct AppliedShape {
-    static int bps, tpn, fbps;  // shape currently set on the instantiation's kernels (-2: unknown)
+    static int bps, tpn, fbps, pbps;  // shape currently set on the instantiation's kernels (-2: unknown)
 };
+template <class L, int K, int KB>
+int AppliedShape<L, K, KB>::pbps = -2;
 template <class L, int K, int KB>
 int AppliedShape<L, K, KB>::bps = -2;
 template <class L, int K, int KB>
@@ -1514,12 +1517,13 @@ int apply_shape(const TunedShape& sh) {
     int& applied_fbps = AppliedShape<L, K, KB>::fbps;
     std::lock_guard<std::mutex> lk(g_shape_mu);
     const int bps = sh.bps;
-    if (applied == bps && applied_tpn == sh.tpn && applied_fbps == sh.fbps) return NAGA_OK;
+    int& applied_pbps = AppliedShape<L, K, KB>::pbps;
+    if (applied == bps && applied_tpn == sh.tpn && applied_fbps == sh.fbps && applied_pbps == sh.pbps) return NAGA_OK;
     using TF = float2;  // filter records
     const size_t s4 = tile_bytes<L, K, float4>(), s2 = tile_bytes<L, K, TF>(), sb = tile_bytes<L, KB, float2>();
     int rc;
     const int bo = other_bps<L>(bps);
-    if ((rc = set_blocks_per_sm(k_pml_gather<L, K>, s4, bps)) ||
+    if ((rc = set_blocks_per_sm(k_pml_gather<L, K>, s4, sh.pbps)) ||
         (rc = rk_each_stage<L, K>(sh.tpn, [&](auto kern, int) { return set_blocks_per_sm(kern, s4, bps); })) ||
         (rc = set_blocks_per_sm(k_filter<L, K>, s2, sh.fbps)) ||
         (rc = set_blocks_per_sm(k_edge_collide<L, KB>, sb, bo)) ||
@@ -1528,6 +1532,7 @@ int apply_shape(const TunedShape& sh) {
     applied = bps;
     applied_tpn = sh.tpn;
     applied_fbps = sh.fbps;
+    applied_pbps = sh.pbps;
     return NAGA_OK;
 }
 
@@ -1598,7 +1603,7 @@ int enqueue_step_k(const StepLaunch& P, cudaStream_t st) {
     }
     LAUNCH(K_MACRO, P.n_all, keep(launch_step_kernel(k_macro_pml<L>, grid(P.n_all), kBlock, 0, st, P.all, P.n_all, P.scenes)));
     LAUNCH(K_TAIL, P.nscenes, keep(launch_step_kernel(k_scene_tail<L::QP>, dim3(P.nscenes, 2 * L::QP + 1), 256, 0, st, P.scenes)));
-    LAUNCH(K_PML, P.n_pml, keep(launch_step_kernel(k_pml_gather<L, K>, pgrid_b(k_pml_gather<L, K>, s4, P.n_pml, RB, bps), RB, s4, st, P.pml, P.n_pml, P.scenes)));
+    LAUNCH(K_PML, P.n_pml, keep(launch_step_kernel(k_pml_gather<L, K>, pgrid_b(k_pml_gather<L, K>, s4, P.n_pml, RB, sh.pbps), RB, s4, st, P.pml, P.n_pml, P.scenes)));
     LAUNCH(K_EDGE_COLLIDE, P.n_edge,
            keep(launch_step_kernel(k_edge_collide<L, KB>, pgrid(k_edge_collide<L, KB>, sb, P.n_edge), FB, sb, st, P.edge, P.n_edge, P.scenes)));
     LAUNCH(K_FILTER, P.n_all_mt,
@@ -1648,6 +1653,7 @@ int tune_k(const StepLaunch& P, cudaStream_t st) {
         TunedShape sh;
         sh.bps = env_bps ? std::max(0, std::atoi(env_bps)) : 0;
         sh.fbps = filter_bps<L>(sh.bps);
+        sh.pbps = sh.bps;
         const int t = env_tpn ? std::atoi(env_tpn) : 0;
         for (int c = 0; c < RkShapes<L>::n; ++c)
             if (RkShapes<L>::tpn[c] == t && (K > 0 || c == 0)) sh.tpn = c == 0 ? 0 : t;
@@ -1724,64 +1730,72 @@ int tune_k(const StepLaunch& P, cudaStream_t st) {
     }
     // a non-default shape must beat the default by 3%
     if (best_default_ms > 0.f && (best.bps != 0 || best.tpn != 0) && best_ms > 0.97f * best_default_ms) best = {};
-    // the filter's resident blocks per SM, timed on its dry variant (same
-    // gathers, result into dead scratch) over the batch's items: the default
-    // carveout, then 2 .. max; a fixed carveout must win by 3%
-    if (rc == NAGA_OK && P.n_all_mt > 0) {
-        auto fk = k_filter<L, K, true>;
-        const size_t s2 = tile_bytes<L, K, float2>();
-        constexpr int FFB = MTFF<L>::BLOCK;
-        float fbest = -1.f, fdefault = -1.f;
-        int fb = 0;
-        int maxr = 0;
-        if ((rc = allow_smem(fk, s2)) == NAGA_OK && (rc = set_blocks_per_sm(fk, s2, 0)) == NAGA_OK &&
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxr, fk, FFB, s2) == cudaSuccess) {
-            maxr = std::max(maxr, 1);
-            log += " | filter";
-            for (int bps = 0; bps <= maxr; bps = bps == 0 ? 2 : bps + 1) {
-                if ((rc = set_blocks_per_sm(fk, s2, bps))) break;
-                const int g = std::min(P.n_all_mt, (bps > 0 ? bps : maxr) * sms);
-                auto timed = [&](int reps, float* ms) -> bool {
-                    cudaEventRecord(e0, st);
-                    for (int q = 0; q < reps; ++q) fk<<<g, FFB, s2, st>>>(P.all_mt, P.n_all_mt, P.scenes);
-                    cudaEventRecord(e1, st);
-                    if (cudaEventSynchronize(e1) != cudaSuccess || cudaGetLastError() != cudaSuccess) return false;
-                    cudaEventElapsedTime(ms, e0, e1);
-                    *ms /= reps;
-                    return true;
-                };
-                fk<<<g, FFB, s2, st>>>(P.all_mt, P.n_all_mt, P.scenes);
-                float ms = 0.f, ms2 = 0.f;
-                const int reps = 1;
-                bool ok = timed(reps, &ms);
-                const int reps2 = ms < 0.4f ? std::min(8, std::max(2, (int)(2.f / std::max(ms, 1e-3f)))) : 1;
-                if (ok && timed(reps2, &ms2)) ms = std::min(ms, ms2);
-                if (!ok) {
-                    rc = set_error(NAGA_ECUDA, "launch-shape tuning: a filter trial launch failed");
-                    break;
-                }
-                std::snprintf(line, sizeof line, " %d:%.1fus", bps, ms * 1000.f);
-                log += line;
-                if (bps == 0) fdefault = ms;
-                if (fbest < 0.f || ms < fbest) {
-                    fbest = ms;
-                    fb = bps;
-                }
-            }
-            if (fb != 0 && fbest > 0.97f * fdefault) fb = 0;
-            best.fbps = fb;
+    // resident blocks per SM of the filter, timed on its dry variant (same
+    // gathers, result into dead scratch), and of the PML gather, which only
+    // adds into the collision scratch (dead between steps), over the batch's
+    // items: the default carveout, then 2 .. max; a fixed carveout must win
+    // by 3%
+    auto tune_bps = [&](auto kern, size_t smem, int block, const WorkItem* list, int n, const char* name,
+                        int* out) {
+        if (rc != NAGA_OK || n <= 0) return;
+        float kbest = -1.f, kdefault = -1.f;
+        int kb = 0, maxr = 0;
+        if ((rc = allow_smem(kern, smem)) || (rc = set_blocks_per_sm(kern, smem, 0))) return;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxr, kern, block, smem) != cudaSuccess) {
+            rc = set_error(NAGA_ECUDA, "launch-shape tuning: occupancy query failed");
+            return;
         }
-    }
+        maxr = std::max(maxr, 1);
+        log += " | ";
+        log += name;
+        for (int bps = 0; bps <= maxr; bps = bps == 0 ? 2 : bps + 1) {
+            if ((rc = set_blocks_per_sm(kern, smem, bps))) return;
+            const int g = std::min(n, (bps > 0 ? bps : maxr) * sms);
+            auto timed = [&](int reps, float* ms) -> bool {
+                cudaEventRecord(e0, st);
+                for (int q = 0; q < reps; ++q) kern<<<g, block, smem, st>>>(list, n, P.scenes);
+                cudaEventRecord(e1, st);
+                if (cudaEventSynchronize(e1) != cudaSuccess || cudaGetLastError() != cudaSuccess) return false;
+                cudaEventElapsedTime(ms, e0, e1);
+                *ms /= reps;
+                return true;
+            };
+            kern<<<g, block, smem, st>>>(list, n, P.scenes);
+            float ms = 0.f, ms2 = 0.f;
+            bool ok = timed(1, &ms);
+            const int reps2 = ms < 0.4f ? std::min(8, std::max(2, (int)(2.f / std::max(ms, 1e-3f)))) : 1;
+            if (ok && timed(reps2, &ms2)) ms = std::min(ms, ms2);
+            if (!ok) {
+                rc = set_error(NAGA_ECUDA, "launch-shape tuning: a trial launch failed");
+                return;
+            }
+            std::snprintf(line, sizeof line, " %d:%.1fus", bps, ms * 1000.f);
+            log += line;
+            if (bps == 0) kdefault = ms;
+            if (kbest < 0.f || ms < kbest) {
+                kbest = ms;
+                kb = bps;
+            }
+        }
+        if (kb != 0 && kbest > 0.97f * kdefault) kb = 0;
+        *out = kb;
+        rc = set_blocks_per_sm(kern, smem, 0);
+    };
+    tune_bps(k_filter<L, K, true>, tile_bytes<L, K, float2>(), MTFF<L>::BLOCK, P.all_mt, P.n_all_mt, "filter",
+             &best.fbps);
+    tune_bps(k_pml_gather<L, K>, s4, MTR<L>::BLOCK, P.pml, P.n_pml, "pml", &best.pbps);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     AppliedShape<L, K, KB>::bps = -2;  // the trials changed rk stage 1's carveouts
     AppliedShape<L, K, KB>::tpn = -2;
     AppliedShape<L, K, KB>::fbps = -2;
+    AppliedShape<L, K, KB>::pbps = -2;
     if (rc) return rc;
     std::lock_guard<std::mutex> lk(g_shape_mu);
     g_shape[key] = best;
-    std::snprintf(line, sizeof line, "dim %d k %d kb %d items 2^%d: tpn %d bps %d filter bps %d of", key.dim,
-                  key.k, key.kb, key.bucket, best.tpn ? best.tpn : MTR<L>::TPN, best.bps, best.fbps);
+    std::snprintf(line, sizeof line, "dim %d k %d kb %d items 2^%d: tpn %d bps %d filter bps %d pml bps %d of",
+                  key.dim, key.k, key.kb, key.bucket, best.tpn ? best.tpn : MTR<L>::TPN, best.bps, best.fbps,
+                  best.pbps);
     g_tune_log += line + log + "\n";
     return NAGA_OK;
 }
