@@ -464,6 +464,14 @@ int scene_setup(naga_scene* s) {
         if ((rc = compact_records_device(W, (int64_t)k * N, str, st))) return rc;
     }
     V.stR = str;
+    // halo blobs of the D3Q27 RK stages (one per bulk/layer pass)
+    float4* sth = nullptr;
+    if (D == 3 && k == kHaloK && npb == 32 && s->nbl > 0) {
+        const int64_t n_pass = (s->nbl + npb - 1) / npb;
+        if ((rc = s->alloc(&sth, n_pass * (kHaloBlobBytes / 16)))) return rc;
+        if ((rc = halo_build_device(W, s->nbl, k, npb, sth, st))) return rc;
+    }
+    V.stH = sth;
 
     // boundary interpolation: kNN among bulk + layer, RPIM at the boundary
     // node with the nodal spacing (detail/simulation_engine.cuh:223-258)

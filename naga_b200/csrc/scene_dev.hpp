@@ -59,6 +59,7 @@ struct SceneDev {
     float4* M;
     // tables
     const float4* stW;
+    const float4* stH;  // D3Q27, k = kHaloK: halo blobs of the bulk/layer passes (below), else null
     const float4* stP;  // PML gather records, pass order (Wx, Wy, Wz or 0, PHI row bits)
     const float* stR;   // D2Q9: the stencil records compacted to (Wx, Wy, index bits), pass order
     const float4* PV;  // [nbl][2]: (V1, V2) = sum over layer supports of W_s sigma_j, W_s sigma_j^2
@@ -92,6 +93,21 @@ __host__ __device__ inline int64_t pass_record(int64_t i, int t, int k, int64_t 
     const int64_t nn = end - b < npb ? end - b : npb;
     return b * k + (int64_t)t * nn + (i - b);
 }
+
+// Halo blobs of the D3Q27 RK stages at k = kHaloK: one per bulk/layer pass
+// (the passes of [0, nbl), in order), kHaloBlobBytes each:
+//   u32 [4 + kHaloCap]   row count m, three zero pads, the pass's m distinct
+//                        neighbour rows in ascending order (zero after m)
+//   float4 [npb k]       the pass's stencil records in tile order, with the
+//                        row's position in that list in place of the node
+//                        index; zero after the pass's nn k records
+// A pass with m > kHaloCap keeps the node indices in its records and its
+// stages gather the rows from global memory.
+constexpr int kHaloK = 32;
+constexpr int kHaloCap = 272;
+constexpr int kHaloListBytes = (4 + kHaloCap) * 4;
+constexpr int kHaloBlobBytes = kHaloListBytes + 32 * kHaloK * 16;
+static_assert(kHaloListBytes % 16 == 0 && kHaloBlobBytes % 16 == 0, "bulk-copy sizes");
 
 struct WorkItem {
     uint32_t scene;
@@ -160,6 +176,9 @@ int compact_records_device(const float4* stW, int64_t count, float* stR, cudaStr
 // the PML gather records of a scene (stW in pass order)
 int pml_table_device(int dim, const float4* stW, int64_t nb, int64_t nl, int64_t nbl, int64_t n, int k, float4* stP,
                      cudaStream_t st);
+// the halo blobs of a D3Q27 scene with k = kHaloK (stW in pass order,
+// npb-node passes over [0, nbl)); stH holds ceil(nbl / npb) blobs
+int halo_build_device(const float4* stW, int64_t nbl, int k, int npb, float4* stH, cudaStream_t st);
 // the per-node PML vectors PV of a scene (stW in pass order)
 int pml_vectors_device(int dim, const float4* stW, const float* sigma, int64_t nb, int64_t nl, int64_t nbl, int64_t n,
                        int k, float4* PV, cudaStream_t st);

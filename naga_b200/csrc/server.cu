@@ -227,6 +227,8 @@ extern "C" int64_t naga_scene_estimate_bytes(const naga_scene_desc* d) {
     b += d->n_layer * QP * 4 + (d->n_bulk + d->n_layer + 1) * 32;
     if (d->n_layer > 0) b += (d->n_bulk + d->n_layer) * (int64_t)d->k * 16;  // PML gather records
     if (d->dim == 2) b += N * (int64_t)d->k * 12;                           // compact stencil triplets
+    if (d->dim == 3 && d->k == kHaloK)                                      // RK stage halo blobs
+        b += (d->n_bulk + d->n_layer + 31) / 32 * (int64_t)kHaloBlobBytes;
     // set-up scratch: kNN sort + distances, nearest-neighbour means
     b += N * (16 + 12 + (int64_t)d->k * 4 + 8);
     return b;

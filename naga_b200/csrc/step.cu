@@ -44,6 +44,9 @@
 #include <type_traits>
 #include <utility>
 
+#include <cub/block/block_radix_sort.cuh>
+#include <cub/block/block_scan.cuh>
+
 #include "common.cuh"
 #include "scene_dev.hpp"
 
@@ -1095,6 +1098,23 @@ __global__ void __launch_bounds__(MTFF<L>::BLOCK) k_filter(const WorkItem* __res
     NAGA_PIPE_END
 }
 
+// one stencil term of an RK stage gather on a thread's chunk: the two
+// opposite pairs (d0, -d0), (d1, -d1) of the chunk, record (Wx, Wy, Wz | -),
+// neighbour values v: r += ((d0 . W) v.x, -(d0 . W) v.y, (d1 . W) v.z,
+// -(d1 . W) v.w). Shared by every RK stage kernel so that all of them round
+// alike.
+template <class L>
+__device__ __forceinline__ void rk_term(const float4& rec, const float* d0, const float* d1, const float4& v,
+                                        float4& r) {
+    const float wz = L::D == 3 ? rec.z : 0.f;
+    const float p0 = d0[0] * rec.x + d0[1] * rec.y + d0[2] * wz;
+    const float p1 = d1[0] * rec.x + d1[1] * rec.y + d1[2] * wz;
+    r.x = fmaf(p0, v.x, r.x);
+    r.y = fmaf(-p0, v.y, r.y);
+    r.z = fmaf(p1, v.z, r.z);
+    r.w = fmaf(-p1, v.w, r.w);
+}
+
 // RK4 stage STAGE (detail/rk4_solver.cuh:48-171) with the streaming rates
 // rate_a(i) = -sum_s (c_a . W_s) g_a(j_s) (pde_right_hand_side.cuh:82-176,
 // divergence.cuh:377-488). The rates are linear in g and independent of t
@@ -1154,14 +1174,8 @@ __global__ void __launch_bounds__(MT<L>::NPB * TPN_) k_rk(const WorkItem* __rest
                 rec = reinterpret_cast<const float4*>(tile)[s * nn + ns];
             }
             const uint32_t j = __float_as_uint(rec.w);
-            const float wz = L::D == 3 ? rec.z : 0.f;
             const float4 v = QSRC == QP ? ld4g<L>(src, j, c) : ld4s<L>(src, j, c);
-            const float p0 = d0[0] * rec.x + d0[1] * rec.y + d0[2] * wz;
-            const float p1 = d1[0] * rec.x + d1[1] * rec.y + d1[2] * wz;
-            r.x = fmaf(p0, v.x, r.x);
-            r.y = fmaf(-p0, v.y, r.y);
-            r.z = fmaf(p1, v.z, r.z);
-            r.w = fmaf(-p1, v.w, r.w);
+            rk_term<L>(rec, d0, d1, v, r);
         }
         // rate = -r; stage value = g + a rate
         st4(dst, i, QDST, c, make_float4(fmaf(-a, r.x, f0.x), fmaf(-a, r.y, f0.y), fmaf(-a, r.z, f0.z),
@@ -1186,6 +1200,203 @@ struct RkShapes<D2Q9> {
     static constexpr int n = 2;
     static constexpr int tpn[2] = {2, 1};
 };
+
+// Shape code of the halo RK stages in the tuner's threads-per-node slot
+constexpr int kRkHalo = 100;
+// dynamic shared memory of k_rk_halo: three blob buffers (the pass being
+// computed and two in flight) and two halo row buffers (the pass being
+// computed and the next), two blocks per SM
+constexpr int kHaloRowChunks = D3Q27::NGATHER;
+constexpr size_t kHaloSmem = 3 * (size_t)kHaloBlobBytes + 2 * (size_t)kHaloCap * kHaloRowChunks * 16;
+
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(sdst)), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// RK stage STAGE of D3Q27 at k = kHaloK with the neighbour rows of each pass
+// read from shared memory. A pass of 32 nodes references 1024 neighbour
+// rows but only ~190 distinct ones on the benchmark grid (set-up lists them
+// in the pass's halo blob, see SceneDev::stH); gathering each (node,
+// neighbour, chunk) value from L2 moves ~5x the rows a pass needs and is
+// bound by L2 latency. Here each block streams its passes through a
+// pipeline: the halo blob (records with list positions, and the list) is
+// bulk-copied two passes ahead; one pass ahead, the listed rows' gathered
+// chunks are copied into shared memory with cp.async (16 B per thread, the
+// 7 chunks of a row by 7 consecutive threads); the stage then reads its
+// operands from shared memory, eight threads per node as in k_rk, so each
+// quarter warp reads one row's 112 contiguous bytes (no bank conflicts).
+// The arithmetic is k_rk's (rk_term, same order), so results are bit-equal
+// to every other RK stage shape. A pass whose list overflowed (more than
+// kHaloCap rows) gathers from global memory like k_rk.
+template <int STAGE>
+__global__ void __launch_bounds__(256, 2) k_rk_halo(const WorkItem* __restrict__ items, int nitems,
+                                                    const SceneDev* __restrict__ scenes) {
+    using L = D3Q27;
+    constexpr int K = kHaloK, TPN = 8, NPB = MT<L>::NPB, NCH = kHaloRowChunks, QP = L::QP;
+    constexpr int NB = 3, NH = 2, BLOB = kHaloBlobBytes;
+    static_assert(NPB * TPN == 256 && NPB == 32, "one 32-node pass per 256-thread block");
+    extern __shared__ __align__(128) unsigned char dyn_smem[];
+    unsigned char* const blobs = dyn_smem;
+    float4* const halo = reinterpret_cast<float4*>(dyn_smem + NB * BLOB);
+    __shared__ __align__(8) uint64_t bar[NB];
+    __shared__ SceneDev S;
+    const int c = threadIdx.x % TPN, ns = threadIdx.x / TPN;
+    if (threadIdx.x == 0) {
+        for (int b = 0; b < NB; ++b) mbar_init(&bar[b]);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    // this block's passes: items blockIdx.x + t gridDim.x, t < T. The items
+    // of passes t + 1 and t + 2 are held in registers and pass t + 3's is
+    // loaded one iteration before its use, and the scene fields the copies
+    // need are re-read only when the scene changes, so no dependent global
+    // load stalls a pass
+    const int T = (int)blockIdx.x < nitems ? (nitems - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    auto item_of = [&](int t) {
+        return t < T ? items[(int)blockIdx.x + t * (int)gridDim.x] : WorkItem{0u, 0u, 0u, 0u};
+    };
+    int issued = 0, waited = 0;  // blob copies (thread 0 issues; every thread waits)
+    uint32_t par = 0;
+    bool ok = true;
+    uint32_t blob_scene = 0xFFFFFFFFu;  // thread 0: the scene whose blobs blob_base points at
+    const float4* blob_base = nullptr;
+    auto issue_blob = [&](const WorkItem& w, int t) {
+        if (w.scene != blob_scene) {
+            blob_scene = w.scene;
+            blob_base = scenes[w.scene].stH;
+        }
+        // bulk/layer pass w.begin / NPB of its scene (the passes start at
+        // multiples of NPB)
+        bulk_load(blobs + (t % NB) * BLOB, blob_base + (int64_t)(w.begin / NPB) * (BLOB / 16), BLOB, &bar[t % NB]);
+        ++issued;
+    };
+    auto wait_blob = [&](int t) {
+        if (!ok) return;
+        const int b = t % NB;
+        ok = mbar_wait(&bar[b], (par >> b) & 1u);
+        if (ok) {
+            par ^= 1u << b;
+            ++waited;
+        }
+    };
+    // the listed rows of pass t (stage source rows of its scene) into halo
+    // buffer t % NH
+    uint32_t row_scene = 0xFFFFFFFFu;
+    const float* row_src = nullptr;
+    uint32_t row_n = 0;
+    auto issue_rows = [&](const WorkItem& w, int t) {
+        const uint32_t* list = reinterpret_cast<const uint32_t*>(blobs + (t % NB) * BLOB);
+        const uint32_t m = list[0];
+        if (m > (uint32_t)kHaloCap) return;
+        if (w.scene != row_scene) {
+            const SceneDev& sc = scenes[w.scene];
+            row_scene = w.scene;
+            row_src = STAGE == 1 ? sc.G : STAGE == 3 ? sc.G2 : sc.G1;
+            row_n = (uint32_t)sc.N;
+        }
+        // thread (row r, chunk ch): rows r = threadIdx / 8 + 32 q, the
+        // eighth lane of each row idle
+        float4* hb = halo + (t % NH) * kHaloCap * NCH + c;
+        if (c < NCH)
+            for (int row = ns; row < (int)m; row += NPB) {
+                const uint32_t j = list[4 + row];
+                if (j < row_n) cp_async16(hb + row * NCH, row_src + (int64_t)j * QP + 4 * c);
+            }
+    };
+    WorkItem w0 = item_of(0), w1 = item_of(1), w2 = item_of(2);
+    // the tables do not depend on the previous kernel: the first blobs are
+    // in flight before the wait for it
+    if (threadIdx.x == 0) {
+        if (T > 0) issue_blob(w0, 0);
+        if (T > 1) issue_blob(w1, 1);
+    }
+    pdl_wait_prev();
+    if (T > 0) {
+        wait_blob(0);
+        if (ok) issue_rows(w0, 0);
+    }
+    cp_async_commit();
+    float d0[3], d1[3];
+    pair_dirs<L>(c < NCH ? c : 0, d0, d1);
+    uint32_t cur_scene = 0xFFFFFFFFu;
+    for (int t = 0; t < T; ++t) {
+        const WorkItem w3 = item_of(t + 3);
+        // the previous pass is done with S, its blob and its halo buffer
+        __syncthreads();
+        if (w0.scene != cur_scene) {
+            cur_scene = w0.scene;
+            load_scene(S, scenes + w0.scene);
+        }
+        if (threadIdx.x == 0 && t + 2 < T) issue_blob(w2, t + 2);
+        if (t + 1 < T) {
+            wait_blob(t + 1);
+            if (ok) issue_rows(w1, t + 1);
+        }
+        cp_async_commit();
+        cp_async_wait<1>();  // this pass's rows (committed one pass ago)
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) atomicOr(&g_tile_timeout, 1u);
+            break;
+        }
+        const unsigned char* blob = blobs + (t % NB) * BLOB;
+        const uint32_t m = reinterpret_cast<const uint32_t*>(blob)[0];
+        const float4* tile = reinterpret_cast<const float4*>(blob + kHaloListBytes);
+        const int nn = (int)(w0.end - w0.begin);
+        const int64_t i = (int64_t)w0.begin + ns;
+        if (ns < nn && c < NCH) {
+            // stage buffers as in k_rk: G1 = g + dt/4 A g, G2 = g + dt/3 A G1,
+            // G1 = g + dt/2 A G2, G = g + dt A G1
+            const float* src = STAGE == 1 ? S.G : STAGE == 3 ? S.G2 : S.G1;
+            float* dst = (STAGE == 1 || STAGE == 3) ? S.G1 : STAGE == 2 ? S.G2 : S.G;
+            const float a = S.rk_a[STAGE - 1];
+            const float4 f0 = ld4(S.G, i, QP, c);
+            float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (m <= (uint32_t)kHaloCap) {
+                const float4* hb = halo + (t % NH) * kHaloCap * NCH + c;
+                if (nn == NPB) {
+                    // a full pass: records at a fixed stride
+#pragma unroll 16
+                    for (int s = 0; s < K; ++s) {
+                        const float4 rec = tile[s * NPB + ns];
+                        rk_term<L>(rec, d0, d1, hb[__float_as_uint(rec.w) * NCH], r);
+                    }
+                } else {
+#pragma unroll 4
+                    for (int s = 0; s < K; ++s) {
+                        const float4 rec = tile[s * nn + ns];
+                        rk_term<L>(rec, d0, d1, hb[__float_as_uint(rec.w) * NCH], r);
+                    }
+                }
+            } else {
+                // (rare: kept short so it does not raise the register count)
+#pragma unroll 4
+                for (int s = 0; s < K; ++s) {
+                    const float4 rec = tile[s * nn + ns];
+                    rk_term<L>(rec, d0, d1, ld4g<L>(src, __float_as_uint(rec.w), c), r);
+                }
+            }
+            st4(dst, i, STAGE == 4 ? QP : L::QS, c,
+                make_float4(fmaf(-a, r.x, f0.x), fmaf(-a, r.y, f0.y), fmaf(-a, r.z, f0.z), fmaf(-a, r.w, f0.w)));
+        }
+        w0 = w1;
+        w1 = w2;
+        w2 = w3;
+    }
+    cp_async_wait<0>();
+    // a block that gave up waits (bounded) for the blob copies it still has
+    // in flight before it exits
+    if (threadIdx.x == 0)
+        for (int t = waited; t < issued; ++t) {
+            const int b = t % NB;
+            if (mbar_wait(&bar[b], (par >> b) & 1u)) par ^= 1u << b;
+        }
+    pdl_allow_next();
+}
 
 // boundary: f = interp(f of bulk + layer) (simulation_engine.cuh:1370)
 template <class L, int KB>
@@ -1298,6 +1509,84 @@ __global__ void compact_records_kernel(const float4* __restrict__ stW, int64_t c
 int compact_records_device(const float4* stW, int64_t count, float* stR, cudaStream_t st) {
     if (count <= 0) return NAGA_OK;
     compact_records_kernel<<<(unsigned)((count + 255) / 256), 256, 0, st>>>(stW, count, stR);
+    NAGA_CUDA_TRY(cudaGetLastError());
+    return NAGA_OK;
+}
+
+namespace {
+// One block per bulk/layer pass: the pass's nn k neighbour indices (at most
+// 1024) are sorted, their distinct values listed, and each record's index
+// replaced by its position in the list (binary search), or kept when the
+// list would exceed kHaloCap (layout at SceneDev::stH)
+__global__ void __launch_bounds__(256) halo_build_kernel(const float4* __restrict__ stW, int64_t nbl, int npb,
+                                                         float4* __restrict__ stH) {
+    constexpr int K = kHaloK, PER = 4, CAP = 256 * PER;
+    static_assert(32 * K <= CAP, "a pass's records fit the block's keys");
+    using Sort = cub::BlockRadixSort<uint32_t, 256, PER>;
+    using Scan = cub::BlockScan<int, 256>;
+    __shared__ union {
+        typename Sort::TempStorage sort;
+        typename Scan::TempStorage scan;
+    } tmp;
+    __shared__ uint32_t sorted[CAP];
+    __shared__ uint32_t uniq[CAP];
+    const int64_t b = (int64_t)blockIdx.x * npb;
+    const int nn = (int)(nbl - b < npb ? nbl - b : npb);
+    const int total = nn * K;
+    const float4* rec = stW + b * K;
+    uint32_t keys[PER];
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+        const int e = threadIdx.x * PER + q;
+        keys[q] = e < total ? __float_as_uint(rec[e].w) : 0xFFFFFFFFu;
+    }
+    Sort(tmp.sort).Sort(keys);
+#pragma unroll
+    for (int q = 0; q < PER; ++q) sorted[threadIdx.x * PER + q] = keys[q];
+    __syncthreads();
+    int flag[PER], pos[PER], m = 0;
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+        const int e = threadIdx.x * PER + q;
+        flag[q] = e < total && (e == 0 || sorted[e] != sorted[e - 1]);
+    }
+    Scan(tmp.scan).ExclusiveSum(flag, pos, m);
+#pragma unroll
+    for (int q = 0; q < PER; ++q)
+        if (flag[q]) uniq[pos[q]] = sorted[threadIdx.x * PER + q];
+    __syncthreads();
+    uint32_t* list = reinterpret_cast<uint32_t*>(stH + (int64_t)blockIdx.x * (kHaloBlobBytes / 16));
+    float4* out = stH + (int64_t)blockIdx.x * (kHaloBlobBytes / 16) + kHaloListBytes / 16;
+    const bool local = m <= kHaloCap;
+    for (int e = threadIdx.x; e < 4 + kHaloCap; e += blockDim.x)
+        list[e] = e == 0 ? (uint32_t)m : (e >= 4 && local && e - 4 < m ? uniq[e - 4] : 0u);
+    for (int e = threadIdx.x; e < 32 * K; e += blockDim.x) {
+        float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (e < total) {
+            r = rec[e];
+            if (local) {
+                const uint32_t j = __float_as_uint(r.w);
+                int lo = 0, hi = m - 1;  // j is in the list
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (uniq[mid] < j)
+                        lo = mid + 1;
+                    else
+                        hi = mid;
+                }
+                r.w = __uint_as_float((uint32_t)lo);
+            }
+        }
+        out[e] = r;
+    }
+}
+}  // namespace
+
+int halo_build_device(const float4* stW, int64_t nbl, int k, int npb, float4* stH, cudaStream_t st) {
+    if (k != kHaloK || npb != 32) return set_error(NAGA_EINVAL, "halo blobs: need k = 32 and 32-node passes");
+    if (nbl <= 0) return NAGA_OK;
+    const int64_t n_pass = (nbl + npb - 1) / npb;
+    halo_build_kernel<<<(unsigned)n_pass, 256, 0, st>>>(stW, nbl, npb, stH);
     NAGA_CUDA_TRY(cudaGetLastError());
     return NAGA_OK;
 }
@@ -1471,20 +1760,38 @@ TunedShape tuned_shape(const ShapeKey& key) {
     return f == g_shape.end() ? TunedShape{} : f->second;
 }
 
-// fn(kernel, threads per node) with RK stage STAGE's instantiation for tpn
-// (the unrolled stencil sizes have every RkShapes candidate; the generic
-// K == 0 kernels only the default)
+// fn(kernel, block, dynamic shared memory) with RK stage STAGE's
+// instantiation for the shape code tpn: threads per node (the unrolled
+// stencil sizes have every RkShapes candidate; the generic K == 0 kernels
+// only the default) or kRkHalo (D3Q27 at k = kHaloK)
 template <class L, int K, int STAGE, class Fn>
 int rk_dispatch(int tpn, Fn&& fn) {
+    constexpr size_t s4 = K > 0 ? 0 : 2 * (size_t)MT<L>::NPB * 64 * sizeof(float4);
+    constexpr int NPB = MT<L>::NPB;
     if constexpr (K > 0) {
         if constexpr (L::D == 3) {
-            if (tpn == 7) return fn(k_rk<L, K, STAGE, 7>, 7);
-            if (tpn == 4) return fn(k_rk<L, K, STAGE, 4>, 4);
+            if constexpr (K == kHaloK)
+                if (tpn == kRkHalo) return fn(k_rk_halo<STAGE>, 256, kHaloSmem);
+            if (tpn == 7) return fn(k_rk<L, K, STAGE, 7>, NPB * 7, s4);
+            if (tpn == 4) return fn(k_rk<L, K, STAGE, 4>, NPB * 4, s4);
         } else {
-            if (tpn == 1) return fn(k_rk<L, K, STAGE, 1>, 1);
+            if (tpn == 1) return fn(k_rk<L, K, STAGE, 1>, NPB * 1, s4);
         }
     }
-    return fn(k_rk<L, K, STAGE, MTR<L>::TPN>, MTR<L>::TPN);
+    return fn(k_rk<L, K, STAGE, MTR<L>::TPN>, NPB * MTR<L>::TPN, s4);
+}
+// resident blocks per SM the RK stages of shape code tpn run at for the
+// tuned bps (the halo stages always at their two)
+inline int rk_bps(int tpn, int bps) { return tpn == kRkHalo ? 2 : bps; }
+// the halo shape is offered for D3Q27 at k = kHaloK
+template <class L, int K>
+constexpr bool has_halo() {
+    return L::D == 3 && K == kHaloK;
+}
+// a shape code as the tuner's log names it
+template <class L>
+std::string shape_name(int tpn) {
+    return tpn == kRkHalo ? std::string("halo") : std::to_string(tpn ? tpn : MTR<L>::TPN);
 }
 template <class L, int K, class Fn>
 int rk_each_stage(int tpn, Fn&& fn) {
@@ -1524,7 +1831,9 @@ int apply_shape(const TunedShape& sh) {
     int rc;
     const int bo = other_bps<L>(bps);
     if ((rc = set_blocks_per_sm(k_pml_gather<L, K>, s4, sh.pbps)) ||
-        (rc = rk_each_stage<L, K>(sh.tpn, [&](auto kern, int) { return set_blocks_per_sm(kern, s4, bps); })) ||
+        (rc = rk_each_stage<L, K>(sh.tpn, [&](auto kern, int, size_t sm) {
+             return set_blocks_per_sm(kern, sm, rk_bps(sh.tpn, bps));
+         })) ||
         (rc = set_blocks_per_sm(k_filter<L, K>, s2, sh.fbps)) ||
         (rc = set_blocks_per_sm(k_edge_collide<L, KB>, sb, bo)) ||
         (rc = set_blocks_per_sm(k_edge_interp<L, KB>, sb, bo)))
@@ -1569,7 +1878,7 @@ int enqueue_step_k(const StepLaunch& P, cudaStream_t st) {
     int rc;
     const TunedShape sh = tuned_shape(shape_key(L::D, K, KB, P.n_fluid));
     if ((rc = allow_smem(k_pml_gather<L, K>, s4)) ||
-        (rc = rk_each_stage<L, K>(sh.tpn, [&](auto kern, int) { return allow_smem(kern, s4); })) ||
+        (rc = rk_each_stage<L, K>(sh.tpn, [&](auto kern, int, size_t sm) { return allow_smem(kern, sm); })) ||
         (rc = allow_smem(k_filter<L, K>, s2)) || (rc = allow_smem(k_edge_collide<L, KB>, sb)) ||
         (rc = allow_smem(k_edge_interp<L, KB>, sb)))
         return rc;
@@ -1609,10 +1918,9 @@ int enqueue_step_k(const StepLaunch& P, cudaStream_t st) {
     LAUNCH(K_FILTER, P.n_all_mt,
            keep(launch_step_kernel(k_filter<L, K>, pgrid_b(k_filter<L, K>, s2, P.n_all_mt, FFB, sh.fbps), FFB, s2, st, P.all_mt, P.n_all_mt, P.scenes)));
     // the RK stages at the tuned threads per node
-    auto rk_launch = [&](auto kern, int tpn) {
-        const int blk = MT<L>::NPB * tpn;
-        keep(launch_step_kernel(kern, pgrid_b(kern, s4, P.n_fluid, blk, bps), blk, s4, st, P.fluid, P.n_fluid,
-                                P.scenes));
+    auto rk_launch = [&](auto kern, int blk, size_t sm) {
+        keep(launch_step_kernel(kern, pgrid_b(kern, sm, P.n_fluid, blk, rk_bps(sh.tpn, bps)), blk, sm, st, P.fluid,
+                                P.n_fluid, P.scenes));
         return NAGA_OK;
     };
     LAUNCH(K_RK1, P.n_fluid, (rk_dispatch<L, K, 1>(sh.tpn, rk_launch)));
@@ -1657,11 +1965,12 @@ int tune_k(const StepLaunch& P, cudaStream_t st) {
         const int t = env_tpn ? std::atoi(env_tpn) : 0;
         for (int c = 0; c < RkShapes<L>::n; ++c)
             if (RkShapes<L>::tpn[c] == t && (K > 0 || c == 0)) sh.tpn = c == 0 ? 0 : t;
+        if (env_tpn && std::string(env_tpn) == "halo" && has_halo<L, K>()) sh.tpn = kRkHalo;
         std::lock_guard<std::mutex> lk(g_shape_mu);
         g_shape[key] = sh;
         std::snprintf(line, sizeof line,
-                      "dim %d k %d kb %d items 2^%d: tpn %d bps %d filter bps %d (NAGA_GATHER_BPS / _TPN)\n",
-                      key.dim, key.k, key.kb, key.bucket, sh.tpn ? sh.tpn : MTR<L>::TPN, sh.bps, sh.fbps);
+                      "dim %d k %d kb %d items 2^%d: tpn %s bps %d filter bps %d (NAGA_GATHER_BPS / _TPN)\n",
+                      key.dim, key.k, key.kb, key.bucket, shape_name<L>(sh.tpn).c_str(), sh.bps, sh.fbps);
         g_tune_log += line;
         return NAGA_OK;
     }
@@ -1672,33 +1981,37 @@ int tune_k(const StepLaunch& P, cudaStream_t st) {
     TunedShape best;
     float best_ms = -1.f, best_default_ms = -1.f;
     std::string log;
-    const int ncand = K > 0 ? RkShapes<L>::n : 1;
+    // candidates: the RkShapes thread shapes, then the halo stages (timed at
+    // their own two blocks per SM only; NAGA_RK_HALO=0 leaves them out)
+    const char* env_halo = std::getenv("NAGA_RK_HALO");
+    const bool try_halo = has_halo<L, K>() && !(env_halo && env_halo[0] == '0');
+    const int ncand = (K > 0 ? RkShapes<L>::n : 1) + (try_halo ? 1 : 0);
     for (int ci = 0; ci < ncand && rc == NAGA_OK; ++ci) {
-        const int tpn = ci == 0 ? 0 : RkShapes<L>::tpn[ci];
-        rc = rk_dispatch<L, K, 1>(tpn, [&](auto kern, int t) -> int {
-            const int blk = MT<L>::NPB * t;
+        const bool halo = try_halo && ci == ncand - 1;
+        const int tpn = halo ? kRkHalo : ci == 0 ? 0 : RkShapes<L>::tpn[ci];
+        rc = rk_dispatch<L, K, 1>(tpn, [&](auto kern, int blk, size_t sm) -> int {
             int r;
-            if ((r = allow_smem(kern, s4)) || (r = set_blocks_per_sm(kern, s4, 0))) return r;
+            if ((r = allow_smem(kern, sm)) || (r = set_blocks_per_sm(kern, sm, 0))) return r;
             int maxr = 0;
-            NAGA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxr, kern, blk, s4));
-            maxr = std::max(maxr, 1);
-            std::snprintf(line, sizeof line, " | tpn %d", t);
+            NAGA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxr, kern, blk, sm));
+            maxr = std::max(maxr, halo ? rk_bps(tpn, 0) : 1);
+            std::snprintf(line, sizeof line, " | tpn %s", shape_name<L>(tpn).c_str());
             log += line;
-            for (int bps = 0; bps <= maxr; bps = bps == 0 ? 2 : bps + 1) {
-                if ((r = set_blocks_per_sm(kern, s4, bps))) return r;
+            for (int bps = halo ? rk_bps(tpn, 0) : 0; bps <= maxr; bps = bps == 0 ? 2 : bps + 1) {
+                if ((r = set_blocks_per_sm(kern, sm, bps))) return r;
                 const int g = std::min(P.n_fluid, (bps > 0 ? bps : maxr) * sms);
                 // one untimed and one timed launch; launches shorter than
                 // ~0.4 ms are timed again over enough repetitions to span ~2 ms
                 auto timed = [&](int reps, float* ms) -> bool {
                     cudaEventRecord(e0, st);
-                    for (int q = 0; q < reps; ++q) kern<<<g, blk, s4, st>>>(P.fluid, P.n_fluid, P.scenes);
+                    for (int q = 0; q < reps; ++q) kern<<<g, blk, sm, st>>>(P.fluid, P.n_fluid, P.scenes);
                     cudaEventRecord(e1, st);
                     if (cudaEventSynchronize(e1) != cudaSuccess || cudaGetLastError() != cudaSuccess) return false;
                     cudaEventElapsedTime(ms, e0, e1);
                     *ms /= reps;
                     return true;
                 };
-                kern<<<g, blk, s4, st>>>(P.fluid, P.n_fluid, P.scenes);
+                kern<<<g, blk, sm, st>>>(P.fluid, P.n_fluid, P.scenes);
                 float ms = 0.f, ms2 = 0.f;
                 bool ok = timed(1, &ms);
                 if (ok && ms < 0.4f) ok = timed(std::min(8, std::max(2, (int)(2.f / std::max(ms, 1e-3f)))), &ms);
@@ -1713,7 +2026,9 @@ int tune_k(const StepLaunch& P, cudaStream_t st) {
                 if (is_default) best_default_ms = ms;
                 const bool hopeless = tpn != 0 && bps == 0 && best_ms > 0.f && ms > 1.25f * best_ms;
                 if (best_ms < 0.f || ms < best_ms) {
-                    best.bps = bps;
+                    // the halo stages keep their own carveout; the other
+                    // gather kernels stay at the default
+                    best.bps = halo ? 0 : bps;
                     best.tpn = tpn;
                     best_ms = ms;
                 }
@@ -1725,7 +2040,7 @@ int tune_k(const StepLaunch& P, cudaStream_t st) {
                 }
             }
             // the trials changed this kernel's carveout
-            return set_blocks_per_sm(kern, s4, 0);
+            return set_blocks_per_sm(kern, sm, 0);
         });
     }
     // a non-default shape must beat the default by 3%
@@ -1793,8 +2108,8 @@ int tune_k(const StepLaunch& P, cudaStream_t st) {
     if (rc) return rc;
     std::lock_guard<std::mutex> lk(g_shape_mu);
     g_shape[key] = best;
-    std::snprintf(line, sizeof line, "dim %d k %d kb %d items 2^%d: tpn %d bps %d filter bps %d pml bps %d of",
-                  key.dim, key.k, key.kb, key.bucket, best.tpn ? best.tpn : MTR<L>::TPN, best.bps, best.fbps,
+    std::snprintf(line, sizeof line, "dim %d k %d kb %d items 2^%d: tpn %s bps %d filter bps %d pml bps %d of",
+                  key.dim, key.k, key.kb, key.bucket, shape_name<L>(best.tpn).c_str(), best.bps, best.fbps,
                   best.pbps);
     g_tune_log += line + log + "\n";
     return NAGA_OK;

@@ -177,8 +177,13 @@ import sys, numpy as np
 sys.path.insert(0, {root!r})
 import naga_b200 as naga
 out = []
-for dim, n, k in ((3, 20, 32), (2, 48, 16)):
+for dim, n, k, scramble in ((3, 20, 32, False), (2, 48, 16, False), (3, 20, 32, True)):
     g = naga.generate_grid(dim, n, 3, 4)
+    if scramble:
+        # bulk nodes in random order: a pass's supports are scattered and
+        # most passes list more rows than the halo stages keep
+        perm = np.random.default_rng(5).permutation(g["n_bulk"])
+        g["points"][: g["n_bulk"]] = g["points"][perm]
     pr = np.array({probes3!r} if dim == 3 else {probes2!r}, np.float32)
     s = naga.Scene(g, k=k, shape=0 if dim == 3 else 1, probes=pr)
     s.set_density(naga.gaussian_pulse(g["points"], [0.5] * dim, 1e-3, 0.05))
@@ -191,18 +196,20 @@ print(naga.tuning_report())
 
 def test_launch_shape_does_not_change_results(tmp_path):
     """The tuner's choices -- resident blocks per SM of the gather kernels, of
-    the filter, and threads per node of the RK stages -- change only the
-    launch: runs with
-    the tuned shape and with shapes forced through NAGA_GATHER_BPS /
-    NAGA_GATHER_TPN (D3Q27 at 7 and 4 threads per node, D2Q9 at 1) agree bit
-    for bit, and the tuner logs what it measured."""
+    the filter, threads per node of the RK stages, and the shared-memory halo
+    RK stages -- change only the launch: runs with the tuned shape and with
+    shapes forced through NAGA_GATHER_BPS / NAGA_GATHER_TPN (D3Q27 at 7 and 4
+    threads per node and with the halo stages, D2Q9 at 1) agree bit for bit,
+    on Morton-ordered scenes and on one with its bulk nodes scrambled (whose
+    passes overflow the halo list and gather from global memory), and the
+    tuner logs what it measured."""
     import os
     import subprocess
     import sys
 
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     outs, logs = [], []
-    for env_bps, env_tpn in ((None, None), ("2", None), (None, "7"), ("3", "4"), (None, "1")):
+    for env_bps, env_tpn in ((None, None), ("2", None), (None, "7"), ("3", "4"), (None, "1"), (None, "halo")):
         out = str(tmp_path / f"run_{env_bps}_{env_tpn}.npy")
         env = dict(os.environ)
         env.pop("NAGA_GATHER_BPS", None)
@@ -224,6 +231,8 @@ def test_launch_shape_does_not_change_results(tmp_path):
     assert "dim 3 k 32 kb 32 items 2^" in logs[2] and "tpn 7 bps 0 filter bps 0 (NAGA_GATHER" in logs[2]
     assert "tpn 4 bps 3 filter bps" in logs[3]
     assert "dim 2 k 16 kb 16 items 2^" in logs[4] and "tpn 1 bps 0 filter bps 0 (NAGA_GATHER" in logs[4]
+    assert "| tpn halo 2:" in logs[0]
+    assert "dim 3 k 32 kb 32 items 2^" in logs[5] and "tpn halo bps 0 filter bps 0 (NAGA_GATHER" in logs[5]
 
 
 def test_async_probe_reads_match_synchronous(naga, oracle):
