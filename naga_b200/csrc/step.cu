@@ -1680,9 +1680,15 @@ template <class L, int K, class T>
 size_t tile_bytes() {
     return K > 0 ? 0 : 2 * (size_t)MT<L>::NPB * 64 * sizeof(T);
 }
+// opts a kernel into `bytes` of dynamic shared memory when its static plus
+// dynamic shared memory exceeds the 48 KB a launch gets without opting in
 template <class Kern>
 int allow_smem(Kern kern, size_t bytes) {
-    if (bytes > 48 * 1024) NAGA_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    if (bytes == 0) return NAGA_OK;
+    cudaFuncAttributes fa{};
+    NAGA_CUDA_TRY(cudaFuncGetAttributes(&fa, kern));
+    if (fa.sharedSizeBytes + bytes > 48 * 1024)
+        NAGA_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
     return NAGA_OK;
 }
 
@@ -1987,6 +1993,7 @@ int tune_k(const StepLaunch& P, cudaStream_t st) {
     cudaEvent_t e0, e1;
     NAGA_CUDA_TRY(cudaEventCreate(&e0));
     NAGA_CUDA_TRY(cudaEventCreate(&e1));
+    cudaError_t terr = cudaSuccess;  // the error of a failed trial
     TunedShape best;
     float best_ms = -1.f, best_default_ms = -1.f;
     std::string log;
@@ -2015,7 +2022,9 @@ int tune_k(const StepLaunch& P, cudaStream_t st) {
                     cudaEventRecord(e0, st);
                     for (int q = 0; q < reps; ++q) kern<<<g, blk, sm, st>>>(P.fluid, P.n_fluid, P.scenes);
                     cudaEventRecord(e1, st);
-                    if (cudaEventSynchronize(e1) != cudaSuccess || cudaGetLastError() != cudaSuccess) return false;
+                    terr = cudaEventSynchronize(e1);
+                    if (terr == cudaSuccess) terr = cudaGetLastError();
+                    if (terr != cudaSuccess) return false;
                     cudaEventElapsedTime(ms, e0, e1);
                     *ms /= reps;
                     return true;
@@ -2028,7 +2037,9 @@ int tune_k(const StepLaunch& P, cudaStream_t st) {
                 // scene set-up) can slow a single trial
                 const int reps2 = ms < 0.4f ? std::min(8, std::max(2, (int)(2.f / std::max(ms, 1e-3f)))) : 1;
                 if (ok && timed(reps2, &ms2)) ms = std::min(ms, ms2);
-                if (!ok) return set_error(NAGA_ECUDA, "launch-shape tuning: a trial launch failed");
+                if (!ok)
+                    return set_error(NAGA_ECUDA,
+                                     std::string("launch-shape tuning: a trial launch failed: ") + cudaGetErrorString(terr));
                 std::snprintf(line, sizeof line, " %d:%.1fus", bps, ms * 1000.f);
                 log += line;
                 const bool is_default = tpn == 0 && bps == 0;
@@ -2081,7 +2092,9 @@ int tune_k(const StepLaunch& P, cudaStream_t st) {
                 cudaEventRecord(e0, st);
                 for (int q = 0; q < reps; ++q) kern<<<g, block, smem, st>>>(list, n, P.scenes);
                 cudaEventRecord(e1, st);
-                if (cudaEventSynchronize(e1) != cudaSuccess || cudaGetLastError() != cudaSuccess) return false;
+                terr = cudaEventSynchronize(e1);
+                if (terr == cudaSuccess) terr = cudaGetLastError();
+                if (terr != cudaSuccess) return false;
                 cudaEventElapsedTime(ms, e0, e1);
                 *ms /= reps;
                 return true;
@@ -2092,7 +2105,8 @@ int tune_k(const StepLaunch& P, cudaStream_t st) {
             const int reps2 = ms < 0.4f ? std::min(8, std::max(2, (int)(2.f / std::max(ms, 1e-3f)))) : 1;
             if (ok && timed(reps2, &ms2)) ms = std::min(ms, ms2);
             if (!ok) {
-                rc = set_error(NAGA_ECUDA, "launch-shape tuning: a trial launch failed");
+                rc = set_error(NAGA_ECUDA,
+                               std::string("launch-shape tuning: a trial launch failed: ") + cudaGetErrorString(terr));
                 return;
             }
             std::snprintf(line, sizeof line, " %d:%.1fus", bps, ms * 1000.f);
