@@ -546,12 +546,28 @@ __global__ void __launch_bounds__(kBlock, (L::D == 3 ? 4 : 8)) k_macro_pml(const
     const float sf = field ? __ldg(S.sigma + (jf - S.nb)) : 0.f;
     const bool src = active && i < S.nbl && S.is_src[i];
     {
+        // copied with cp.async (16 B a thread and copy, no register staging),
+        // all of the thread's copies in flight at once
         const float4* g4 = reinterpret_cast<const float4*>(S.G + (int64_t)it.begin * QP);
         const float4* q4 = reinterpret_cast<const float4*>(Q1prev + (int64_t)it.begin * QP);
-        for (int e = threadIdx.x; e < nn * QP / 4; e += blockDim.x) {
-            rowG[e] = g4[e];
-            rowQ[e] = q4[e];
+        constexpr int NQ = QP / 4;  // float4 per row: the block moves kBlock * NQ of each
+        const int ne = nn * NQ;
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            const int e = (int)threadIdx.x + q * kBlock;
+            if (e < ne) {
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                                 (uint32_t)__cvta_generic_to_shared(rowG + e)),
+                             "l"(g4 + e)
+                             : "memory");
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                                 (uint32_t)__cvta_generic_to_shared(rowQ + e)),
+                             "l"(q4 + e)
+                             : "memory");
+            }
         }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
     }
     __syncthreads();
     float* myG = reinterpret_cast<float*>(rowG) + threadIdx.x * QP;
