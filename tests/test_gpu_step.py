@@ -132,6 +132,51 @@ def test_batch_equals_individual_scenes(naga, oracle, priority):
     b.close()
 
 
+_BATCH3_RUN = """
+import sys, numpy as np
+sys.path.insert(0, {root!r})
+import naga_b200 as naga
+pr = np.array({probes3!r}, np.float32)
+gs = [naga.generate_grid(3, n, 3, s) for n, s in ((14, 1), (17, 2), (15, 3))]
+solo, members = [], []
+for g in gs:
+    for lst in (solo, members):
+        s = naga.Scene(g, k=32, shape=0, probes=pr)
+        s.set_density(naga.gaussian_pulse(g["points"], [0.5] * 3, 1e-3, 0.08))
+        lst.append(s)
+b = naga.Batch(3)
+for s in members:
+    b.add(s)
+b.step(12)
+for s in solo:
+    s.step(12)
+ok = all(np.array_equal(a.probes(0, 12), m.probes(0, 12)) and np.array_equal(a.state()[0], m.state()[0])
+         for a, m in zip(solo, members))
+b.close()
+print("equal" if ok else "differ")
+print(naga.tuning_report())
+"""
+
+
+def test_batch_of_3d_scenes_with_halo_stages(tmp_path):
+    """A batch of three D3Q27 scenes at k = 32 takes the same steps as each
+    scene alone, bit for bit, with the shared-memory halo RK stages forced:
+    their passes switch between the scenes' blobs and rows."""
+    import os
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ)
+    env["NAGA_GATHER_TPN"] = "halo"
+    env.pop("NAGA_GATHER_BPS", None)
+    code = _BATCH3_RUN.format(root=root, probes3=PROBES3.tolist())
+    r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.startswith("equal"), r.stdout
+    assert "tpn halo" in r.stdout
+
+
 def test_batch_membership_changes(naga, oracle):
     """Scenes leave and join a stepping batch (its item tables are rebuilt
     in place on the device); every scene's trace still equals the same
