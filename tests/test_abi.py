@@ -116,3 +116,25 @@ def test_library_lattice_matches_oracle(naga, oracle, dim):
     oc, ow, _, _ = oracle.lattice(dim)
     assert np.array_equal(c, oc.astype(np.int32))
     assert np.allclose(w, ow, rtol=0, atol=1e-7)
+
+
+def test_scene_estimate_counts_the_halo_lists(naga):
+    """The admission estimate grows linearly with k (stencil records), except
+    at k = 32 in 3-D, where the scene also holds the halo lists of its RK
+    stages: 17,488 B per 32-node bulk/layer pass."""
+    import ctypes as C
+
+    g = naga.generate_grid(3, 20, 3, 1)
+    est = {}
+    for k in (31, 32, 33):
+        d, keep = naga.scene_desc(g, k=k)
+        est[k] = naga.lib().naga_scene_estimate_bytes(C.byref(d))
+    passes = (g["n_bulk"] + g["n_layer"] + 31) // 32
+    linear = (est[31] + est[33]) // 2
+    assert est[32] - linear == 17488 * passes
+    g2 = naga.generate_grid(2, 30, 3, 1)
+    e2 = {}
+    for k in (31, 32, 33):
+        d, keep = naga.scene_desc(g2, k=k)
+        e2[k] = naga.lib().naga_scene_estimate_bytes(C.byref(d))
+    assert e2[32] * 2 == e2[31] + e2[33]
