@@ -225,10 +225,15 @@ out = []
 for dim, n, k, scramble in ((3, 20, 32, False), (2, 48, 16, False), (3, 20, 32, True)):
     g = naga.generate_grid(dim, n, 3, 4)
     if scramble:
-        # bulk nodes in random order: a pass's supports are scattered and
-        # most passes list more rows than the halo stages keep
-        perm = np.random.default_rng(5).permutation(g["n_bulk"])
+        # bulk and boundary nodes in random order: a pass's supports are
+        # scattered and most passes list more rows than the halo stages keep
+        rng = np.random.default_rng(5)
+        perm = rng.permutation(g["n_bulk"])
         g["points"][: g["n_bulk"]] = g["points"][perm]
+        b0 = g["n_bulk"] + g["n_layer"]
+        pb = rng.permutation(g["n_boundary"])
+        g["points"][b0 : b0 + g["n_boundary"]] = g["points"][b0 + pb]
+        g["normals"] = np.ascontiguousarray(g["normals"][pb])
     pr = np.array({probes3!r} if dim == 3 else {probes2!r}, np.float32)
     s = naga.Scene(g, k=k, shape=0 if dim == 3 else 1, probes=pr)
     s.set_density(naga.gaussian_pulse(g["points"], [0.5] * dim, 1e-3, 0.05))
