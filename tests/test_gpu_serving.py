@@ -66,6 +66,44 @@ def test_results_alone_equal_results_in_the_mix(naga):
     assert np.array_equal(s.probes(0, steps[2]), alone[2])
 
 
+PROBES3 = np.array([[0.35, 0.5, 0.5], [0.65, 0.5, 0.5]], np.float32)
+
+
+def test_3d_results_alone_equal_results_in_the_mix(naga):
+    """D3Q27 requests at k = 32 (the benchmark's lattice and stencil size:
+    halo lists built on the set-up thread, steps in a growing 3-D batch)
+    give the same probe traces alone, in the mix and as a plain scene."""
+    reqs = []
+    for n, seed, width in ((14, 1, 0.08), (17, 2, 0.1), (15, 3, 0.09)):
+        g = naga.generate_grid(3, n, 3, seed)
+        reqs.append((g, naga.gaussian_pulse(g["points"], [0.5] * 3, 1e-3, width)))
+    steps = [24, 16, 30]
+    kw = dict(k=32, shape=0, probes=PROBES3)
+    alone = []
+    for (g, d), n in zip(reqs, steps):
+        srv = naga.Server(3, memory_budget=1 << 31, steps_per_tick=8)
+        rid = srv.submit(g, d, n, **kw)
+        _run_until_done(srv, [rid])
+        alone.append(srv.result(rid))
+        srv.close()
+    srv = naga.Server(3, memory_budget=1 << 31, steps_per_tick=8, max_active=3)
+    ids = [srv.submit(reqs[0][0], reqs[0][1], steps[0], **kw)]
+    deadline = time.time() + 60
+    while time.time() < deadline and srv.stats()["ticks"] < 2:
+        _tick(srv)
+    ids += [srv.submit(g, d, n, **kw) for (g, d), n in zip(reqs[1:], steps[1:])]
+    _run_until_done(srv, ids)
+    st = srv.stats()
+    assert st["done"] == 3 and st["failed"] == 0
+    for rid, a in zip(ids, alone):
+        assert np.array_equal(srv.result(rid), a)
+    srv.close()
+    s = naga.Scene(reqs[1][0], **kw)
+    s.set_density(reqs[1][1])
+    s.step(steps[1])
+    assert np.array_equal(s.probes(0, steps[1]), alone[1])
+
+
 def test_admission_by_memory_budget(naga):
     g, d = _req(naga, 40, 5, 0.06)
     desc, _ = naga.scene_desc(g, k=16, probes=PROBES2, probe_capacity=40)
