@@ -1271,7 +1271,9 @@ __global__ void __launch_bounds__(256, 2) k_rk_halo(const WorkItem* __restrict__
     unsigned char* const blobs = dyn_smem;
     float4* const halo = reinterpret_cast<float4*>(dyn_smem + NB * BLOB);
     __shared__ __align__(8) uint64_t bar[NB];
-    __shared__ SceneDev S;
+    // the scenes of the pass being computed and of the next one (pass t uses
+    // S2[t % 2]), so the next pass's scene loads without a barrier
+    __shared__ SceneDev S2[2];
     const int c = threadIdx.x % TPN, ns = threadIdx.x / TPN;
     if (threadIdx.x == 0) {
         for (int b = 0; b < NB; ++b) mbar_init(&bar[b]);
@@ -1342,6 +1344,11 @@ __global__ void __launch_bounds__(256, 2) k_rk_halo(const WorkItem* __restrict__
         if (T > 0) issue_blob(w0, 0);
         if (T > 1) issue_blob(w1, 1);
     }
+    uint32_t scene_even = 0xFFFFFFFFu, scene_odd = 0xFFFFFFFFu;  // the scenes in S2[0], S2[1]
+    if (T > 0) {
+        scene_even = w0.scene;
+        load_scene(S2[0], scenes + w0.scene);
+    }
     pdl_wait_prev();
     if (T > 0) {
         wait_blob(0);
@@ -1350,26 +1357,28 @@ __global__ void __launch_bounds__(256, 2) k_rk_halo(const WorkItem* __restrict__
     cp_async_commit();
     float d0[3], d1[3];
     pair_dirs<L>(c < NCH ? c : 0, d0, d1);
-    uint32_t cur_scene = 0xFFFFFFFFu;
+    // one barrier a pass: after it, this pass's rows are in shared memory and
+    // every thread is done with pass t - 1, whose blob, halo and scene
+    // buffers the copies for passes t + 1 and t + 2 then reuse
     for (int t = 0; t < T; ++t) {
         const WorkItem w3 = item_of(t + 3);
-        // the previous pass is done with S, its blob and its halo buffer
-        __syncthreads();
-        if (w0.scene != cur_scene) {
-            cur_scene = w0.scene;
-            load_scene(S, scenes + w0.scene);
+        cp_async_wait<0>();  // this pass's rows (this thread's copies)
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) atomicOr(&g_tile_timeout, 1u);
+            break;
         }
         if (threadIdx.x == 0 && t + 2 < T) issue_blob(w2, t + 2);
         if (t + 1 < T) {
             wait_blob(t + 1);
             if (ok) issue_rows(w1, t + 1);
+            uint32_t& held = ((t + 1) & 1) ? scene_odd : scene_even;
+            if (w1.scene != held) {
+                held = w1.scene;
+                load_scene(S2[(t + 1) & 1], scenes + w1.scene);
+            }
         }
         cp_async_commit();
-        cp_async_wait<1>();  // this pass's rows (committed one pass ago)
-        if (__syncthreads_or(!ok)) {
-            if (threadIdx.x == 0) atomicOr(&g_tile_timeout, 1u);
-            break;
-        }
+        const SceneDev& S = S2[t & 1];
         const unsigned char* blob = blobs + (t % NB) * BLOB;
         const uint32_t m = reinterpret_cast<const uint32_t*>(blob)[0];
         const float4* tile = reinterpret_cast<const float4*>(blob + kHaloListBytes);
