@@ -776,6 +776,11 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int po
     return false;
 }
 
+// a plain arrive (release) on a count-1 barrier: completes its phase
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 }  // namespace
 
 // set (never cleared by the kernels) when a tile wait ran out: the step
@@ -818,11 +823,18 @@ constexpr int tile_cap() {
 
 // Item loop of the gather kernels. SRC(scene, item) names the item's table
 // block (TileSrc); inside the loop, `S` is the item's scene, `it` the item
-// and `tile` its records.
+// and `tile` its records. One block barrier an item: right after it, the
+// next item's table block (bulk copy) and scene (shared slot) go into the
+// previous item's buffers, and every thread waits for that block at the end
+// of the current item, so the next barrier also checks the waits. An item
+// whose table block cannot be bulk-copied (empty, or larger than a tile
+// buffer) completes its buffer's phase with a plain arrive, which also
+// publishes the block's mode; the block then copies what fits of it after
+// the barrier.
 #define NAGA_PIPE_BEGIN(T, CAP, SRC)                                                                   \
-    __shared__ SceneDev S;                                                                             \
+    __shared__ SceneDev pipe_S_[2];                                                                    \
     __shared__ __align__(8) uint64_t pipe_bar_[2];                                                     \
-    __shared__ int pipe_bulk_[2];                                                                      \
+    __shared__ int pipe_mode_[2]; /* 0 bulk-copied, 1 copied after the barrier, 2 empty */             \
     T* const pipe_buf_ = tile_pair<T, G::NPB, K_>();                                                   \
     if (threadIdx.x == 0) {                                                                            \
         mbar_init(&pipe_bar_[0]);                                                                      \
@@ -830,47 +842,61 @@ constexpr int tile_cap() {
         mbar_init_fence();                                                                             \
     }                                                                                                  \
     __syncthreads();                                                                                   \
-    auto pipe_issue_ = [&](int w, int b) {                                                             \
-        const WorkItem itn = items[w];                                                                 \
+    auto pipe_issue_ = [&](const WorkItem& itn, int b) {                                               \
         const TileSrc ts = SRC(scenes[itn.scene], itn);                                                \
         const bool bulk = ts.bytes > 0 && ts.bytes % 16 == 0 && ((uintptr_t)ts.p & 15) == 0 &&         \
                           ts.bytes <= (uint32_t)(CAP * sizeof(T));                                     \
-        pipe_bulk_[b] = bulk;                                                                          \
-        if (bulk) bulk_load(pipe_buf_ + b * (CAP), ts.p, ts.bytes, &pipe_bar_[b]);                      \
+        pipe_mode_[b] = bulk ? 0 : (ts.bytes > 0 ? 1 : 2);                                             \
+        if (bulk)                                                                                      \
+            bulk_load(pipe_buf_ + b * (CAP), ts.p, ts.bytes, &pipe_bar_[b]);                           \
+        else                                                                                           \
+            mbar_arrive(&pipe_bar_[b]);                                                                \
     };                                                                                                 \
     uint32_t pipe_par_ = 0;                                                                            \
-    if (threadIdx.x == 0 && (int)blockIdx.x < nitems) pipe_issue_(blockIdx.x, 0);                      \
+    bool pipe_ok_ = true;                                                                              \
+    auto pipe_wait_ = [&](int b) {                                                                     \
+        if (!pipe_ok_) return;                                                                         \
+        pipe_ok_ = mbar_wait(&pipe_bar_[b], (pipe_par_ >> b) & 1u);                                    \
+        if (pipe_ok_) pipe_par_ ^= 1u << b;                                                            \
+    };                                                                                                 \
+    WorkItem pipe_it_ = (int)blockIdx.x < nitems ? items[blockIdx.x] : WorkItem{0u, 0u, 0u, 0u};       \
+    if ((int)blockIdx.x < nitems) {                                                                    \
+        if (threadIdx.x == 0) pipe_issue_(pipe_it_, 0);                                                \
+        load_scene(pipe_S_[0], scenes + pipe_it_.scene);                                               \
+    }                                                                                                  \
     pdl_wait_prev();                                                                                   \
+    if ((int)blockIdx.x < nitems) pipe_wait_(0);                                                       \
     int pipe_t_ = 0;                                                                                   \
     for (int w_ = blockIdx.x; w_ < nitems; w_ += gridDim.x, ++pipe_t_) {                               \
         const int b_ = pipe_t_ & 1;                                                                    \
-        const WorkItem it = items[w_];                                                                 \
-        __syncthreads();                                                                               \
-        load_scene(S, scenes + it.scene);                                                              \
+        const WorkItem it = pipe_it_;                                                                  \
         const bool more_ = w_ + (int)gridDim.x < nitems;                                               \
-        if (threadIdx.x == 0 && more_) pipe_issue_(w_ + gridDim.x, b_ ^ 1);                            \
-        __syncthreads();                                                                               \
-        T* const tile = pipe_buf_ + b_ * (CAP);                                                        \
-        if (pipe_bulk_[b_]) {                                                                          \
-            const bool ok_ = mbar_wait(&pipe_bar_[b_], (pipe_par_ >> b_) & 1u);                        \
-            pipe_par_ ^= 1u << b_;                                                                     \
-            if (__syncthreads_or(!ok_)) {                                                              \
-                if (threadIdx.x == 0) {                                                                \
-                    atomicOr(&g_tile_timeout, 1u);                                                     \
-                    if (more_ && pipe_bulk_[b_ ^ 1])                                                   \
-                        mbar_wait(&pipe_bar_[b_ ^ 1], (pipe_par_ >> (b_ ^ 1)) & 1u);                   \
-                }                                                                                      \
-                return;                                                                                \
+        if (__syncthreads_or(!pipe_ok_)) {                                                             \
+            if (threadIdx.x == 0) {                                                                    \
+                atomicOr(&g_tile_timeout, 1u);                                                         \
+                mbar_wait(&pipe_bar_[b_], (pipe_par_ >> b_) & 1u); /* the copy still in flight */      \
             }                                                                                          \
-        } else {                                                                                       \
+            return;                                                                                    \
+        }                                                                                              \
+        if (more_) {                                                                                   \
+            pipe_it_ = items[w_ + gridDim.x];                                                          \
+            if (threadIdx.x == 0) pipe_issue_(pipe_it_, b_ ^ 1);                                       \
+            load_scene(pipe_S_[b_ ^ 1], scenes + pipe_it_.scene);                                      \
+        }                                                                                              \
+        const SceneDev& S = pipe_S_[b_];                                                               \
+        T* const tile = pipe_buf_ + b_ * (CAP);                                                        \
+        if (pipe_mode_[b_] == 1) {                                                                     \
             TileSrc ts_ = SRC(S, it);                                                                  \
             if (ts_.bytes > (uint32_t)((CAP) * sizeof(T))) ts_.bytes = (uint32_t)((CAP) * sizeof(T));  \
             copy_tile(tile, ts_);                                                                      \
             __syncthreads();                                                                           \
-        }
+        }                                                                                              \
+        {
 
-#define NAGA_PIPE_END \
-    }                     \
+#define NAGA_PIPE_END                   \
+        }                               \
+        if (more_) pipe_wait_(b_ ^ 1);  \
+    }                                   \
     pdl_allow_next();
 
 // table blocks of the gather kernels
@@ -1060,7 +1086,7 @@ __global__ void __launch_bounds__(MTF<L>::BLOCK, 5) k_edge_collide(const WorkIte
 // the result written into the interpolation-source scratch S1P (dead between
 // steps: the next step's node-local kernel rewrites it) instead of the state
 template <class L, int K, bool DRY = false>
-__global__ void __launch_bounds__(MTFF<L>::BLOCK) k_filter(const WorkItem* __restrict__ items, int nitems,
+__global__ void __launch_bounds__(MTFF<L>::BLOCK, (L::D == 3 ? 6 : 12)) k_filter(const WorkItem* __restrict__ items, int nitems,
                                                            const SceneDev* __restrict__ scenes) {
     using G = MTFF<L>;
     // D2Q9: slot of the rest population (chunk NGATHER, first float)
