@@ -129,6 +129,20 @@ def kernel_bytes(dim, N, nb, nl, nbd, k, kb, pml=None):
     }
 
 
+def gather_bytes(nb, nl, nbd, k, kb, pml):
+    """Bytes the neighbour-row loads of each D3Q27 gather kernel move into the
+    SMs per launch: one 112-B row per (node, stencil support) reference --
+    from L2 in the L2-form kernels, from shared memory in the halo RK stages
+    (whose L2 traffic is each pass's distinct rows once). Beside the DRAM
+    fraction it shows the load the gather path carries: a kernel low on the
+    HBM roofline may still move several times the HBM bandwidth in rows."""
+    row = 4 * 28
+    nbl = nb + nl
+    rk = nbl * k * row
+    return {"pml_gather": pml[1] * row, "edge_collide": nbd * kb * row, "filter": nbl * k * row,
+            "rk_stage1": rk, "rk_stage2": rk, "rk_stage3": rk, "rk_stage4": rk, "edge_interp": nbd * kb * row}
+
+
 def batch_roofline(naga, scenes, prof, peak):
     """Roofline of the batch's longest step kernel: its algorithmic bytes
     summed over the member scenes per launch, over its mean launch time."""
@@ -613,7 +627,9 @@ def run_naga(args, rank, world, local_rank):
 
     # ---- per-kernel timing (CUDA events around each launch, separate run)
     prof = profile_kernels(naga, lambda: scene.step(1), steps=5)
-    kb = kernel_bytes(3, N, g["n_bulk"], g["n_layer"], g["n_boundary"], cfg["k"], cfg["k"], pml_counts(naga, scene))
+    pmlc = pml_counts(naga, scene)
+    kb = kernel_bytes(3, N, g["n_bulk"], g["n_layer"], g["n_boundary"], cfg["k"], cfg["k"], pmlc)
+    gb = gather_bytes(g["n_bulk"], g["n_layer"], g["n_boundary"], cfg["k"], cfg["k"], pmlc)
     step_ms = sum(ms for (_, ms) in prof.values()) / 5
     top = max(kb, key=lambda n: prof.get(n, (0, 0.0))[1])
     launches, tot = prof[top]
@@ -631,7 +647,12 @@ def run_naga(args, rank, world, local_rank):
             # every step kernel's algorithmic bytes / its launch time / peak
             "kernel_fracs": {n: round(kb[n] / (prof[n][1] / prof[n][0] * 1e-3) / 1e9 / peak, 3)
                              for n in kb if prof.get(n, (0, 0.0))[0]},
-            "step_frac": sum(kb.values()) / (step_ms * 1e-3) / 1e9 / peak}
+            "step_frac": sum(kb.values()) / (step_ms * 1e-3) / 1e9 / peak,
+            # neighbour-row bytes each gather kernel's loads move into the
+            # SMs (L2 or shared memory) per launch, and their rate
+            "gather": {"unit": "GB/s", "row_bytes_per_launch": gb,
+                       "achieved": {n: round(gb[n] / (prof[n][1] / prof[n][0] * 1e-3) / 1e9)
+                                    for n in gb if prof.get(n, (0, 0.0))[0]}}}
     gpu_launches = sum(l for (l, _) in prof.values()) // 5 * K
 
     cb = None
