@@ -2,9 +2,13 @@
 //
 // HBM layout of a scene with N nodes (order: bulk [0, nb), layer
 // [nb, nb + nl), boundary [nbl, nbl + nbd), ghost [.., N)):
-//   populations   G, G1, G2, S1, S1P: node-major rows of QP floats
-//                 (QP = 28 for D3Q27, 12 for D2Q9), centred: g = f - w,
-//                 populations in paired slot order (common.cuh)
+//   populations   centred g = f - w, populations in paired slot order
+//                 (common.cuh). G: node-major rows of QP floats (QP = 28
+//                 for D3Q27, 12 for D2Q9); RK stage buffers G1, G2: rows of
+//                 the gathered chunks (QS floats: 28, 8); collision scratch
+//                 S1, S1P: D3Q27 rows of QP floats, D2Q9 rows of the 8
+//                 moving populations followed by the N rest populations
+//                 (s1_ld in step.cu)
 //   Q1a, Q1b      PML trapezoid integrals, rows of QP floats, ping-pong
 //                 by step parity
 //   PHI           rows of the layer nodes' PML field -2 sigma Q1 + sigma^2 Q2

@@ -148,6 +148,44 @@ __device__ __forceinline__ void store_row(float* base, int64_t i, const float* v
 __device__ __forceinline__ float4 ld4(const float* base, int64_t i, int qp, int c) {
     return __ldg(reinterpret_cast<const float4*>(base + i * qp) + c);
 }
+
+// The collision scratch S1, S1P of a scene of n nodes. D3Q27: node-major
+// rows of QP floats like G. D2Q9: rows of the eight moving populations
+// (32 B: one sector per neighbour gather instead of two for a 48-B row),
+// the rest population of node i at 8 n + i. Chunk c of node i as a float4;
+// D2Q9's chunk 2 carries the rest population in x (its other lanes zero).
+template <class L>
+__device__ __forceinline__ float4 s1_ld(const float* base, int64_t n, int64_t i, int c) {
+    if constexpr (L::D == 2) {
+        if (c >= L::NGATHER) return make_float4(base[L::QS * n + i], 0.f, 0.f, 0.f);
+        return reinterpret_cast<const float4*>(base + i * L::QS)[c];
+    } else {
+        return reinterpret_cast<const float4*>(base + i * L::QP)[c];
+    }
+}
+template <class L>
+__device__ __forceinline__ void s1_st(float* base, int64_t n, int64_t i, int c, const float4& v) {
+    if constexpr (L::D == 2) {
+        if (c >= L::NGATHER)
+            base[L::QS * n + i] = v.x;
+        else
+            reinterpret_cast<float4*>(base + i * L::QS)[c] = v;
+    } else {
+        reinterpret_cast<float4*>(base + i * L::QP)[c] = v;
+    }
+}
+// the whole row (slot order, QP floats of which the pads are not stored)
+template <class L>
+__device__ __forceinline__ void s1_store_row(float* base, int64_t n, int64_t i, const float* v) {
+    if constexpr (L::D == 2) {
+        float4* p = reinterpret_cast<float4*>(base + i * L::QS);
+#pragma unroll
+        for (int c = 0; c < L::NGATHER; ++c) p[c] = make_float4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
+        base[L::QS * n + i] = v[L::QS];
+    } else {
+        store_row<L>(base, i, v);
+    }
+}
 // neighbour-row gathers cached in L2 only (.cg): the rows of a pass's
 // neighbours are re-read by other passes long after L1 would have evicted
 // them, and allocating them in L1 costs more than it saves (D3Q27 RK gather:
@@ -174,6 +212,16 @@ __device__ __forceinline__ float4 ld4s(const float* base, int64_t i, int c) {
         return ld4cg(base, i, L::QS, c);
     else
         return __ldg(reinterpret_cast<const float4*>(base + i * L::QS) + c);
+}
+// the gather load of chunk c of a collision scratch row (s1_ld's layout)
+template <class L>
+__device__ __forceinline__ float4 s1_ldg(const float* base, int64_t n, int64_t j, int c) {
+    if constexpr (L::D == 2) {
+        if (c >= L::NGATHER) return make_float4(__ldg(base + L::QS * n + j), 0.f, 0.f, 0.f);
+        return __ldg(reinterpret_cast<const float4*>(base + j * L::QS) + c);
+    } else {
+        return ld4g<L>(base, j, c);
+    }
 }
 __device__ __forceinline__ float4 ld4rw(const float* base, int64_t i, int qp, int c) {
     return reinterpret_cast<const float4*>(base + i * qp)[c];
@@ -622,14 +670,14 @@ __global__ void __launch_bounds__(kBlock, (L::D == 3 ? 4 : 8)) k_macro_pml(const
             for (int c = 0; c < L::QS / 4; ++c)
                 pr[c] = make_float4(phi[4 * c], phi[4 * c + 1], phi[4 * c + 2], phi[4 * c + 3]);
         }
-        if (src) store_row<L>(S.S1P, i, out);
+        if (src) s1_store_row<L>(S.S1P, S.N, i, out);
         const bool boundary = i >= S.nbl && i < S.nbl + S.nbd;
 #pragma unroll
         for (int a = 0; a < Q; ++a) {
             const int t = L::pos(a);
             out[t] = boundary ? dcol[a] : out[t] + dcol[a];
         }
-        store_row<L>(S.S1, i, out);
+        s1_store_row<L>(S.S1, S.N, i, out);
     } else {
 #pragma unroll
         for (int t = 0; t < QP; ++t) myG[t] = myQ[t] = 0.f;
@@ -1013,11 +1061,11 @@ __global__ void __launch_bounds__(MTR<L>::BLOCK) k_pml_gather(const WorkItem* __
         dv.y -= 2.f * m1.y * e1 - m2.y * e2;
         dv.z += 2.f * m1.z * f1 - m2.z * f2;
         dv.w -= 2.f * m1.w * f1 - m2.w * f2;
-        const float4 o = ld4rw(S.S1, i, QP, c);
-        st4(S.S1, i, QP, c, make_float4(o.x + dv.x, o.y + dv.y, o.z + dv.z, o.w + dv.w));
+        const float4 o = s1_ld<L>(S.S1, S.N, i, c);
+        s1_st<L>(S.S1, S.N, i, c, make_float4(o.x + dv.x, o.y + dv.y, o.z + dv.z, o.w + dv.w));
         if (S.is_src[i]) {
-            const float4 q = ld4rw(S.S1P, i, QP, c);
-            st4(S.S1P, i, QP, c, make_float4(q.x + dv.x, q.y + dv.y, q.z + dv.z, q.w + dv.w));
+            const float4 q = s1_ld<L>(S.S1P, S.N, i, c);
+            s1_st<L>(S.S1P, S.N, i, c, make_float4(q.x + dv.x, q.y + dv.y, q.z + dv.z, q.w + dv.w));
         }
     }
     NAGA_PIPE_END
@@ -1033,8 +1081,11 @@ __global__ void __launch_bounds__(MTR<L>::BLOCK) k_pml_gather(const WorkItem* __
 // the benchmark scene stays resident in one wave (measured: 17.4 -> 13.8
 // and 15.4 -> 13.5 us; a bound of 2 allows 117 registers but needs three
 // waves)
-template <class L, int KB>
-__device__ __forceinline__ float4 edge_sum(const float2* tile, int kb, int nn, int ns, const float* rows, int c) {
+// (S1ROWS: rows in the collision scratch layout, see s1_ld; else rows of
+// QP floats)
+template <class L, int KB, bool S1ROWS>
+__device__ __forceinline__ float4 edge_sum(const float2* tile, int kb, int nn, int ns, const float* rows, int64_t n,
+                                           int c) {
     float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
     constexpr int B = 16;
     for (int s0 = 0; s0 < kb; s0 += B) {
@@ -1045,7 +1096,7 @@ __device__ __forceinline__ float4 edge_sum(const float2* tile, int kb, int nn, i
             if (KB > 0 || s0 + u < kb) {
                 const float2 r = tile[(s0 + u) * nn + ns];
                 w[u] = r.x;
-                v[u] = ld4g<L>(rows, __float_as_uint(r.y), c);
+                v[u] = S1ROWS ? s1_ldg<L>(rows, n, __float_as_uint(r.y), c) : ld4g<L>(rows, __float_as_uint(r.y), c);
             }
         }
 #pragma unroll
@@ -1072,9 +1123,9 @@ __global__ void __launch_bounds__(MTF<L>::BLOCK, 5) k_edge_collide(const WorkIte
     const int nn = (int)(it.end - it.begin);
     const int64_t i = (int64_t)it.begin + ns;
     if (ns < nn && c < G::NCH) {
-        const float4 acc = edge_sum<L, KB>(tile, kb, nn, ns, S.S1P, c);
-        const float4 d = ld4rw(S.S1, i, QP, c);
-        st4(S.S1, i, QP, c, make_float4(acc.x + d.x, acc.y + d.y, acc.z + d.z, acc.w + d.w));
+        const float4 acc = edge_sum<L, KB, true>(tile, kb, nn, ns, S.S1P, S.N, c);
+        const float4 d = s1_ld<L>(S.S1, S.N, i, c);
+        s1_st<L>(S.S1, S.N, i, c, make_float4(acc.x + d.x, acc.y + d.y, acc.z + d.z, acc.w + d.w));
     }
     NAGA_PIPE_END
 }
@@ -1103,10 +1154,10 @@ __global__ void __launch_bounds__(MTFF<L>::BLOCK, (L::D == 3 ? 6 : 12)) k_filter
     const int nn = (int)(it.end - it.begin);
     const int64_t i = (int64_t)it.begin + ns;
     if (ns < nn && c < G::NCH) {
-        const float4 f = ld4rw(S.S1, i, QP, c);
-        // D2Q9 thread 0 also carries the rest population
+        const float4 f = s1_ld<L>(S.S1, S.N, i, c);
+        // D2Q9 thread 0 also carries the rest population (s1_ld's chunk 2)
         const bool rest = L::D == 2 && c == 0;
-        const float fr = rest ? S.S1[i * QP + REST] : 0.f;
+        const float fr = rest ? s1_ld<L>(S.S1, S.N, i, L::NGATHER).x : 0.f;
         float outr = fr;
         float4 out;
         if (i < S.nbl) {
@@ -1116,12 +1167,12 @@ __global__ void __launch_bounds__(MTFF<L>::BLOCK, (L::D == 3 ? 6 : 12)) k_filter
             for (int s = 0; s < k; ++s) {
                 const float2 r = tile[s * nn + ns];
                 const uint32_t j = __float_as_uint(r.y);
-                const float4 v = ld4g<L>(S.S1, j, c);
+                const float4 v = s1_ldg<L>(S.S1, S.N, j, c);
                 sum.x = fmaf(r.x, v.x - f.x, sum.x);
                 sum.y = fmaf(r.x, v.y - f.y, sum.y);
                 sum.z = fmaf(r.x, v.z - f.z, sum.z);
                 sum.w = fmaf(r.x, v.w - f.w, sum.w);
-                if (rest) sumr = fmaf(r.x, __ldg(S.S1 + (int64_t)j * QP + REST) - fr, sumr);
+                if (rest) sumr = fmaf(r.x, s1_ldg<L>(S.S1, S.N, j, L::NGATHER).x - fr, sumr);
             }
             out = make_float4(fmaf(0.75f, sum.x, f.x), fmaf(0.75f, sum.y, f.y), fmaf(0.75f, sum.z, f.z),
                               fmaf(0.75f, sum.w, f.w));
@@ -1473,7 +1524,7 @@ __global__ void __launch_bounds__(MTF<L>::BLOCK, 5) k_edge_interp(const WorkItem
     const int nn = (int)(it.end - it.begin);
     const int64_t i = (int64_t)it.begin + ns;
     if (ns < nn && c < G::NCH) {
-        const float4 acc = edge_sum<L, KB>(tile, kb, nn, ns, S.G, c);
+        const float4 acc = edge_sum<L, KB, false>(tile, kb, nn, ns, S.G, S.N, c);
         st4(S.G, i, QP, c, acc);
     }
     NAGA_PIPE_END
