@@ -39,3 +39,20 @@ def test_gather_bytes_one_row_per_reference():
     assert gb["edge_collide"] == gb["edge_interp"] == 4 * 32 * 112
     # every step kernel with a gather is covered, and only those
     assert set(gb) == set(bench.kernel_bytes(3, 20, 10, 6, 4, 32, 32, (7, 50))) - {"macro_pml"}
+
+
+def test_dominant_kernel_counts_the_rk_stages_as_one():
+    # the PML gather is the longest single launch, but the four RK stages
+    # (one kernel, four launches a step) take the largest share
+    kb = bench.kernel_bytes(3, 20, 10, 6, 4, 32, 32, (7, 50))
+    prof = {n: (5, 0.30) for n in kb}
+    prof.update({"pml_gather": (5, 0.40), "rk_stage1": (5, 0.34), "rk_stage2": (5, 0.36),
+                 "rk_stage3": (5, 0.36), "rk_stage4": (5, 0.36)})
+    top, per_launch, avg_ms, members = bench.dominant_kernel(kb, prof)
+    assert top == "rk_stage1..4" and members == list(bench.RK_STAGES)
+    assert per_launch == sum(kb[n] for n in bench.RK_STAGES) / 4
+    assert abs(avg_ms - (0.34 + 3 * 0.36) / 20) < 1e-12
+    # a kernel that takes more than the four stages together is dominant
+    prof["filter"] = (5, 2.0)
+    top, per_launch, avg_ms, members = bench.dominant_kernel(kb, prof)
+    assert top == "filter" and members == ["filter"] and per_launch == kb["filter"] and avg_ms == 2.0 / 5
