@@ -83,7 +83,7 @@ struct SceneDev {
     const float* src_vals;
     int64_t src_n, src_first, src_steps;  // rows apply to steps [src_first, src_first + src_steps)
     float* probe_ring;
-    double* partials;  // [n_all_items][2 QP], slot order
+    double* partials;  // [2 QP][n_all_items]: column t (slot order) of every item's sums
     float* means;      // [2 QP], slot order
     unsigned long long* step;
 };

@@ -699,7 +699,7 @@ __global__ void __launch_bounds__(kBlock, (L::D == 3 ? 4 : 8)) k_macro_pml(const
     }
     __syncthreads();
     if (threadIdx.x < 2 * QP)
-        S.partials[(int64_t)it.local * 2 * QP + threadIdx.x] =
+        S.partials[(int64_t)threadIdx.x * S.n_all_items + it.local] =
             touches ? red[0][threadIdx.x] + red[1][threadIdx.x] : 0.0;
     NAGA_END_ITEMS
 }
@@ -720,19 +720,20 @@ __global__ void __launch_bounds__(256) k_scene_tail(const SceneDev* __restrict__
     const int t = blockIdx.y;
     if (t < 2 * QP) {
         // the thread's partials in item order, loads issued eight at a time
-        // ahead of their adds (same order of additions)
+        // ahead of their adds (same order of additions); column t is
+        // contiguous, so the block's loads are coalesced
         double acc = 0.0;
-        const double* col = S.partials + t;
+        const double* col = S.partials + (int64_t)t * S.n_all_items;
         const int bs = (int)blockDim.x;
         int it = threadIdx.x;
         for (; it + 7 * bs < S.n_all_items; it += 8 * bs) {
             double v[8];
 #pragma unroll
-            for (int u = 0; u < 8; ++u) v[u] = col[(int64_t)(it + u * bs) * 2 * QP];
+            for (int u = 0; u < 8; ++u) v[u] = col[it + u * bs];
 #pragma unroll
             for (int u = 0; u < 8; ++u) acc += v[u];
         }
-        for (; it < S.n_all_items; it += bs) acc += col[(int64_t)it * 2 * QP];
+        for (; it < S.n_all_items; it += bs) acc += col[it];
         red[threadIdx.x] = acc;
         __syncthreads();
         for (int o = blockDim.x / 2; o >= 32; o >>= 1) {
